@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: A^H A (normal-operator) applies/s of the laminography operator.
+
+Workload (the reference's README-size reconstruction): recon 3 x 51 x 511 x 511
+float32, padded internally to (W, T, H) = (721, 71, 721); 4 gamma datasets
+(0/45/90/135 deg) x 361 angles uniform in [0, 2 pi) (seeded); 511 x 511
+detector padded to 1233 x 1233 (MBIR2 padding).  One step = one sum-over-gamma
+A^H A apply (src/gradient.cpp:34-89 summed as src/mbir_sb.cpp:89-97) through
+the Toeplitz operator, inputs resident in HBM.  Inputs (443 MB) and spectra
+(GBs) exceed the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per rank, launched by torchrun); the
+operator has no cross-GPU exchange.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "A^H A applies/s at 3x51x511x511"
+RECON = (51, 511, 511)              # (T, H, W) as in the reference's config
+PADDED = (721, 71, 721)             # internal (W, T, H) after MBIR2 padding
+GAMMAS_DEG = (0.0, 45.0, 90.0, 135.0)
+NPROJ = 361
+DET_PADDED = 1233
+
+
+def workload_config(precision: str, n: int):
+    return {
+        "workload": "toeplitz normal operator, 3x51x511x511 recon (padded 721x71x721), "
+                    "4 gammas x 361 angles, 1233x1233 padded projections",
+        "recon_dims": list(RECON), "padded_dims": list(PADDED), "gammas_deg": list(GAMMAS_DEG),
+        "angles_per_gamma": NPROJ, "projection_grid": [DET_PADDED, DET_PADDED],
+        "kernel_spectra": precision, "parallelism": f"replicas{n}" if n > 1 else "single",
+        "l2": "inputs larger than L2 (x 443 MB, spectra > 1 GB); no flush",
+    }
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port, bounded sample, extrapolated to one apply
+# ---------------------------------------------------------------------------
+
+_CPU_CACHE: dict = {}
+
+
+def cpu_sample_seconds(planes: int = 16, rows: int = 64):
+    """Time the oracle's FP32 ES-kernel NUFFT pieces at the full workload size on a
+    bounded sample and extrapolate one sum-over-gamma sysmat apply (per gamma
+    3 type-2 + 3 type-1 transforms, src/gradient.cpp:34-89; each = one fine-grid
+    3-D FFT + gridding of 361 x 1233^2 points).
+
+    Sample: the three 1-D FFT passes of the (1458, 144, 1458) complex64 fine grid
+    over `planes`-thick slabs, and ES interp + spread of `rows` detector rows of
+    one projection.  Returns (seconds per apply, threads, description)."""
+    import ctypes
+
+    import numpy as np
+    from oracle import oracle as O
+    import scipy.fft as sfft
+
+    w, beta = O.es_params(1.2e-6)
+    nf = tuple(O.next_smooth_even(max(2 * n, 2 * w)) for n in PADDED)  # (z, y, x)
+    threads = O.num_threads()
+    if "G" not in _CPU_CACHE:  # one-off setup, outside the timed sample
+        rng = np.random.default_rng(0)
+        th = rng.uniform(0, 2 * np.pi, 1).astype(np.float32)
+        pg = O.PolarGrid(th, DET_PADDED, DET_PADDED, np.float32(np.pi / 4))
+        _CPU_CACHE["pts"] = (pg.x[0], pg.y[0], pg.z[0])
+        G = np.zeros(nf, np.complex64)
+        G[:64] = (rng.standard_normal((64,) + nf[1:]) + 1j).astype(np.complex64)
+        G[:, :64] = 1.0 + 0.5j
+        _CPU_CACHE["G"] = G
+    G = _CPU_CACHE["G"]
+    r0 = (DET_PADDED - rows) // 2
+    x, y, z = (np.ascontiguousarray(a[r0:r0 + rows]).ravel() for a in _CPU_CACHE["pts"])
+    fp = ctypes.POINTER(ctypes.c_float)
+    lib = O._lib()
+    c = np.zeros(x.size, np.complex64)
+    t = time.perf_counter()
+    sfft.fft(G[:planes], axis=2, workers=threads)        # x lines of `planes` z-planes
+    t_x = time.perf_counter() - t
+    t = time.perf_counter()
+    sfft.fft(G[:planes], axis=1, workers=threads)        # y lines of `planes` z-planes
+    t_y = time.perf_counter() - t
+    t = time.perf_counter()
+    sfft.fft(G[:, :planes], axis=0, workers=threads)     # z lines of `planes` y-planes
+    t_z = time.perf_counter() - t
+    t = time.perf_counter()
+    lib.oracle_es_interp_f(x.size, x.ctypes.data_as(fp), y.ctypes.data_as(fp), z.ctypes.data_as(fp),
+                           nf[2], nf[1], nf[0], G.view(np.float32).ctypes.data_as(fp), w, beta,
+                           c.view(np.float32).ctypes.data_as(fp))
+    t_int = time.perf_counter() - t
+    t = time.perf_counter()
+    lib.oracle_es_spread_f(x.size, x.ctypes.data_as(fp), y.ctypes.data_as(fp), z.ctypes.data_as(fp),
+                           c.view(np.float32).ctypes.data_as(fp), nf[2], nf[1], nf[0],
+                           G.view(np.float32).ctypes.data_as(fp), w, beta)
+    t_spr = time.perf_counter() - t
+    fft3 = t_x * nf[0] / planes + t_y * nf[0] / planes + t_z * nf[1] / planes
+    per_proj = DET_PADDED / rows
+    grid_int = t_int * per_proj * NPROJ
+    grid_spr = t_spr * per_proj * NPROJ
+    per_apply = len(GAMMAS_DEG) * (6 * fft3 + 3 * grid_int + 3 * grid_spr)
+    sample = (f"oracle port, FP32 ES kernel w={w}, full-size fine grid {nf}: 1-D FFT passes over "
+              f"{planes}-plane slabs (3-D FFT extrapolated {fft3:.2f} s) and interp/spread of {rows} of "
+              f"{DET_PADDED} rows of one projection (extrapolated {grid_int:.2f} / {grid_spr:.2f} s per "
+              f"361-angle transform); one apply = 4 gammas x (6 FFT + 3 interp + 3 spread)")
+    return per_apply, threads, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    # per-step sample sized so warmup + steps stay within a few minutes
+    budget = 150.0 / (args.steps + args.warmup)
+    planes, rows = (16, 64) if budget > 1.5 else ((8, 32) if budget > 0.5 else (4, 8))
+    for _ in range(args.warmup):
+        cpu_sample_seconds(planes, rows)
+    t_start = time.perf_counter()
+    samples = []
+    for _ in range(args.steps):
+        sec, threads, sample = cpu_sample_seconds(planes, rows)
+        samples.append(sec)
+    wall = time.perf_counter() - t_start
+    mean = statistics.mean(samples)
+    v = 1.0 / mean
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "applies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config("n/a", args.gpus),
+        "cpu_baseline": {"value": v, "unit": "applies/s", "cores": threads, "kind": "port",
+                         "sample": sample + "; reference CPU path = this project's oracle port "
+                                            "(FINUFFT/FFTW absent, reference NUFFT path unbuildable)"},
+        "e2e": {"value": v, "unit": "applies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "50", "-i", str(gpu_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def synthetic_magnetization_gpu(torch, dims, seed=1234, sigma=5.0, lateral_frac=0.8):
+    """Unit vectors i.i.d. per voxel, Gaussian-smoothed (sigma voxels, reflect),
+    renormalised, zeroed outside a full-thickness x central-80% lateral slab."""
+    import torch.nn.functional as F
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    m = torch.randn((3,) + tuple(dims), device="cuda", generator=g)
+    m = m / (torch.linalg.vector_norm(m, dim=0, keepdim=True) + 1e-12)
+    r = int(3 * sigma)
+    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device="cuda", dtype=torch.float32) / sigma) ** 2)
+    k = k / k.sum()
+    v = m.unsqueeze(1)  # (3, 1, n1, n2, n3)
+    for ax in range(3):
+        shape = [1, 1, 1, 1, 1]
+        shape[2 + ax] = 2 * r + 1
+        pad = [0, 0, 0, 0, 0, 0]
+        pad[2 * (2 - ax)] = pad[2 * (2 - ax) + 1] = r
+        v = F.conv3d(F.pad(v, pad, mode="reflect"), k.view(shape))
+    m = v.squeeze(1)
+    m = m / (torch.linalg.vector_norm(m, dim=0, keepdim=True) + 1e-12)
+    n1, n2, n3 = dims
+    a1, a3 = round(n1 * (1 - lateral_frac) / 2), round(n3 * (1 - lateral_frac) / 2)
+    mask = torch.zeros(dims, device="cuda")
+    mask[a1:n1 - a1, :, a3:n3 - a3] = 1
+    return (m * mask).contiguous()
+
+
+def read_traffic(stage: str):
+    """DRAM bytes per launch of a stage's kernel from the committed ncu summary, if any."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            txt = f.read()
+        m = re.search(rf"traffic\[{re.escape(stage)}\]:\s*([0-9.eE+]+)", txt)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import lamino_b200 as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    L.lib()
+
+    rng = np.random.default_rng(2026)
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, NPROJ).astype(np.float32), DET_PADDED, DET_PADDED,
+                       np.float32(np.deg2rad(g))) for g in GAMMAS_DEG]
+    t0 = time.perf_counter()
+    op = L.ToeplitzNormal(pgs, PADDED, args.precision)
+    build_s = time.perf_counter() - t0
+    x = synthetic_magnetization_gpu(torch, PADDED)
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        op(x, out=y)
+    torch.cuda.synchronize()
+
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    phys = int(visible.split(",")[local]) if visible else local
+    op.profile(True, args.steps)
+    sampler = ClockSampler(phys) if rank == 0 else None
+    time.sleep(0.2 if sampler else 0)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op(x, out=y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = e0.elapsed_time(e1)
+    stages, napplies, kpa = op.stage_times()
+    op.profile(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    value = world * args.steps / (ms / 1e3)
+
+    # e2e: the same apply through the C ABI with pinned host buffers (H2D + apply + D2H)
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    for _ in range(2):
+        op(xh, out=yh)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k_e2e = args.steps
+    f0.record(stream)
+    for _ in range(k_e2e):
+        op(xh, out=yh)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = t.item()
+    nbytes = x.numel() * 4
+
+    # roofline of the dominant stage
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms = stages[dom][0] / max(napplies, 1)
+    dom_bytes = stages[dom][1]
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": read_traffic(dom),
+                "stages_ms_per_apply": {k: v[0] / max(napplies, 1) for k, v in stages.items()},
+                "stages_algorithmic_bytes": {k: v[1] for k, v in stages.items()}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded smoothed unit-vector magnetization, "
+                                                     "seeded angles)",
+        "config": workload_config(args.precision, world),
+        "e2e": {"value": world * k_e2e / (ms_e2e / 1e3), "unit": "applies/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": kpa * args.steps,
+        "roofline": roofline,
+        "clocks": clocks,
+        "operator_build_s": build_s,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, threads, sample = cpu_sample_seconds(128, DET_PADDED)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "applies/s", "cores": threads, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,167 @@
+/*
+ * lamino_b200 C ABI: the GPU (sm_100a) laminography operator and solvers.
+ *
+ * Drop-in boundary for the reference's FINUFFT/OpenMP path.  Every entry point
+ * names the reference interface it replaces (paths relative to the reference
+ * project root).  Conventions:
+ *   - All functions return 0 on success or a LAMINO_ERR_* code; the message of
+ *     the last failure on the calling thread is lamino_last_error().  No C++
+ *     exception crosses this boundary.
+ *   - Array pointers may be host or device memory (detected per call); host
+ *     buffers are staged through device memory inside the call.
+ *   - Volumes are 3 contiguous float32 components [3][n1][n2][n3] (n3 fastest),
+ *     in the reference's internal order (n1, n2, n3) = (W, T, H).
+ *   - Projections are float32 [nproj][nrows][ncols] (ncols fastest).
+ *   - `stream` is a cudaStream_t (NULL = default stream).  Calls with host
+ *     buffers synchronise the stream before returning.
+ *   - Handles are thread-compatible: one thread at a time per handle.
+ */
+#ifndef LAMINO_H
+#define LAMINO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAMINO_OK 0
+#define LAMINO_ERR_ARG 1
+#define LAMINO_ERR_OOM 2
+#define LAMINO_ERR_CUDA 3
+#define LAMINO_ERR_CUFFT 4
+#define LAMINO_ERR_TIMEOUT 5
+#define LAMINO_ERR_NONFINITE 6
+#define LAMINO_ERR_STATE 7
+
+typedef struct lamino_geom_s *lamino_geom_t;     /* one gamma dataset's polar grid */
+typedef struct lamino_plan_s *lamino_plan_t;     /* NUFFT plan for one volume size */
+typedef struct lamino_normal_s *lamino_normal_t; /* Toeplitz sum_gamma sysmat */
+typedef struct lamino_op_s *lamino_op_t;         /* any normal operator, for the solvers */
+
+/* Message of the last failure on this thread ("" if none). */
+const char *lamino_last_error(void);
+/* Library version string. */
+const char *lamino_version(void);
+
+/* ---- geometry ------------------------------------------------------------
+ * Replaces tomocam::PolarGrid<float>::PolarGrid(angles, nrows, ncols, gamma)
+ * (include/polar_grid.h:44-75).  `angles` (radians) and `gamma` are host values.
+ */
+int lamino_geom_create(const float *angles, int64_t nproj, int64_t nrows, int64_t ncols, float gamma,
+                       lamino_geom_t *out);
+/* Materialises the PolarGrid x, y, z arrays (each nproj*nrows*ncols floats). */
+int lamino_geom_points(lamino_geom_t g, float *x, float *y, float *z, void *stream);
+int lamino_geom_destroy(lamino_geom_t g);
+
+/* ---- NUFFT plan -----------------------------------------------------------
+ * Replaces tomocam::nufft::plans::cache<float> / FinufftPlanWrapper<float>
+ * (include/finufft_plan_cache.h:34-72, include/finufft_plan.h:93-129): one
+ * plan per volume size (n1, n2, n3) and tolerance instead of one per process.
+ * eps = 1.2e-6 reproduces the reference's float tolerance (finufft_plan.h:66).
+ */
+int lamino_plan_create(int64_t n1, int64_t n2, int64_t n3, double eps, lamino_plan_t *out);
+int lamino_plan_destroy(lamino_plan_t p);
+/* Type 2, iflag -1: c[j] = sum_k modes[k] e^{-i k.x_j} (include/nufft.h:52-64).
+ * modes: complex64 interleaved [n1][n2][n3]; c: complex64 [nproj][nrows][ncols]. */
+int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream);
+/* Type 1, iflag +1: modes[k] = sum_j c[j] e^{+i k.x_j} (include/nufft.h:37-49). */
+int lamino_nufft3d1(lamino_plan_t p, lamino_geom_t g, const float *c, float *modes, void *stream);
+
+/* ---- operators ------------------------------------------------------------ */
+/* tomocam::forward (include/projection.h:52-54, src/projection.cpp:42-77):
+ * m3 [3][n1][n2][n3] -> proj [nproj][nrows][ncols]. */
+int lamino_forward(lamino_plan_t p, lamino_geom_t g, const float *m3, float *proj, void *stream);
+/* tomocam::adjoint (include/projection.h:64-66, src/projection.cpp:90-126). */
+int lamino_adjoint(lamino_plan_t p, lamino_geom_t g, const float *proj, float *m3, void *stream);
+/* sum over geometries of tomocam::sysmat (include/tomocam.h:50-52, src/gradient.cpp:34-89),
+ * evaluated with the NUFFT (interp -> weight -> spread) on the GPU. */
+int lamino_sysmat(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, const float *x3, float *y3,
+                  void *stream);
+/* tomocam::gradient (include/tomocam.h:64-67, src/gradient.cpp:98-105): sysmat(f) - yT. */
+int lamino_gradient(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float *out3,
+                    void *stream);
+/* tomocam::residual (include/tomocam.h:79-82, src/gradient.cpp:117-127). */
+int lamino_residual(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float yTy, double *out,
+                    void *stream);
+
+/* ---- Toeplitz normal operator ----------------------------------------------
+ * sum_gamma sysmat as a 3x3 block convolution (no reference counterpart; it
+ * replaces the MBIR `A` closures src/mbir_cg.cpp:97-105, src/mbir_sb.cpp:89-97).
+ * precision: 0 = FP32 spectra, 1 = FP16 spectra with per-plane power-of-two scales.
+ */
+#define LAMINO_PREC_FP32 0
+#define LAMINO_PREC_FP16 1
+int lamino_normal_create(const lamino_geom_t *geoms, int ngeom, int64_t n1, int64_t n2, int64_t n3, int precision,
+                         lamino_normal_t *out, void *stream);
+int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *stream);
+/* Embedding-grid sizes L[3] = (L1, L2, L3) and device bytes held by the operator. */
+int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes);
+int lamino_normal_destroy(lamino_normal_t op);
+/* Per-stage CUDA-event timing of lamino_normal_apply on the launching stream
+ * (measurement hook; no reference counterpart).  enable != 0 records events for
+ * up to max_applies subsequent applies. */
+int lamino_normal_profile(lamino_normal_t op, int enable, int max_applies);
+/* Stage timings accumulated since lamino_normal_profile: nstages (<= 8) stages in
+ * the order pad, r2c, multiply, c2r, crop; ms[k] summed milliseconds; bytes[k] the
+ * algorithmic bytes of one apply of stage k; napplies profiled applies;
+ * kernels_per_apply this library's kernel launches in one apply.  Any output
+ * pointer except nstages may be NULL. */
+int lamino_normal_stage_times(lamino_normal_t op, int *nstages, double *ms, int64_t *bytes, int *napplies,
+                              int *kernels_per_apply);
+
+/* ---- regularisers / finite differences (one component of dims n1,n2,n3) ---- */
+/* tomocam::opt::qggmrf (include/optimize.h:146-153, src/qggmrf.cpp:60-95): g += prior gradient. */
+int lamino_qggmrf(float *g, const float *x, int64_t n1, int64_t n2, int64_t n3, float sigma, float p,
+                  void *stream);
+/* tomocam::opt::grad_u (src/finitediff.cpp:8-47): out3 = 3 directional central differences. */
+int lamino_grad_u(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out3, void *stream);
+/* tomocam::opt::divergence (src/finitediff.cpp:54-71): negative divergence of du3. */
+int lamino_divergence(const float *du3, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream);
+/* tomocam::opt::laplacian (include/bregman.h:34-36): divergence(grad_u(u)). */
+int lamino_laplacian(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream);
+/* tomocam::opt::RampPreconditioner::apply (include/precond.h:72-86), all 3 components. */
+int lamino_ramp_precond(const float *r3, int64_t n1, int64_t n2, int64_t n3, float *z3, void *stream);
+
+/* ---- solvers over a normal operator ---------------------------------------- */
+/* Operator handles: the Toeplitz operator, or the NUFFT form over geometries. */
+int lamino_op_from_normal(lamino_normal_t n, lamino_op_t *out);
+int lamino_op_from_plan(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, lamino_op_t *out);
+int lamino_op_apply(lamino_op_t op, const float *x3, float *y3, void *stream);
+int lamino_op_destroy(lamino_op_t op);
+/* tomocam::opt::cgsolver (include/optimize.h:101-103, src/conjgrad.cpp:37-117).
+ * x3: x0 on entry, solution on exit.  iters (may be NULL): iterations run. */
+int lamino_cgsolver(lamino_op_t A, const float *y3, float *x3, int64_t n1, int64_t n2, int64_t n3, int max_iter,
+                    float tol, int *iters, void *stream);
+/* tomocam::opt::split_bregman (include/optimize.h:85-88, src/bregman.cpp:39-134). */
+int lamino_split_bregman(lamino_op_t A, const float *yT3, float *x3, int64_t n1, int64_t n2, int64_t n3,
+                         float lambda, float mu, int outer_max, int inner_max, float tol, float xtol, int *iters,
+                         void *stream);
+/* tomocam::opt::lipschitz (include/optimize.h:135-137, src/lipschitz.cpp:31-53):
+ * power-iteration estimate of ||A|| with FP64 norms and a seeded start. */
+int lamino_lipschitz(lamino_op_t A, int64_t n1, int64_t n2, int64_t n3, int max_iters, double tol, uint64_t seed,
+                     double *L, void *stream);
+
+/* ---- MBIR drivers ------------------------------------------------------------
+ * tomocam::MBIR1 / MBIR2 / MBIR3 (include/tomocam.h:101-154; src/mbir_cg.cpp:48-128,
+ * src/mbir_sb.cpp:47-114, src/mbir3.cpp:47-135).  Fields default as
+ * tomocam::ReconParams (include/config.h:146-158); lamino_recon_params_default fills them.
+ * op_kind: 0 Toeplitz FP32, 1 Toeplitz FP16 spectra, 2 NUFFT form.
+ */
+typedef struct {
+    int max_iters, inner_iters;
+    float sigma, p, lambda, mu, tol, xtol, pad_factor;
+    int op_kind;
+    double eps;
+} lamino_recon_params;
+void lamino_recon_params_default(lamino_recon_params *p);
+/* method 1, 2 or 3.  projs[i]: [proj_dims[3i]][proj_dims[3i+1]][proj_dims[3i+2]];
+ * angles[i]: proj_dims[3i] radians (host); out3: [3][r1][r2][r3]. */
+int lamino_mbir(int method, int ndatasets, const float *const *projs, const int64_t *proj_dims,
+                const float *const *angles, const float *gammas, int64_t r1, int64_t r2, int64_t r3,
+                const lamino_recon_params *params, float *out3, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LAMINO_H */

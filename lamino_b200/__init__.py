@@ -1,0 +1,510 @@
+"""lamino_b200: B200-native laminography NUFFT operator and solvers.
+
+Python mirror of the reference's operator surface (``tomocam::PolarGrid``,
+``forward``, ``adjoint``, ``sysmat``, ``gradient``, ``residual``, ``MBIR1-3``
+and ``tomocam::opt::*``) over the C ABI of ``liblamino_b200.so``
+(include/lamino.h).  Arrays may be numpy arrays (host; staged through device
+memory by the library) or torch CUDA tensors (device; used in place).  There is
+no CPU fallback: every call goes through the CUDA library and raises if it is
+missing or fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+__all__ = [
+    "LaminoError", "lib", "PolarGrid", "NufftPlan", "ToeplitzNormal", "beam_dir_vector",
+    "forward", "adjoint", "sysmat", "gradient", "residual", "nufft3d1", "nufft3d2",
+    "MBIR1", "MBIR2", "MBIR3", "ReconParams", "opt", "padded_volume_dims",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblamino_b200.so")
+_lib = None
+
+
+class LaminoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"lamino error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load liblamino_b200.so (building it first if it is missing and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _b
+        _b.build()
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i64, i32, f32, f64 = (ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_float,
+                              ctypes.c_double)
+    P = ctypes.POINTER
+    sig = {
+        "lamino_last_error": ([], ctypes.c_char_p),
+        "lamino_version": ([], ctypes.c_char_p),
+        "lamino_geom_create": ([vp, i64, i64, i64, f32, P(vp)], i32),
+        "lamino_geom_points": ([vp, vp, vp, vp, vp], i32),
+        "lamino_geom_destroy": ([vp], i32),
+        "lamino_plan_create": ([i64, i64, i64, f64, P(vp)], i32),
+        "lamino_plan_destroy": ([vp], i32),
+        "lamino_nufft3d2": ([vp, vp, vp, vp, vp], i32),
+        "lamino_nufft3d1": ([vp, vp, vp, vp, vp], i32),
+        "lamino_forward": ([vp, vp, vp, vp, vp], i32),
+        "lamino_adjoint": ([vp, vp, vp, vp, vp], i32),
+        "lamino_sysmat": ([vp, P(vp), i32, vp, vp, vp], i32),
+        "lamino_gradient": ([vp, vp, vp, vp, vp, vp], i32),
+        "lamino_residual": ([vp, vp, vp, vp, f32, P(f64), vp], i32),
+        "lamino_normal_create": ([P(vp), i32, i64, i64, i64, i32, P(vp), vp], i32),
+        "lamino_normal_apply": ([vp, vp, vp, vp], i32),
+        "lamino_normal_info": ([vp, P(i64), P(i64)], i32),
+        "lamino_normal_destroy": ([vp], i32),
+        "lamino_normal_profile": ([vp, i32, i32], i32),
+        "lamino_normal_stage_times": ([vp, P(i32), P(f64), P(i64), P(i32), P(i32)], i32),
+        "lamino_qggmrf": ([vp, vp, i64, i64, i64, f32, f32, vp], i32),
+        "lamino_grad_u": ([vp, i64, i64, i64, vp, vp], i32),
+        "lamino_divergence": ([vp, i64, i64, i64, vp, vp], i32),
+        "lamino_laplacian": ([vp, i64, i64, i64, vp, vp], i32),
+        "lamino_ramp_precond": ([vp, i64, i64, i64, vp, vp], i32),
+        "lamino_op_from_normal": ([vp, P(vp)], i32),
+        "lamino_op_from_plan": ([vp, P(vp), i32, P(vp)], i32),
+        "lamino_op_apply": ([vp, vp, vp, vp], i32),
+        "lamino_op_destroy": ([vp], i32),
+        "lamino_cgsolver": ([vp, vp, vp, i64, i64, i64, i32, f32, P(i32), vp], i32),
+        "lamino_split_bregman": ([vp, vp, vp, i64, i64, i64, f32, f32, i32, i32, f32, f32, P(i32), vp], i32),
+        "lamino_lipschitz": ([vp, i64, i64, i64, i32, f64, ctypes.c_uint64, P(f64), vp], i32),
+        "lamino_recon_params_default": ([vp], None),
+        "lamino_mbir": ([i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, vp, vp], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise LaminoError(rc, lib().lamino_last_error().decode())
+
+
+def version() -> str:
+    return lib().lamino_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# array plumbing: numpy (host) or torch CUDA tensors (device)
+# ---------------------------------------------------------------------------
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a):
+    if _is_torch(a):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr())
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _as_f32(a):
+    if _is_torch(a):
+        import torch
+        if a.dtype != torch.float32:
+            raise TypeError("expected a float32 tensor")
+        return a.contiguous()
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _empty_like_kind(ref, shape, dtype="float32"):
+    if _is_torch(ref):
+        import torch
+        tdt = {"float32": torch.float32, "complex64": torch.complex64}[dtype]
+        return torch.empty(shape, dtype=tdt, device=ref.device)
+    return np.empty(shape, dtype=dtype)
+
+
+def _stream(a=None):
+    if a is not None and _is_torch(a) and a.is_cuda:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
+    return ctypes.c_void_p(0)
+
+
+# ---------------------------------------------------------------------------
+# geometry / plans / operators
+# ---------------------------------------------------------------------------
+
+def beam_dir_vector(gamma: float, alpha: float):
+    """include/projection.h:37-41 in float32."""
+    g, a = np.float32(gamma), np.float32(alpha)
+    return (np.sin(g) * np.sin(a), np.cos(a), np.cos(g) * np.sin(a))
+
+
+class PolarGrid:
+    """tomocam::PolarGrid<float> (include/polar_grid.h:44-75).  Points are not stored:
+    the GPU kernels regenerate them from per-row/column/angle factors."""
+
+    def __init__(self, angles, nrows: int, ncols: int, gamma: float):
+        self.theta = np.ascontiguousarray(angles, dtype=np.float32)
+        self.nrows, self.ncols, self.gamma = int(nrows), int(ncols), float(np.float32(gamma))
+        h = ctypes.c_void_p()
+        _check(lib().lamino_geom_create(_ptr(self.theta), len(self.theta), self.nrows, self.ncols,
+                                        self.gamma, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.lamino_geom_destroy(self._h)
+            self._h = None
+
+    def dims(self):
+        return (len(self.theta), self.nrows, self.ncols)
+
+    def nprojs(self):
+        return len(self.theta)
+
+    def size(self):
+        return len(self.theta) * self.nrows * self.ncols
+
+    def points(self):
+        """Materialise (x, y, z), each (nproj, nrows, ncols) float32, on the host."""
+        out = [np.empty(self.dims(), np.float32) for _ in range(3)]
+        _check(lib().lamino_geom_points(self._h, *[_ptr(a) for a in out], ctypes.c_void_p(0)))
+        return out
+
+
+class NufftPlan:
+    """One GPU NUFFT plan per volume size (replaces the process-global FINUFFT plan
+    cache of include/finufft_plan_cache.h:34-72)."""
+
+    def __init__(self, dims, eps: float = 1.2e-6):
+        self.dims = tuple(int(d) for d in dims)
+        h = ctypes.c_void_p()
+        _check(lib().lamino_plan_create(*self.dims, float(eps), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.lamino_plan_destroy(self._h)
+            self._h = None
+
+
+_plans: dict = {}
+
+
+def _plan_for(dims, eps=1.2e-6) -> NufftPlan:
+    key = (tuple(int(d) for d in dims), float(eps))
+    if key not in _plans:
+        _plans[key] = NufftPlan(key[0], key[1])
+    return _plans[key]
+
+
+def nufft3d2(modes, pg: PolarGrid, plan: NufftPlan | None = None):
+    """include/nufft.h:52-64: complex64 modes (n1,n2,n3) -> complex64 (nproj,nrows,ncols)."""
+    plan = plan or _plan_for(modes.shape)
+    if _is_torch(modes):
+        out = _empty_like_kind(modes, pg.dims(), "complex64")
+        m = modes.contiguous()
+    else:
+        m = np.ascontiguousarray(modes, dtype=np.complex64)
+        out = np.empty(pg.dims(), np.complex64)
+    _check(lib().lamino_nufft3d2(plan._h, pg._h, _ptr(m), _ptr(out), _stream(modes)))
+    return out
+
+
+def nufft3d1(c, pg: PolarGrid, recon_dims, plan: NufftPlan | None = None):
+    """include/nufft.h:37-49: complex64 points -> complex64 modes recon_dims."""
+    plan = plan or _plan_for(recon_dims)
+    if _is_torch(c):
+        out = _empty_like_kind(c, tuple(recon_dims), "complex64")
+        cc = c.contiguous()
+    else:
+        cc = np.ascontiguousarray(c, dtype=np.complex64)
+        out = np.empty(tuple(recon_dims), np.complex64)
+    _check(lib().lamino_nufft3d1(plan._h, pg._h, _ptr(cc), _ptr(out), _stream(c)))
+    return out
+
+
+def forward(m, pg: PolarGrid, gamma=None, plan: NufftPlan | None = None):
+    """tomocam::forward (src/projection.cpp:42-77).  m: (3, n1, n2, n3)."""
+    m = _as_f32(m)
+    plan = plan or _plan_for(m.shape[1:])
+    out = _empty_like_kind(m, pg.dims())
+    _check(lib().lamino_forward(plan._h, pg._h, _ptr(m), _ptr(out), _stream(m)))
+    return out
+
+
+def adjoint(proj, pg: PolarGrid, recon_dims, gamma=None, plan: NufftPlan | None = None):
+    """tomocam::adjoint (src/projection.cpp:90-126) -> (3, *recon_dims)."""
+    proj = _as_f32(proj)
+    plan = plan or _plan_for(recon_dims)
+    out = _empty_like_kind(proj, (3,) + tuple(recon_dims))
+    _check(lib().lamino_adjoint(plan._h, pg._h, _ptr(proj), _ptr(out), _stream(proj)))
+    return out
+
+
+def _geom_array(grids):
+    arr = (ctypes.c_void_p * len(grids))(*[g._h.value for g in grids])
+    return ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p)), arr
+
+
+def sysmat(x, grid, gamma=None, plan: NufftPlan | None = None):
+    """tomocam::sysmat (src/gradient.cpp:34-89) in NUFFT form; `grid` may be a list
+    of PolarGrids, in which case the sum over them is returned."""
+    grids = grid if isinstance(grid, (list, tuple)) else [grid]
+    x = _as_f32(x)
+    plan = plan or _plan_for(x.shape[1:])
+    out = _empty_like_kind(x, tuple(x.shape))
+    gp, keep = _geom_array(grids)
+    _check(lib().lamino_sysmat(plan._h, gp, len(grids), _ptr(x), _ptr(out), _stream(x)))
+    return out
+
+
+def gradient(f, yT, grid, gamma=None, plan=None):
+    """tomocam::gradient (src/gradient.cpp:98-105): sysmat(f) - yT."""
+    f, yT = _as_f32(f), _as_f32(yT)
+    plan = plan or _plan_for(f.shape[1:])
+    out = _empty_like_kind(f, tuple(f.shape))
+    _check(lib().lamino_gradient(plan._h, grid._h, _ptr(f), _ptr(yT), _ptr(out), _stream(f)))
+    return out
+
+
+def residual(f, yT, grid, yTy: float, gamma=None, plan=None) -> float:
+    """tomocam::residual (src/gradient.cpp:117-127)."""
+    f, yT = _as_f32(f), _as_f32(yT)
+    plan = plan or _plan_for(f.shape[1:])
+    r = ctypes.c_double()
+    _check(lib().lamino_residual(plan._h, grid._h, _ptr(f), _ptr(yT), float(yTy), ctypes.byref(r),
+                                 _stream(f)))
+    return r.value
+
+
+class ToeplitzNormal:
+    """sum_gamma sysmat as a Toeplitz (block-convolution) operator; precision
+    'fp32' or 'fp16' (spectra stored in half precision with per-plane scales)."""
+
+    def __init__(self, grids: Sequence[PolarGrid], dims, precision: str = "fp32", stream=None):
+        self.dims = tuple(int(d) for d in dims)
+        self.grids = list(grids)
+        gp, keep = _geom_array(self.grids)
+        h = ctypes.c_void_p()
+        prec = {"fp32": 0, "fp16": 1}[precision]
+        _check(lib().lamino_normal_create(gp, len(self.grids), *self.dims, prec, ctypes.byref(h),
+                                          stream or ctypes.c_void_p(0)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.lamino_normal_destroy(self._h)
+            self._h = None
+
+    def __call__(self, x, out=None):
+        x = _as_f32(x)
+        if out is None:
+            out = _empty_like_kind(x, tuple(x.shape))
+        _check(lib().lamino_normal_apply(self._h, _ptr(x), _ptr(out), _stream(x)))
+        return out
+
+    def profile(self, enable: bool, max_applies: int = 64):
+        _check(lib().lamino_normal_profile(self._h, int(bool(enable)), int(max_applies)))
+
+    def stage_times(self):
+        """{stage: (total_ms, bytes_per_apply)}, applies profiled, own kernels per apply."""
+        n = ctypes.c_int()
+        ms = (ctypes.c_double * 8)()
+        by = (ctypes.c_int64 * 8)()
+        na, kp = ctypes.c_int(), ctypes.c_int()
+        _check(lib().lamino_normal_stage_times(self._h, ctypes.byref(n), ms, by, ctypes.byref(na),
+                                               ctypes.byref(kp)))
+        names = ["pad", "r2c", "multiply", "c2r", "crop", "s5", "s6", "s7"]
+        return ({names[k]: (ms[k], by[k]) for k in range(n.value)}, na.value, kp.value)
+
+    def info(self):
+        L = (ctypes.c_int64 * 3)()
+        b = ctypes.c_int64()
+        _check(lib().lamino_normal_info(self._h, L, ctypes.byref(b)))
+        return tuple(L), b.value
+
+
+def _pad_n(n: int, f) -> int:
+    return int(n) + 2 * (int(np.float32(n) * np.float32(f)) // 2)
+
+
+def padded_volume_dims(recon_dims, method: int = 2, pad_factor=np.float32(1.4142)):
+    """Volume padding of MBIR1 (T(PAD-1.0)) and MBIR2/3 (T(PAD)-1 in float)."""
+    if method == 1:
+        f = np.float32(float(np.float32(pad_factor)) - 1.0)
+    else:
+        f = np.float32(pad_factor) - np.float32(1.0)
+    return tuple(_pad_n(n, f) for n in recon_dims)
+
+
+# ---------------------------------------------------------------------------
+# solvers (tomocam::opt)
+# ---------------------------------------------------------------------------
+
+class _Op:
+    def __init__(self, A, dims):
+        self.dims = tuple(int(d) for d in dims)
+        h = ctypes.c_void_p()
+        if isinstance(A, ToeplitzNormal):
+            _check(lib().lamino_op_from_normal(A._h, ctypes.byref(h)))
+        else:
+            plan, grids = A
+            gp, keep = _geom_array(grids)
+            _check(lib().lamino_op_from_plan(plan._h, gp, len(grids), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.lamino_op_destroy(self._h)
+
+
+class opt:  # namespace mirroring tomocam::opt
+    @staticmethod
+    def qggmrf(g, x, sigma: float, p: float):
+        """src/qggmrf.cpp:60-95: g += prior gradient (in place; returns g)."""
+        x = _as_f32(x)
+        _check(lib().lamino_qggmrf(_ptr(g), _ptr(x), *x.shape, float(sigma), float(p), _stream(x)))
+        return g
+
+    @staticmethod
+    def grad_u(u):
+        u = _as_f32(u)
+        out = _empty_like_kind(u, (3,) + tuple(u.shape))
+        _check(lib().lamino_grad_u(_ptr(u), *u.shape, _ptr(out), _stream(u)))
+        return out
+
+    @staticmethod
+    def divergence(du):
+        du = _as_f32(du)
+        out = _empty_like_kind(du, tuple(du.shape[1:]))
+        _check(lib().lamino_divergence(_ptr(du), *du.shape[1:], _ptr(out), _stream(du)))
+        return out
+
+    @staticmethod
+    def laplacian(u):
+        u = _as_f32(u)
+        out = _empty_like_kind(u, tuple(u.shape))
+        _check(lib().lamino_laplacian(_ptr(u), *u.shape, _ptr(out), _stream(u)))
+        return out
+
+    @staticmethod
+    def ramp_precond(r3):
+        r3 = _as_f32(r3)
+        out = _empty_like_kind(r3, tuple(r3.shape))
+        _check(lib().lamino_ramp_precond(_ptr(r3), *r3.shape[1:], _ptr(out), _stream(r3)))
+        return out
+
+    @staticmethod
+    def cgsolver(A, y, x0, max_iter: int, tol: float):
+        """src/conjgrad.cpp:37-117.  A: ToeplitzNormal or (NufftPlan, [PolarGrid])."""
+        y = _as_f32(y)
+        x = _as_f32(x0).clone() if _is_torch(x0) else np.array(x0, dtype=np.float32)
+        op = _Op(A, y.shape[1:])
+        it = ctypes.c_int()
+        _check(lib().lamino_cgsolver(op._h, _ptr(y), _ptr(x), *op.dims, int(max_iter), float(tol),
+                                     ctypes.byref(it), _stream(y)))
+        return x
+
+    @staticmethod
+    def split_bregman(A, yT, x0, lam, mu, outer_max, inner_max, tol, xtol):
+        """src/bregman.cpp:39-134."""
+        yT = _as_f32(yT)
+        x = _as_f32(x0).clone() if _is_torch(x0) else np.array(x0, dtype=np.float32)
+        op = _Op(A, yT.shape[1:])
+        it = ctypes.c_int()
+        _check(lib().lamino_split_bregman(op._h, _ptr(yT), _ptr(x), *op.dims, float(lam), float(mu),
+                                          int(outer_max), int(inner_max), float(tol), float(xtol),
+                                          ctypes.byref(it), _stream(yT)))
+        return x
+
+    @staticmethod
+    def lipschitz(A, dims, max_iters: int = 30, tol: float = 1e-5, seed: int = 0) -> float:
+        op = _Op(A, dims)
+        L = ctypes.c_double()
+        _check(lib().lamino_lipschitz(op._h, *op.dims, int(max_iters), float(tol), int(seed),
+                                      ctypes.byref(L), ctypes.c_void_p(0)))
+        return L.value
+
+
+# ---------------------------------------------------------------------------
+# MBIR drivers
+# ---------------------------------------------------------------------------
+
+class _ReconParamsC(ctypes.Structure):
+    _fields_ = [("max_iters", ctypes.c_int), ("inner_iters", ctypes.c_int),
+                ("sigma", ctypes.c_float), ("p", ctypes.c_float), ("lam", ctypes.c_float),
+                ("mu", ctypes.c_float), ("tol", ctypes.c_float), ("xtol", ctypes.c_float),
+                ("pad_factor", ctypes.c_float), ("op_kind", ctypes.c_int), ("eps", ctypes.c_double)]
+
+
+class ReconParams:
+    """tomocam::ReconParams defaults (include/config.h:146-158) plus the operator
+    form: op_kind 'toeplitz' (FP32 spectra), 'toeplitz_fp16' or 'nufft'."""
+
+    def __init__(self, **kw):
+        c = _ReconParamsC()
+        lib().lamino_recon_params_default(ctypes.byref(c))
+        self.maxIters, self.innerIters = c.max_iters, c.inner_iters
+        self.sigma, self.p, self.lam, self.mu = c.sigma, c.p, c.lam, c.mu
+        self.tol, self.xtol, self.PAD_FACTOR = c.tol, c.xtol, c.pad_factor
+        self.op_kind, self.eps = "toeplitz", c.eps
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+    def _c(self):
+        kind = {"toeplitz": 0, "toeplitz_fp16": 1, "nufft": 2}[self.op_kind]
+        return _ReconParamsC(int(self.maxIters), int(self.innerIters), float(self.sigma), float(self.p),
+                             float(self.lam), float(self.mu), float(self.tol), float(self.xtol),
+                             float(self.PAD_FACTOR), kind, float(self.eps))
+
+
+def _mbir(method, datasets, recon_dims, params):
+    params = params or ReconParams()
+    n = len(datasets)
+    keep = []
+    projs = (ctypes.c_void_p * n)()
+    angs = (ctypes.c_void_p * n)()
+    dims = (ctypes.c_int64 * (3 * n))()
+    gam = (ctypes.c_float * n)()
+    ref = None
+    for i, (proj, angles, gamma) in enumerate(datasets):
+        p = _as_f32(proj)
+        a = np.ascontiguousarray(angles, dtype=np.float32)
+        keep += [p, a]
+        ref = p if ref is None else ref
+        projs[i] = _ptr(p).value
+        angs[i] = _ptr(a).value
+        dims[3 * i:3 * i + 3] = list(p.shape)
+        gam[i] = float(gamma)
+    out = _empty_like_kind(ref, (3,) + tuple(recon_dims))
+    pc = params._c()
+    _check(lib().lamino_mbir(method, n, projs, dims, angs, gam, *[int(d) for d in recon_dims],
+                             ctypes.byref(pc), _ptr(out), _stream(ref)))
+    return out
+
+
+def MBIR1(datasets, recon_dims, params: ReconParams | None = None):
+    """tomocam::MBIR1 (src/mbir_cg.cpp:48-128): CG on sum_gamma sysmat."""
+    return _mbir(1, datasets, recon_dims, params)
+
+
+def MBIR2(datasets, recon_dims, params: ReconParams | None = None):
+    """tomocam::MBIR2 (src/mbir_sb.cpp:47-114): split-Bregman isotropic TV."""
+    return _mbir(2, datasets, recon_dims, params)
+
+
+def MBIR3(datasets, recon_dims, params: ReconParams | None = None):
+    """tomocam::MBIR3 (src/mbir3.cpp:47-135): Nesterov + qGGMRF."""
+    return _mbir(3, datasets, recon_dims, params)

@@ -1,0 +1,534 @@
+// C ABI of lamino_b200 (declared in include/lamino.h).  Every entry point
+// converts C++ exceptions into status codes plus a thread-local message, and
+// stages host buffers through device memory when it is given host pointers.
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/lamino.h"
+#include "mbir.cuh"
+
+using namespace lamino;
+
+struct lamino_geom_s {
+    std::unique_ptr<Geom> g;
+};
+struct lamino_plan_s {
+    std::unique_ptr<NufftPlan> p;
+};
+struct lamino_normal_s {
+    std::unique_ptr<Toeplitz> t;
+    DevBuf<float> sx, sy;  // staging for host-pointer calls, kept across calls
+};
+struct lamino_op_s {
+    OpFn fn;
+    Dims3 d;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Input array: device pointer as is, host pointer copied in.
+template <typename T>
+struct In {
+    const T *d = nullptr;
+    DevBuf<T> own;
+    bool host = false;
+    In(const T *p, size_t n, cudaStream_t s) {
+        if (!p) throw Error(ERR_ARG, "null input pointer");
+        if (is_device_ptr(p)) {
+            d = p;
+        } else {
+            host = true;
+            own.alloc(n);
+            LAMINO_CUDA(cudaMemcpyAsync(own.p, p, n * sizeof(T), cudaMemcpyHostToDevice, s));
+            d = own.p;
+        }
+    }
+};
+
+// Output array: device pointer as is, host pointer filled on finish().
+template <typename T>
+struct Out {
+    T *d = nullptr;
+    T *h = nullptr;
+    size_t n = 0;
+    DevBuf<T> own;
+    Out(T *p, size_t count, cudaStream_t s, bool preload = false) : n(count) {
+        if (!p) throw Error(ERR_ARG, "null output pointer");
+        if (is_device_ptr(p)) {
+            d = p;
+        } else {
+            h = p;
+            own.alloc(count);
+            d = own.p;
+            if (preload) LAMINO_CUDA(cudaMemcpyAsync(own.p, p, n * sizeof(T), cudaMemcpyHostToDevice, s));
+        }
+    }
+    void finish(cudaStream_t s) {
+        if (h) LAMINO_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+        if (h) LAMINO_CUDA(cudaStreamSynchronize(s));
+    }
+};
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+Dims3 dims_of(int64_t n1, int64_t n2, int64_t n3) {
+    if (n1 <= 0 || n2 <= 0 || n3 <= 0) throw Error(ERR_ARG, "dims must be positive");
+    return Dims3{n1, n2, n3};
+}
+
+std::vector<const Geom *> geoms_of(const lamino_geom_t *gs, int n) {
+    if (!gs || n <= 0) throw Error(ERR_ARG, "need at least one geometry");
+    std::vector<const Geom *> v;
+    for (int i = 0; i < n; ++i) {
+        if (!gs[i] || !gs[i]->g) throw Error(ERR_ARG, "null geometry handle");
+        v.push_back(gs[i]->g.get());
+    }
+    return v;
+}
+
+__global__ void k_points(GeomView g, float *x, float *y, float *z) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        uint32_t plane = (uint32_t)g.nrows * g.ncols;
+        int p = (int)(pid / plane);
+        uint32_t r = pid - p * plane;
+        int j = (int)(r / g.ncols), k = (int)(r % g.ncols);
+        point_xyz(g, p, j, k, x[pid], y[pid], z[pid]);
+    }
+}
+
+__global__ void k_sub(float *out, const float *a, const float *b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] - b[i];
+}
+}  // namespace
+
+#define API_BEGIN try {
+#define API_END                                                        \
+    }                                                                  \
+    catch (const Error &e) { return fail(e.code, e.what()); }          \
+    catch (const std::bad_alloc &) { return fail(ERR_OOM, "host out of memory"); } \
+    catch (const std::exception &e) { return fail(ERR_STATE, e.what()); } \
+    return LAMINO_OK;
+
+extern "C" {
+
+const char *lamino_last_error(void) { return g_err.c_str(); }
+const char *lamino_version(void) { return "lamino_b200 0.1.0 (sm_100a)"; }
+
+int lamino_geom_create(const float *angles, int64_t nproj, int64_t nrows, int64_t ncols, float gamma,
+                       lamino_geom_t *out) {
+    API_BEGIN
+    if (!angles || !out) throw Error(ERR_ARG, "null argument");
+    auto h = std::make_unique<lamino_geom_s>();
+    h->g.reset(new Geom(angles, nproj, nrows, ncols, gamma));
+    *out = h.release();
+    API_END
+}
+
+int lamino_geom_points(lamino_geom_t g, float *x, float *y, float *z, void *stream) {
+    API_BEGIN
+    if (!g) throw Error(ERR_ARG, "null geometry");
+    size_t M = (size_t)g->g->npts();
+    Out<float> ox(x, M, S(stream)), oy(y, M, S(stream)), oz(z, M, S(stream));
+    k_points<<<grid_for(M, 256), 256, 0, S(stream)>>>(g->g->view(), ox.d, oy.d, oz.d);
+    LAMINO_LAUNCH("k_points");
+    ox.finish(S(stream)); oy.finish(S(stream)); oz.finish(S(stream));
+    API_END
+}
+
+int lamino_geom_destroy(lamino_geom_t g) {
+    API_BEGIN
+    delete g;
+    API_END
+}
+
+int lamino_plan_create(int64_t n1, int64_t n2, int64_t n3, double eps, lamino_plan_t *out) {
+    API_BEGIN
+    if (!out) throw Error(ERR_ARG, "null argument");
+    if (!(eps > 0)) throw Error(ERR_ARG, "eps must be positive");
+    auto h = std::make_unique<lamino_plan_s>();
+    h->p.reset(new NufftPlan(dims_of(n1, n2, n3), eps));
+    *out = h.release();
+    API_END
+}
+
+int lamino_plan_destroy(lamino_plan_t p) {
+    API_BEGIN
+    delete p;
+    API_END
+}
+
+int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream) {
+    API_BEGIN
+    if (!p || !g) throw Error(ERR_ARG, "null handle");
+    size_t V = (size_t)p->p->vol.size(), M = (size_t)g->g->npts();
+    In<float2> in(reinterpret_cast<const float2 *>(modes), V, S(stream));
+    Out<float2> out(reinterpret_cast<float2 *>(c), M, S(stream));
+    p->p->type2(*g->g, in.d, out.d, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_nufft3d1(lamino_plan_t p, lamino_geom_t g, const float *c, float *modes, void *stream) {
+    API_BEGIN
+    if (!p || !g) throw Error(ERR_ARG, "null handle");
+    size_t V = (size_t)p->p->vol.size(), M = (size_t)g->g->npts();
+    In<float2> in(reinterpret_cast<const float2 *>(c), M, S(stream));
+    Out<float2> out(reinterpret_cast<float2 *>(modes), V, S(stream));
+    p->p->type1(*g->g, in.d, out.d, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_forward(lamino_plan_t p, lamino_geom_t g, const float *m3, float *proj, void *stream) {
+    API_BEGIN
+    if (!p || !g) throw Error(ERR_ARG, "null handle");
+    size_t V = (size_t)p->p->vol.size(), M = (size_t)g->g->npts();
+    In<float> in(m3, 3 * V, S(stream));
+    Out<float> out(proj, M, S(stream));
+    p->p->forward(*g->g, in.d, out.d, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_adjoint(lamino_plan_t p, lamino_geom_t g, const float *proj, float *m3, void *stream) {
+    API_BEGIN
+    if (!p || !g) throw Error(ERR_ARG, "null handle");
+    size_t V = (size_t)p->p->vol.size(), M = (size_t)g->g->npts();
+    In<float> in(proj, M, S(stream));
+    Out<float> out(m3, 3 * V, S(stream));
+    p->p->adjoint(*g->g, in.d, out.d, false, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_sysmat(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, const float *x3, float *y3,
+                  void *stream) {
+    API_BEGIN
+    if (!p) throw Error(ERR_ARG, "null plan");
+    auto gs = geoms_of(geoms, ngeom);
+    size_t V = (size_t)p->p->vol.size();
+    In<float> in(x3, 3 * V, S(stream));
+    Out<float> out(y3, 3 * V, S(stream));
+    p->p->normal(gs, in.d, out.d, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_gradient(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float *out3,
+                    void *stream) {
+    API_BEGIN
+    if (!p || !g) throw Error(ERR_ARG, "null handle");
+    size_t V = (size_t)p->p->vol.size();
+    In<float> in(f3, 3 * V, S(stream)), yt(yT3, 3 * V, S(stream));
+    Out<float> out(out3, 3 * V, S(stream));
+    p->p->normal({g->g.get()}, in.d, out.d, S(stream));
+    k_sub<<<grid_for(3 * V, 256), 256, 0, S(stream)>>>(out.d, out.d, yt.d, (int64_t)(3 * V));
+    LAMINO_LAUNCH("k_sub");
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_residual(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float yTy, double *res,
+                    void *stream) {
+    API_BEGIN
+    if (!p || !g || !res) throw Error(ERR_ARG, "null argument");
+    int64_t V = p->p->vol.size();
+    In<float> in(f3, 3 * V, S(stream)), yt(yT3, 3 * V, S(stream));
+    DevBuf<float> Ax(3 * V);
+    p->p->normal({g->g.get()}, in.d, Ax.p, S(stream));
+    Reducer red(6);
+    red.zero(6, S(stream));
+    for (int i = 0; i < 3; ++i) {
+        vec_dot(in.d + i * V, Ax.p + i * V, V, red.d + i, S(stream));
+        vec_dot(in.d + i * V, yt.d + i * V, V, red.d + 3 + i, S(stream));
+    }
+    red.fetch(6, S(stream));
+    double e = 0;
+    for (int i = 0; i < 3; ++i) e += std::sqrt(red.h[i] - 2.0 * red.h[3 + i] + (double)yTy);
+    *res = e;
+    API_END
+}
+
+int lamino_normal_create(const lamino_geom_t *geoms, int ngeom, int64_t n1, int64_t n2, int64_t n3, int precision,
+                         lamino_normal_t *out, void *stream) {
+    API_BEGIN
+    if (!out) throw Error(ERR_ARG, "null argument");
+    auto gs = geoms_of(geoms, ngeom);
+    auto h = std::make_unique<lamino_normal_s>();
+    h->t.reset(new Toeplitz(gs, dims_of(n1, n2, n3), precision, S(stream)));
+    *out = h.release();
+    API_END
+}
+
+int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *stream) {
+    API_BEGIN
+    if (!op) throw Error(ERR_ARG, "null operator");
+    if (!x3 || !y3) throw Error(ERR_ARG, "null array");
+    const size_t n = 3 * (size_t)op->t->vol.size();
+    cudaStream_t s = S(stream);
+    const float *xd = x3;
+    float *yd = y3;
+    const bool xh = !is_device_ptr(x3), yh = !is_device_ptr(y3);
+    if (xh) {
+        if (op->sx.n != n) op->sx.alloc(n);
+        LAMINO_CUDA(cudaMemcpyAsync(op->sx.p, x3, n * 4, cudaMemcpyHostToDevice, s));
+        xd = op->sx.p;
+    }
+    if (yh) {
+        if (op->sy.n != n) op->sy.alloc(n);
+        yd = op->sy.p;
+    }
+    op->t->apply(xd, yd, s);
+    if (yh) LAMINO_CUDA(cudaMemcpyAsync(y3, yd, n * 4, cudaMemcpyDeviceToHost, s));
+    if (xh || yh) LAMINO_CUDA(cudaStreamSynchronize(s));
+    API_END
+}
+
+int lamino_normal_profile(lamino_normal_t op, int enable, int max_applies) {
+    API_BEGIN
+    if (!op) throw Error(ERR_ARG, "null operator");
+    if (enable && max_applies <= 0) throw Error(ERR_ARG, "max_applies must be positive");
+    op->t->set_profiling(enable != 0, max_applies);
+    API_END
+}
+
+int lamino_normal_stage_times(lamino_normal_t op, int *nstages, double *ms, int64_t *bytes, int *napplies,
+                              int *kernels_per_apply) {
+    API_BEGIN
+    if (!op || !nstages) throw Error(ERR_ARG, "null argument");
+    *nstages = Toeplitz::NSTAGE;
+    double t[Toeplitz::NSTAGE];
+    int64_t b[Toeplitz::NSTAGE];
+    int na = op->t->stage_times(t);
+    op->t->stage_bytes(b);
+    for (int k = 0; k < Toeplitz::NSTAGE; ++k) {
+        if (ms) ms[k] = t[k];
+        if (bytes) bytes[k] = b[k];
+    }
+    if (napplies) *napplies = na;
+    if (kernels_per_apply) *kernels_per_apply = Toeplitz::kernels_per_apply();
+    API_END
+}
+
+int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes) {
+    API_BEGIN
+    if (!op) throw Error(ERR_ARG, "null operator");
+    const Toeplitz &t = *op->t;
+    if (L) { L[0] = t.L1; L[1] = t.L2; L[2] = t.L3; }
+    if (bytes)
+        *bytes = (int64_t)(t.K.bytes() + t.Kh.bytes() + t.Kscale.bytes() + t.xpad.bytes() + t.xhat.bytes() +
+                           t.ypad.bytes());
+    API_END
+}
+
+int lamino_normal_destroy(lamino_normal_t op) {
+    API_BEGIN
+    delete op;
+    API_END
+}
+
+int lamino_qggmrf(float *g, const float *x, int64_t n1, int64_t n2, int64_t n3, float sigma, float p,
+                  void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> xi(x, d.size(), S(stream));
+    Out<float> go(g, d.size(), S(stream), true);
+    qggmrf_add(go.d, xi.d, d, sigma, p, S(stream));
+    go.finish(S(stream));
+    API_END
+}
+
+int lamino_grad_u(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out3, void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> ui(u, d.size(), S(stream));
+    Out<float> o(out3, 3 * d.size(), S(stream));
+    grad_u(ui.d, d, o.d, S(stream));
+    o.finish(S(stream));
+    API_END
+}
+
+int lamino_divergence(const float *du3, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> di(du3, 3 * d.size(), S(stream));
+    Out<float> o(out, d.size(), S(stream));
+    divergence(di.d, d, o.d, S(stream));
+    o.finish(S(stream));
+    API_END
+}
+
+int lamino_laplacian(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> ui(u, d.size(), S(stream));
+    Out<float> o(out, d.size(), S(stream));
+    // laplacian_axpy works on 3 components; run it on a 3-slot scratch
+    DevBuf<float> u3(3 * d.size()), y3(3 * d.size());
+    LAMINO_CUDA(cudaMemsetAsync(u3.p, 0, u3.bytes(), S(stream)));
+    LAMINO_CUDA(cudaMemcpyAsync(u3.p, ui.d, d.size() * 4, cudaMemcpyDeviceToDevice, S(stream)));
+    LAMINO_CUDA(cudaMemsetAsync(y3.p, 0, y3.bytes(), S(stream)));
+    laplacian_axpy(y3.p, 1.0f, u3.p, d, S(stream));
+    LAMINO_CUDA(cudaMemcpyAsync(o.d, y3.p, d.size() * 4, cudaMemcpyDeviceToDevice, S(stream)));
+    o.finish(S(stream));
+    LAMINO_CUDA(cudaStreamSynchronize(S(stream)));
+    API_END
+}
+
+int lamino_ramp_precond(const float *r3, int64_t n1, int64_t n2, int64_t n3, float *z3, void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> ri(r3, 3 * d.size(), S(stream));
+    Out<float> o(z3, 3 * d.size(), S(stream));
+    RampPrecond M(d);
+    M.apply3(ri.d, o.d, S(stream));
+    o.finish(S(stream));
+    LAMINO_CUDA(cudaStreamSynchronize(S(stream)));
+    API_END
+}
+
+int lamino_op_from_normal(lamino_normal_t n, lamino_op_t *out) {
+    API_BEGIN
+    if (!n || !out) throw Error(ERR_ARG, "null argument");
+    auto h = std::make_unique<lamino_op_s>();
+    Toeplitz *t = n->t.get();
+    h->fn = [t](const float *x, float *y, cudaStream_t s) { t->apply(x, y, s); };
+    h->d = t->vol;
+    *out = h.release();
+    API_END
+}
+
+int lamino_op_from_plan(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, lamino_op_t *out) {
+    API_BEGIN
+    if (!p || !out) throw Error(ERR_ARG, "null argument");
+    auto gs = geoms_of(geoms, ngeom);
+    auto h = std::make_unique<lamino_op_s>();
+    NufftPlan *pl = p->p.get();
+    h->fn = [pl, gs](const float *x, float *y, cudaStream_t s) { pl->normal(gs, x, y, s); };
+    h->d = pl->vol;
+    *out = h.release();
+    API_END
+}
+
+int lamino_op_apply(lamino_op_t op, const float *x3, float *y3, void *stream) {
+    API_BEGIN
+    if (!op) throw Error(ERR_ARG, "null operator");
+    size_t V = (size_t)op->d.size();
+    In<float> in(x3, 3 * V, S(stream));
+    Out<float> out(y3, 3 * V, S(stream));
+    op->fn(in.d, out.d, S(stream));
+    out.finish(S(stream));
+    API_END
+}
+
+int lamino_op_destroy(lamino_op_t op) {
+    API_BEGIN
+    delete op;
+    API_END
+}
+
+int lamino_cgsolver(lamino_op_t A, const float *y3, float *x3, int64_t n1, int64_t n2, int64_t n3, int max_iter,
+                    float tol, int *iters, void *stream) {
+    API_BEGIN
+    if (!A) throw Error(ERR_ARG, "null operator");
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> yi(y3, 3 * d.size(), S(stream));
+    Out<float> xo(x3, 3 * d.size(), S(stream), true);
+    CgStats st = cgsolver(A->fn, yi.d, xo.d, d, max_iter, tol, S(stream));
+    if (iters) *iters = st.iters;
+    xo.finish(S(stream));
+    LAMINO_CUDA(cudaStreamSynchronize(S(stream)));
+    API_END
+}
+
+int lamino_split_bregman(lamino_op_t A, const float *yT3, float *x3, int64_t n1, int64_t n2, int64_t n3,
+                         float lambda, float mu, int outer_max, int inner_max, float tol, float xtol, int *iters,
+                         void *stream) {
+    API_BEGIN
+    if (!A) throw Error(ERR_ARG, "null operator");
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> yi(yT3, 3 * d.size(), S(stream));
+    Out<float> xo(x3, 3 * d.size(), S(stream), true);
+    int it = split_bregman(A->fn, yi.d, xo.d, d, lambda, mu, outer_max, inner_max, tol, xtol, S(stream));
+    if (iters) *iters = it;
+    xo.finish(S(stream));
+    API_END
+}
+
+int lamino_lipschitz(lamino_op_t A, int64_t n1, int64_t n2, int64_t n3, int max_iters, double tol, uint64_t seed,
+                     double *L, void *stream) {
+    API_BEGIN
+    if (!A || !L) throw Error(ERR_ARG, "null argument");
+    *L = lipschitz(A->fn, dims_of(n1, n2, n3), max_iters, tol, seed, S(stream));
+    API_END
+}
+
+void lamino_recon_params_default(lamino_recon_params *p) {
+    if (!p) return;
+    ReconParams d;
+    p->max_iters = d.max_iters;
+    p->inner_iters = d.inner_iters;
+    p->sigma = d.sigma;
+    p->p = d.p;
+    p->lambda = d.lambda;
+    p->mu = d.mu;
+    p->tol = d.tol;
+    p->xtol = d.xtol;
+    p->pad_factor = d.pad_factor;
+    p->op_kind = d.op_kind;
+    p->eps = d.eps;
+}
+
+int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *pdims, const float *const *angles,
+                const float *gammas, int64_t r1, int64_t r2, int64_t r3, const lamino_recon_params *params,
+                float *out3, void *stream) {
+    API_BEGIN
+    if (nds <= 0 || !projs || !pdims || !angles || !gammas || !params) throw Error(ERR_ARG, "null argument");
+    Dims3 rd = dims_of(r1, r2, r3);
+    ReconParams prm;
+    prm.max_iters = params->max_iters;
+    prm.inner_iters = params->inner_iters;
+    prm.sigma = params->sigma;
+    prm.p = params->p;
+    prm.lambda = params->lambda;
+    prm.mu = params->mu;
+    prm.tol = params->tol;
+    prm.xtol = params->xtol;
+    prm.pad_factor = params->pad_factor;
+    prm.op_kind = params->op_kind;
+    prm.eps = params->eps;
+    std::vector<std::unique_ptr<In<float>>> ins;
+    std::vector<Dataset> data;
+    for (int i = 0; i < nds; ++i) {
+        int64_t np = pdims[3 * i], nr = pdims[3 * i + 1], nc = pdims[3 * i + 2];
+        if (np <= 0 || nr <= 0 || nc <= 0) throw Error(ERR_ARG, "projection dims must be positive");
+        ins.emplace_back(new In<float>(projs[i], (size_t)(np * nr * nc), S(stream)));
+        data.push_back(Dataset{ins.back()->d, np, nr, nc, angles[i], gammas[i]});
+    }
+    Out<float> o(out3, 3 * rd.size(), S(stream));
+    mbir(method, data, rd, prm, o.d, S(stream));
+    o.finish(S(stream));
+    API_END
+}
+
+}  // extern "C"

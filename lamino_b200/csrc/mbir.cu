@@ -1,0 +1,167 @@
+// MBIR drivers on the GPU path: src/mbir_cg.cpp:48-128 (MBIR1, CG),
+// src/mbir_sb.cpp:47-114 (MBIR2, split Bregman), src/mbir3.cpp:47-135 (MBIR3,
+// NAG + qGGMRF).  Setup, solver and crop keep the reference's order of
+// operations and its quirks (different projection padding for MBIR1 vs 2/3,
+// yT subtracted once per gamma in the MBIR3 gradient, `mu` passed as the
+// Lipschitz constant, per-component square roots in the MBIR3 loss).
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "mbir.cuh"
+
+namespace lamino {
+
+int64_t pad_dim(int64_t n, float f) {
+    int64_t npad = 2 * ((int64_t)((float)n * f) / 2);
+    return n + npad;
+}
+
+__global__ void k_norm_pad2d(const float *__restrict__ in, int64_t np, int nr, int nc, float mx, int onr, int onc,
+                             int d1, int d2, float *__restrict__ out) {
+    const int64_t M = np * nr * nc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        int k = (int)(i % nc);
+        int64_t r = i / nc;
+        int j = (int)(r % nr);
+        int64_t p = r / nr;
+        out[(p * onr + j + d1) * onc + k + d2] = in[i] / mx;
+    }
+}
+
+void normalize_pad2d(const float *proj, int64_t np, int64_t nr, int64_t nc, float mx, float factor,
+                     DevBuf<float> &out, int64_t &onr, int64_t &onc, cudaStream_t s) {
+    int64_t p2 = 0, p3 = 0;
+    if (!(factor < 1.e-06f)) {
+        p2 = 2 * ((int64_t)((float)nr * factor) / 2);
+        p3 = 2 * ((int64_t)((float)nc * factor) / 2);
+    }
+    onr = nr + p2;
+    onc = nc + p3;
+    out.alloc(np * onr * onc);
+    LAMINO_CUDA(cudaMemsetAsync(out.p, 0, out.bytes(), s));
+    k_norm_pad2d<<<grid_for(np * nr * nc, 256), 256, 0, s>>>(proj, np, (int)nr, (int)nc, mx, (int)onr, (int)onc,
+                                                            (int)(p2 / 2), (int)(p3 / 2), out.p);
+    LAMINO_LAUNCH("k_norm_pad2d");
+}
+
+__global__ void k_crop3d3(const float *__restrict__ in, int f1, int f2, int f3, int t1, int t2, int t3, int o1,
+                          int o2, int o3, float *__restrict__ out) {
+    const int64_t V = (int64_t)t1 * t2 * t3, VF = (int64_t)f1 * f2 * f3;
+    const int c = blockIdx.y;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+        int k = (int)(i % t3);
+        int64_t r = i / t3;
+        int j = (int)(r % t2);
+        int a = (int)(r / t2);
+        out[c * V + i] = in[c * VF + ((int64_t)(a + o1) * f2 + j + o2) * f3 + k + o3];
+    }
+}
+
+void crop3d3(const float *in, Dims3 from, Dims3 to, float *out, cudaStream_t s) {
+    dim3 g(grid_for(to.size(), 256), 3);
+    k_crop3d3<<<g, 256, 0, s>>>(in, (int)from.n1, (int)from.n2, (int)from.n3, (int)to.n1, (int)to.n2, (int)to.n3,
+                                (int)((from.n1 - to.n1) / 2), (int)((from.n2 - to.n2) / 2),
+                                (int)((from.n3 - to.n3) / 2), out);
+    LAMINO_LAUNCH("k_crop3d3");
+}
+
+__global__ void k_axpy_scalar(float *__restrict__ y, float a, const float *__restrict__ x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+
+void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
+          cudaStream_t s) {
+    if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1 (CG), 2 (split Bregman) or 3 (NAG)");
+    if (data.empty()) throw Error(ERR_ARG, "no datasets");
+    // volume padding: MBIR1 uses T(PAD-1.0); MBIR2/3 use (T(PAD) - 1) in float
+    float vfac = method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor - 1.0f;
+    Dims3 od{pad_dim(recon.n1, vfac), pad_dim(recon.n2, vfac), pad_dim(recon.n3, vfac)};
+    // projection padding: MBIR1 pads by PAD-1, MBIR2/3 by PAD itself
+    float pfac = method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor;
+    const int64_t V = od.size(), n = 3 * V;
+
+    NufftPlan plan(od, prm.eps);
+    std::vector<std::unique_ptr<Geom>> geoms;
+    DevBuf<float> yT(n);
+    LAMINO_CUDA(cudaMemsetAsync(yT.p, 0, yT.bytes(), s));
+    Reducer red(8);
+    for (const Dataset &ds : data) {
+        red.zero(1, s);
+        vec_max(ds.proj, ds.nproj * ds.nrows * ds.ncols, red.d, s);
+        red.fetch(1, s);
+        float mx = (float)red.h[0];
+        DevBuf<float> y;
+        int64_t nr, nc;
+        normalize_pad2d(ds.proj, ds.nproj, ds.nrows, ds.ncols, mx, pfac, y, nr, nc, s);
+        geoms.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));
+        plan.adjoint(*geoms.back(), y.p, yT.p, true, s);
+        LAMINO_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<const Geom *> gptr;
+    for (auto &g : geoms) gptr.push_back(g.get());
+
+    // normal operator sum_gamma sysmat
+    std::unique_ptr<Toeplitz> T;
+    OpFn A;
+    if (prm.op_kind == OP_NUFFT) {
+        A = [&](const float *x, float *y, cudaStream_t st) { plan.normal(gptr, x, y, st); };
+    } else {
+        T.reset(new Toeplitz(gptr, od, prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : PREC_FP32, s));
+        A = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st); };
+    }
+
+    DevBuf<float> x(n);
+    LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));
+    if (method == 1) {
+        cgsolver(A, yT.p, x.p, od, prm.max_iters, prm.tol, s);
+    } else if (method == 2) {
+        split_bregman(A, yT.p, x.p, od, prm.lambda, prm.mu, prm.max_iters, prm.inner_iters, prm.tol, prm.xtol, s);
+    } else {
+        // per-gamma operators for the loss (sum over gamma of per-component sqrt terms)
+        std::vector<std::unique_ptr<Toeplitz>> Tg;
+        std::vector<OpFn> Ag;
+        for (const Geom *g : gptr) {
+            if (prm.op_kind == OP_NUFFT) {
+                Ag.push_back([&plan, g](const float *xx, float *yy, cudaStream_t st) { plan.normal({g}, xx, yy, st); });
+            } else {
+                Tg.emplace_back(new Toeplitz({g}, od, prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : PREC_FP32, s));
+                Toeplitz *tp = Tg.back().get();
+                Ag.push_back([tp](const float *xx, float *yy, cudaStream_t st) { tp->apply(xx, yy, st); });
+            }
+        }
+        red.zero(1, s);
+        vec_dot(yT.p, yT.p, n, red.d, s);
+        red.fetch(1, s);
+        const double yTy = red.h[0];
+        const float ng = (float)gptr.size();
+        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) {
+            A(xx, g, st);
+            k_axpy_scalar<<<grid_for(n, 256), 256, 0, st>>>(g, -ng, yT.p, n);
+            LAMINO_LAUNCH("k_axpy_scalar");
+            for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od, prm.sigma, prm.p, st);
+        };
+        DevBuf<float> Sx(n);
+        Reducer lr(8);
+        LossFn loss = [&](const float *xx, cudaStream_t st) {
+            double e = 0.0;
+            for (auto &Aq : Ag) {
+                Aq(xx, Sx.p, st);
+                lr.zero(6, st);
+                for (int i = 0; i < 3; ++i) {
+                    vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + i, st);
+                    vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 3 + i, st);
+                }
+                lr.fetch(6, st);
+                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[i] - 2.0 * lr.h[3 + i] + yTy);
+            }
+            return e;
+        };
+        nagopt(grad, loss, x.p, od, prm.max_iters, prm.mu, prm.tol, prm.xtol, prm.inner_iters, s);
+    }
+    crop3d3(x.p, od, recon, out3, s);
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace lamino

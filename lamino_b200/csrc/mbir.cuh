@@ -1,0 +1,46 @@
+// MBIR drivers (src/mbir_cg.cpp, src/mbir_sb.cpp, src/mbir3.cpp) on the GPU path.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "geometry.cuh"
+#include "nufft.cuh"
+#include "solvers.cuh"
+#include "toeplitz.cuh"
+
+namespace lamino {
+
+enum OpKind : int { OP_TOEPLITZ_FP32 = 0, OP_TOEPLITZ_FP16 = 1, OP_NUFFT = 2 };
+
+struct ReconParams {  // include/config.h:146-158 defaults
+    int max_iters = 50;
+    int inner_iters = 3;
+    float sigma = 1000.f, p = 1.2f, lambda = 0.1f, mu = 10.f, tol = 1e-5f, xtol = 1e-5f;
+    float pad_factor = 1.4142f;
+    int op_kind = OP_TOEPLITZ_FP32;
+    double eps = 1.2e-6;
+};
+
+struct Dataset {
+    const float *proj;  // device, (nproj, nrows, ncols)
+    int64_t nproj, nrows, ncols;
+    const float *angles;  // host
+    float gamma;
+};
+
+// Padded volume dims n + 2 floor(n (PAD-1) / 2) (src/mbir_sb.cpp:50-60).
+int64_t pad_dim(int64_t n, float factor_minus_one);
+
+// pad2d (include/padding.h:94-131) fused with the 1/max normalisation; returns new dims
+void normalize_pad2d(const float *proj, int64_t np, int64_t nr, int64_t nc, float inv_max, float factor,
+                     DevBuf<float> &out, int64_t &onr, int64_t &onc, cudaStream_t s);
+// crop3d (include/padding.h:207-232, symmetric), 3 components
+void crop3d3(const float *in, Dims3 from, Dims3 to, float *out, cudaStream_t s);
+
+// method 1 = CG, 2 = split Bregman, 3 = NAG + qGGMRF.  out3: recon dims, device.
+void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
+          cudaStream_t s);
+
+}  // namespace lamino

@@ -1,0 +1,568 @@
+// ES-kernel NUFFT for the laminography operator (sm_100a).
+//
+// Reference behaviour replaced: include/nufft.h:37-64 (FINUFFT 3-D type 1 with
+// iflag +1 and type 2 with iflag -1, n_modes = {ncols, nrows, nslices},
+// upsampfac 2, tol 1.2e-6 in float), src/projection.cpp:42-126 (forward /
+// adjoint) and src/gradient.cpp:34-89 (sysmat).
+//
+// Design: points are never stored or sorted.  Each thread regenerates its
+// point from the per-column / per-row / per-projection factors (geometry.cuh)
+// and consecutive threads walk a projection row, so a warp touches a compact
+// patch of the fine grid.  The fine grid is (nf1, nf2, nf3) complex64 with nf
+// the smallest even 2,3,5-smooth size >= 2n; the uniform FFTs on it use cuFFT.
+// Deconvolution, the pad into the fine grid and the crop out of it are fused
+// into the kernels on either side of cuFFT, and so are the fftshift2 /
+// ifftshift2 index maps and the per-projection beam-vector weighting.
+#include <cmath>
+#include <vector>
+
+#include "nufft.cuh"
+
+namespace lamino {
+
+int64_t next_smooth_even(int64_t n) {
+    if (n < 2) n = 2;
+    if (n % 2) ++n;
+    for (;; n += 2) {
+        int64_t m = n;
+        for (int p : {2, 3, 5})
+            while (m % p == 0) m /= p;
+        if (m == 1) return n;
+    }
+}
+
+// p(k) = (w/2) int_{-1}^{1} phi(t) cos(k pi w t / nf) dt by Gauss-Legendre
+// quadrature in double (nodes by Newton iteration on P_n).
+static std::vector<double> es_fourier(int64_t nf, int64_t N, int w, double beta) {
+    const int nq = 200;
+    std::vector<double> xs(nq), ws(nq);
+    for (int i = 0; i < nq; ++i) {
+        double x = std::cos(M_PI * (i + 0.75) / (nq + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = x;
+            for (int k = 2; k <= nq; ++k) {
+                double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            double dp = nq * (x * p1 - p0) / (x * x - 1.0);
+            double dx = p1 / dp;
+            x -= dx;
+            if (std::fabs(dx) < 1e-16) {
+                ws[i] = 2.0 / ((1.0 - x * x) * dp * dp);
+                break;
+            }
+            ws[i] = 2.0 / ((1.0 - x * x) * dp * dp);
+        }
+        xs[i] = x;
+    }
+    std::vector<double> p(N);
+    for (int64_t i = 0; i < N; ++i) {
+        double k = (double)(i - N / 2);
+        double s = 0.0;
+        for (int q = 0; q < nq; ++q) {
+            double phi = std::exp(beta * (std::sqrt(1.0 - xs[q] * xs[q]) - 1.0));
+            s += ws[q] * phi * std::cos(k * M_PI * w * xs[q] / (double)nf);
+        }
+        p[i] = 0.5 * w * s;
+    }
+    return p;
+}
+
+NufftPlan::NufftPlan(Dims3 d, double eps_) : vol(d), eps(eps_) {
+    if (d.n1 <= 0 || d.n2 <= 0 || d.n3 <= 0) throw Error(ERR_ARG, "volume dims must be positive");
+    w = es_width(eps);
+    if (w < 4 || w > 8) throw Error(ERR_ARG, "NUFFT tolerance must give kernel width 4..8 (eps 1e-3..1e-7)");
+    beta = (float)(2.30 * w);
+    nf1 = next_smooth_even(std::max<int64_t>(2 * d.n1, 2 * w));
+    nf2 = next_smooth_even(std::max<int64_t>(2 * d.n2, 2 * w));
+    nf3 = next_smooth_even(std::max<int64_t>(2 * d.n3, 2 * w));
+    if (nf() > (int64_t)INT32_MAX) throw Error(ERR_ARG, "fine grid too large");
+    auto up = [&](DevBuf<float> &buf, int64_t nf_, int64_t N) {
+        auto p = es_fourier(nf_, N, w, beta);
+        std::vector<float> ip(N);
+        for (int64_t i = 0; i < N; ++i) ip[i] = (float)(1.0 / p[i]);
+        buf.alloc(N);
+        LAMINO_CUDA(cudaMemcpy(buf.p, ip.data(), N * 4, cudaMemcpyHostToDevice));
+    };
+    up(ip1, nf1, d.n1);
+    up(ip2, nf2, d.n2);
+    up(ip3, nf3, d.n3);
+    gin.alloc(3 * nf());
+    gwork.alloc(3 * nf());
+    LAMINO_CUDA(cudaMemset(gin.p, 0, gin.bytes()));
+    int n[3] = {(int)nf1, (int)nf2, (int)nf3};
+    LAMINO_CUFFT(cufftPlanMany(&fft3.h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 1));
+    fft3.valid = true;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+struct Fine {
+    int nf1, nf2, nf3;
+    double s1, s2, s3;  // nf / (2 pi)
+    float beta;
+};
+
+template <int W>
+__device__ __forceinline__ int es_taps(float xc, int nf, double s, float beta, float *wt) {
+    double u = (double)xc * s;
+    double l0 = ceil(u - 0.5 * W);
+    float d0 = (float)(l0 - u);  // in [-W/2, -W/2 + 1)
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+        float a = (d0 + (float)t) * (2.0f / W);
+        float q = 1.0f - a * a;
+        wt[t] = q > 0.f ? expf(beta * (sqrtf(q) - 1.0f)) : 0.f;
+    }
+    int64_t l = (int64_t)l0;
+    l %= nf;
+    if (l < 0) l += nf;
+    return (int)l;
+}
+
+// deconvolve + place modes into the (zero) fine grid; real volume input
+__global__ void k_pad_real(const float *__restrict__ x, int n1, int n2, int n3,
+                           float2 *__restrict__ g, Fine F, const float *__restrict__ ip1,
+                           const float *__restrict__ ip2, const float *__restrict__ ip3) {
+    const int comp = blockIdx.y;
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    const int64_t NF = (int64_t)F.nf1 * F.nf2 * F.nf3;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i3 = (int)(idx % n3);
+        int64_t r = idx / n3;
+        int i2 = (int)(r % n2);
+        int i1 = (int)(r / n2);
+        int l1 = i1 - n1 / 2; if (l1 < 0) l1 += F.nf1;
+        int l2 = i2 - n2 / 2; if (l2 < 0) l2 += F.nf2;
+        int l3 = i3 - n3 / 2; if (l3 < 0) l3 += F.nf3;
+        float v = x[comp * V + idx] * (__ldg(ip1 + i1) * __ldg(ip2 + i2) * __ldg(ip3 + i3));
+        g[comp * NF + ((int64_t)l1 * F.nf2 + l2) * F.nf3 + l3] = make_float2(v, 0.f);
+    }
+}
+
+__global__ void k_pad_complex(const float2 *__restrict__ f, int n1, int n2, int n3,
+                              float2 *__restrict__ g, Fine F, const float *__restrict__ ip1,
+                              const float *__restrict__ ip2, const float *__restrict__ ip3) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i3 = (int)(idx % n3);
+        int64_t r = idx / n3;
+        int i2 = (int)(r % n2);
+        int i1 = (int)(r / n2);
+        int l1 = i1 - n1 / 2; if (l1 < 0) l1 += F.nf1;
+        int l2 = i2 - n2 / 2; if (l2 < 0) l2 += F.nf2;
+        int l3 = i3 - n3 / 2; if (l3 < 0) l3 += F.nf3;
+        float c = __ldg(ip1 + i1) * __ldg(ip2 + i2) * __ldg(ip3 + i3);
+        float2 v = f[idx];
+        g[((int64_t)l1 * F.nf2 + l2) * F.nf3 + l3] = make_float2(v.x * c, v.y * c);
+    }
+}
+
+// fine grid -> modes: y = (acc ? y : 0) + Re(G[k mod nf]) / p(k) * scale
+__global__ void k_extract_real(const float2 *__restrict__ g, int n1, int n2, int n3,
+                               float *__restrict__ y, Fine F, const float *__restrict__ ip1,
+                               const float *__restrict__ ip2, const float *__restrict__ ip3,
+                               float scale, int accumulate) {
+    const int comp = blockIdx.y;
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    const int64_t NF = (int64_t)F.nf1 * F.nf2 * F.nf3;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i3 = (int)(idx % n3);
+        int64_t r = idx / n3;
+        int i2 = (int)(r % n2);
+        int i1 = (int)(r / n2);
+        int l1 = i1 - n1 / 2; if (l1 < 0) l1 += F.nf1;
+        int l2 = i2 - n2 / 2; if (l2 < 0) l2 += F.nf2;
+        int l3 = i3 - n3 / 2; if (l3 < 0) l3 += F.nf3;
+        float c = __ldg(ip1 + i1) * __ldg(ip2 + i2) * __ldg(ip3 + i3) * scale;
+        float v = g[comp * NF + ((int64_t)l1 * F.nf2 + l2) * F.nf3 + l3].x * c;
+        if (accumulate) v += y[comp * V + idx];
+        y[comp * V + idx] = v;
+    }
+}
+
+__global__ void k_extract_complex(const float2 *__restrict__ g, int n1, int n2, int n3,
+                                  float2 *__restrict__ f, Fine F, const float *__restrict__ ip1,
+                                  const float *__restrict__ ip2, const float *__restrict__ ip3) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i3 = (int)(idx % n3);
+        int64_t r = idx / n3;
+        int i2 = (int)(r % n2);
+        int i1 = (int)(r / n2);
+        int l1 = i1 - n1 / 2; if (l1 < 0) l1 += F.nf1;
+        int l2 = i2 - n2 / 2; if (l2 < 0) l2 += F.nf2;
+        int l3 = i3 - n3 / 2; if (l3 < 0) l3 += F.nf3;
+        float c = __ldg(ip1 + i1) * __ldg(ip2 + i2) * __ldg(ip3 + i3);
+        float2 v = g[((int64_t)l1 * F.nf2 + l2) * F.nf3 + l3];
+        f[idx] = make_float2(v.x * c, v.y * c);
+    }
+}
+
+// interpolate NC fine grids at one point
+template <int W, int NC>
+__device__ __forceinline__ void interp_point(const float2 *__restrict__ G, int64_t NF, const Fine &F,
+                                             float x, float y, float z, float2 *out) {
+    float w1[W], w2[W], w3[W];
+    int b3 = es_taps<W>(x, F.nf3, F.s3, F.beta, w3);
+    int b2 = es_taps<W>(y, F.nf2, F.s2, F.beta, w2);
+    int b1 = es_taps<W>(z, F.nf1, F.s1, F.beta, w1);
+    int i3s[W];
+#pragma unroll
+    for (int t = 0; t < W; ++t) { int v = b3 + t; i3s[t] = v >= F.nf3 ? v - F.nf3 : v; }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int t1 = 0; t1 < W; ++t1) {
+        int i1 = b1 + t1; if (i1 >= F.nf1) i1 -= F.nf1;
+#pragma unroll
+        for (int t2 = 0; t2 < W; ++t2) {
+            int i2 = b2 + t2; if (i2 >= F.nf2) i2 -= F.nf2;
+            const int64_t rowo = ((int64_t)i1 * F.nf2 + i2) * F.nf3;
+            float k12 = w1[t1] * w2[t2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const float2 *row = G + c * NF + rowo;
+                float rr = 0.f, ri = 0.f;
+#pragma unroll
+                for (int t3 = 0; t3 < W; ++t3) {
+                    float2 v = __ldg(row + i3s[t3]);
+                    rr = fmaf(w3[t3], v.x, rr);
+                    ri = fmaf(w3[t3], v.y, ri);
+                }
+                out[c].x = fmaf(k12, rr, out[c].x);
+                out[c].y = fmaf(k12, ri, out[c].y);
+            }
+        }
+    }
+}
+
+// spread NC strengths at one point into NC fine grids (float2 vector atomics)
+template <int W, int NC>
+__device__ __forceinline__ void spread_point(float2 *__restrict__ H, int64_t NF, const Fine &F,
+                                             float x, float y, float z, const float2 *str) {
+    float w1[W], w2[W], w3[W];
+    int b3 = es_taps<W>(x, F.nf3, F.s3, F.beta, w3);
+    int b2 = es_taps<W>(y, F.nf2, F.s2, F.beta, w2);
+    int b1 = es_taps<W>(z, F.nf1, F.s1, F.beta, w1);
+    int i3s[W];
+#pragma unroll
+    for (int t = 0; t < W; ++t) { int v = b3 + t; i3s[t] = v >= F.nf3 ? v - F.nf3 : v; }
+#pragma unroll 1
+    for (int t1 = 0; t1 < W; ++t1) {
+        int i1 = b1 + t1; if (i1 >= F.nf1) i1 -= F.nf1;
+#pragma unroll
+        for (int t2 = 0; t2 < W; ++t2) {
+            int i2 = b2 + t2; if (i2 >= F.nf2) i2 -= F.nf2;
+            const int64_t rowo = ((int64_t)i1 * F.nf2 + i2) * F.nf3;
+            float k12 = w1[t1] * w2[t2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                float2 *row = H + c * NF + rowo;
+                float sr = k12 * str[c].x, si = k12 * str[c].y;
+#pragma unroll
+                for (int t3 = 0; t3 < W; ++t3)
+                    atomicAdd(row + i3s[t3], make_float2(w3[t3] * sr, w3[t3] * si));
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void decode_pid(uint32_t pid, const GeomView &g, int &p, int &j, int &k) {
+    uint32_t plane = (uint32_t)g.nrows * (uint32_t)g.ncols;
+    p = (int)(pid / plane);
+    uint32_t r = pid - (uint32_t)p * plane;
+    j = (int)(r / (uint32_t)g.ncols);
+    k = (int)(r - (uint32_t)j * (uint32_t)g.ncols);
+}
+
+// forward: P[fftshift2 position] = sum_i coeff_i(th) * N2(m_i)(point)
+template <int W>
+__global__ void __launch_bounds__(256) k_interp_forward(GeomView g, const float2 *__restrict__ G,
+                                                        int64_t NF, Fine F, float2 *__restrict__ P) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    const int d1 = g.nrows / 2, d2 = g.ncols / 2;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float x, y, z;
+        point_xyz(g, p, j, k, x, y, z);
+        float2 v[3];
+        interp_point<W, 3>(G, NF, F, x, y, z, v);
+        float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
+        float2 o = make_float2(c0 * v[0].x + c1 * v[1].x + c2 * v[2].x, c0 * v[0].y + c1 * v[1].y + c2 * v[2].y);
+        int js = j - d1; if (js < 0) js += g.nrows;
+        int ks = k - d2; if (ks < 0) ks += g.ncols;
+        P[((int64_t)p * g.nrows + js) * g.ncols + ks] = o;
+    }
+}
+
+// raw type 2 (one component), output in point order
+template <int W>
+__global__ void __launch_bounds__(256) k_interp_raw(GeomView g, const float2 *__restrict__ G, int64_t NF,
+                                                    Fine F, float2 *__restrict__ c) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float x, y, z;
+        point_xyz(g, p, j, k, x, y, z);
+        float2 v[1];
+        interp_point<W, 1>(G, NF, F, x, y, z, v);
+        c[pid] = v[0];
+    }
+}
+
+// adjoint: spread coeff_i(th) * c into grid i, c read through ifftshift2
+template <int W>
+__global__ void __launch_bounds__(256) k_spread_adjoint(GeomView g, const float2 *__restrict__ Pf,
+                                                        float2 *__restrict__ H, int64_t NF, Fine F) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    const int e1 = (g.nrows + 1) / 2, e2 = (g.ncols + 1) / 2;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        int js = j + e1; if (js >= g.nrows) js -= g.nrows;
+        int ks = k + e2; if (ks >= g.ncols) ks -= g.ncols;
+        float2 c = Pf[((int64_t)p * g.nrows + js) * g.ncols + ks];
+        float x, y, z;
+        point_xyz(g, p, j, k, x, y, z);
+        float2 s[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            float cq = __ldg(g.coeff + q * g.nproj + p);
+            s[q] = make_float2(cq * c.x, cq * c.y);
+        }
+        spread_point<W, 3>(H, NF, F, x, y, z, s);
+    }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_spread_raw(GeomView g, const float2 *__restrict__ c,
+                                                    float2 *__restrict__ H, int64_t NF, Fine F) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float x, y, z;
+        point_xyz(g, p, j, k, x, y, z);
+        float2 s[1] = {c[pid]};
+        spread_point<W, 1>(H, NF, F, x, y, z, s);
+    }
+}
+
+// sysmat points: v_k = N2(x_k)(pt), s = sum_k c_k v_k, spread c_i s / (nrows ncols) into H_i
+template <int W>
+__global__ void __launch_bounds__(256) k_sysmat_points(GeomView g, const float2 *__restrict__ G,
+                                                       float2 *__restrict__ H, int64_t NF, Fine F,
+                                                       float inv_scale) {
+    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float x, y, z;
+        point_xyz(g, p, j, k, x, y, z);
+        float2 v[3];
+        interp_point<W, 3>(G, NF, F, x, y, z, v);
+        float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
+        float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
+        float si = (c0 * v[0].y + c1 * v[1].y + c2 * v[2].y) * inv_scale;
+        float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si), make_float2(c2 * sr, c2 * si)};
+        spread_point<W, 3>(H, NF, F, x, y, z, s);
+    }
+}
+
+// projection space: proj = Re(P[ifftshift2 position]) * scale
+__global__ void k_proj_post(const float2 *__restrict__ P, int np, int nr, int nc, float scale,
+                            float *__restrict__ proj) {
+    const int64_t M = (int64_t)np * nr * nc;
+    const int e1 = (nr + 1) / 2, e2 = (nc + 1) / 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        int k = (int)(i % nc);
+        int64_t r = i / nc;
+        int j = (int)(r % nr);
+        int64_t p = r / nr;
+        int js = j + e1; if (js >= nr) js -= nr;
+        int ks = k + e2; if (ks >= nc) ks -= nc;
+        proj[i] = P[(p * nr + js) * nc + ks].x * scale;
+    }
+}
+
+// projection space: P = fftshift2(proj) as complex
+__global__ void k_proj_pre(const float *__restrict__ proj, int np, int nr, int nc, float2 *__restrict__ P) {
+    const int64_t M = (int64_t)np * nr * nc;
+    const int d1 = nr / 2, d2 = nc / 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        int k = (int)(i % nc);
+        int64_t r = i / nc;
+        int j = (int)(r % nr);
+        int64_t p = r / nr;
+        int js = j + d1; if (js >= nr) js -= nr;
+        int ks = k + d2; if (ks >= nc) ks -= nc;
+        P[i] = make_float2(proj[(p * nr + js) * nc + ks], 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+static Fine fine_of(const NufftPlan &pl) {
+    Fine F;
+    F.nf1 = (int)pl.nf1; F.nf2 = (int)pl.nf2; F.nf3 = (int)pl.nf3;
+    F.s1 = (double)pl.nf1 / (2 * M_PI);
+    F.s2 = (double)pl.nf2 / (2 * M_PI);
+    F.s3 = (double)pl.nf3 / (2 * M_PI);
+    F.beta = pl.beta;
+    return F;
+}
+
+#define LAMINO_W_DISPATCH(w, KERNEL, GRID, BLOCK, STREAM, ...)                          \
+    switch (w) {                                                                         \
+        case 4: KERNEL<4><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
+        case 5: KERNEL<5><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
+        case 6: KERNEL<6><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
+        case 7: KERNEL<7><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
+        case 8: KERNEL<8><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
+        default: throw Error(ERR_ARG, "unsupported kernel width");                       \
+    }
+
+void NufftPlan::pad_real(const float *x3, int ncomp, cudaStream_t s) {
+    Fine F = fine_of(*this);
+    dim3 grid(grid_for(vol.size(), 256), ncomp);
+    k_pad_real<<<grid, 256, 0, s>>>(x3, (int)vol.n1, (int)vol.n2, (int)vol.n3, gin.p, F, ip1.p, ip2.p, ip3.p);
+    LAMINO_LAUNCH("k_pad_real");
+}
+
+void NufftPlan::pad_complex(const float2 *f, cudaStream_t s) {
+    Fine F = fine_of(*this);
+    k_pad_complex<<<grid_for(vol.size(), 256), 256, 0, s>>>(f, (int)vol.n1, (int)vol.n2, (int)vol.n3, gin.p, F,
+                                                              ip1.p, ip2.p, ip3.p);
+    LAMINO_LAUNCH("k_pad_complex");
+}
+
+// sign -1: gin -> gwork (type 2); sign +1: gwork in place (type 1)
+void NufftPlan::fft_fine(int sign, int ncomp, cudaStream_t s) {
+    LAMINO_CUFFT(cufftSetStream(fft3.h, s));
+    for (int c = 0; c < ncomp; ++c) {
+        if (sign < 0)
+            LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gin.p + c * nf()),
+                                      (cufftComplex *)(gwork.p + c * nf()), CUFFT_FORWARD));
+        else
+            LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gwork.p + c * nf()),
+                                      (cufftComplex *)(gwork.p + c * nf()), CUFFT_INVERSE));
+    }
+}
+
+void NufftPlan::extract_real(float *y3, int ncomp, float scale, bool accumulate, cudaStream_t s) {
+    Fine F = fine_of(*this);
+    dim3 grid(grid_for(vol.size(), 256), ncomp);
+    k_extract_real<<<grid, 256, 0, s>>>(gwork.p, (int)vol.n1, (int)vol.n2, (int)vol.n3, y3, F, ip1.p, ip2.p,
+                                        ip3.p, scale, accumulate ? 1 : 0);
+    LAMINO_LAUNCH("k_extract_real");
+}
+
+void NufftPlan::ensure_proj(const Geom &g, cudaStream_t s) {
+    (void)s;
+    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    if ((int64_t)pbuf.n < g.npts()) pbuf.alloc(g.npts());
+    if (f2_np != g.nproj || f2_nr != g.nrows || f2_nc != g.ncols) {
+        if (fft2.valid) { cufftDestroy(fft2.h); fft2.valid = false; }
+        int n[2] = {(int)g.nrows, (int)g.ncols};
+        LAMINO_CUFFT(cufftPlanMany(&fft2.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)g.nproj));
+        fft2.valid = true;
+        f2_np = g.nproj; f2_nr = g.nrows; f2_nc = g.ncols;
+    }
+}
+
+void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_t s) {
+    ensure_proj(g, s);
+    pad_real(m3, 3, s);
+    fft_fine(-1, 3, s);
+    Fine F = fine_of(*this);
+    GeomView gv = g.view();
+    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    LAMINO_W_DISPATCH(w, k_interp_forward, grid, 256, s, gv, gwork.p, nf(), F, pbuf.p);
+    LAMINO_LAUNCH("k_interp_forward");
+    LAMINO_CUFFT(cufftSetStream(fft2.h, s));
+    LAMINO_CUFFT(cufftExecC2C(fft2.h, (cufftComplex *)pbuf.p, (cufftComplex *)pbuf.p, CUFFT_INVERSE));
+    float scale = 1.0f / (float)(g.nrows * g.ncols);
+    k_proj_post<<<grid_for(g.npts(), 256), 256, 0, s>>>(pbuf.p, (int)g.nproj, (int)g.nrows, (int)g.ncols, scale, proj);
+    LAMINO_LAUNCH("k_proj_post");
+}
+
+void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumulate, cudaStream_t s) {
+    ensure_proj(g, s);
+    k_proj_pre<<<grid_for(g.npts(), 256), 256, 0, s>>>(proj, (int)g.nproj, (int)g.nrows, (int)g.ncols, pbuf.p);
+    LAMINO_LAUNCH("k_proj_pre");
+    LAMINO_CUFFT(cufftSetStream(fft2.h, s));
+    LAMINO_CUFFT(cufftExecC2C(fft2.h, (cufftComplex *)pbuf.p, (cufftComplex *)pbuf.p, CUFFT_FORWARD));
+    LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, gwork.bytes(), s));
+    Fine F = fine_of(*this);
+    GeomView gv = g.view();
+    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    LAMINO_W_DISPATCH(w, k_spread_adjoint, grid, 256, s, gv, pbuf.p, gwork.p, nf(), F);
+    LAMINO_LAUNCH("k_spread_adjoint");
+    fft_fine(+1, 3, s);
+    extract_real(m3, 3, 1.0f / (float)(g.nrows * g.ncols), accumulate, s);
+}
+
+void NufftPlan::normal(const std::vector<const Geom *> &gs, const float *x3, float *y3, cudaStream_t s) {
+    if (gs.empty()) throw Error(ERR_ARG, "normal operator needs at least one geometry");
+    pad_real(x3, 3, s);
+    // forward fine-grid spectra go to gwork; accumulate the spread into gin's
+    // companion: reuse gin after its FFT (re-zeroed below for the next pad).
+    fft_fine(-1, 3, s);
+    // spread target: gin (zeroed) -- gin must be re-zeroed before the next pad_real
+    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
+    Fine F = fine_of(*this);
+    for (const Geom *g : gs) {
+        if (g->npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+        GeomView gv = g->view();
+        unsigned grid = grid_for(g->npts(), 256, 148LL * 16 * 8);
+        float inv_scale = 1.0f / (float)(g->nrows * g->ncols);
+        LAMINO_W_DISPATCH(w, k_sysmat_points, grid, 256, s, gv, gwork.p, gin.p, nf(), F, inv_scale);
+        LAMINO_LAUNCH("k_sysmat_points");
+    }
+    // inverse FFT of the accumulated spread (in gin), then extract
+    LAMINO_CUFFT(cufftSetStream(fft3.h, s));
+    for (int c = 0; c < 3; ++c)
+        LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gin.p + c * nf()),
+                                  (cufftComplex *)(gwork.p + c * nf()), CUFFT_INVERSE));
+    extract_real(y3, 3, 1.0f, false, s);
+    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
+}
+
+void NufftPlan::type2(const Geom &g, const float2 *modes, float2 *c, cudaStream_t s) {
+    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    pad_complex(modes, s);
+    fft_fine(-1, 1, s);
+    Fine F = fine_of(*this);
+    GeomView gv = g.view();
+    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    LAMINO_W_DISPATCH(w, k_interp_raw, grid, 256, s, gv, gwork.p, nf(), F, c);
+    LAMINO_LAUNCH("k_interp_raw");
+}
+
+void NufftPlan::type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_t s) {
+    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, nf() * sizeof(float2), s));
+    Fine F = fine_of(*this);
+    GeomView gv = g.view();
+    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    LAMINO_W_DISPATCH(w, k_spread_raw, grid, 256, s, gv, c, gwork.p, nf(), F);
+    LAMINO_LAUNCH("k_spread_raw");
+    fft_fine(+1, 1, s);
+    k_extract_complex<<<grid_for(vol.size(), 256), 256, 0, s>>>(gwork.p, (int)vol.n1, (int)vol.n2, (int)vol.n3,
+                                                                  modes, F, ip1.p, ip2.p, ip3.p);
+    LAMINO_LAUNCH("k_extract_complex");
+}
+
+}  // namespace lamino

@@ -1,0 +1,57 @@
+// ES-kernel 3-D NUFFT on the laminography planes (type 1 / type 2), plus the
+// projection-space stages of the forward and adjoint operators.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "geometry.cuh"
+
+namespace lamino {
+
+// Width / shape of the exponential-of-semicircle kernel for a tolerance at
+// oversampling 2 (Barnett, Magland, af Klinteberg, SIAM J. Sci. Comput. 2019).
+inline int es_width(double eps) {
+    int w = (int)std::ceil(std::log10(10.0 / eps));
+    return w < 2 ? 2 : w;
+}
+int64_t next_smooth_even(int64_t n);
+
+struct NufftPlan {
+    Dims3 vol;                // recon volume (n1, n2, n3), n3 fastest
+    int64_t nf1, nf2, nf3;    // fine grid paired with n1 (z), n2 (y), n3 (x)
+    int w = 7;
+    float beta = 16.1f;
+    double eps = 1.2e-6;
+    DevBuf<float> ip1, ip2, ip3;   // 1 / p(k) per mode index along each dim
+    DevBuf<float2> gin;            // 3 fine grids: deconvolved modes (zero elsewhere)
+    DevBuf<float2> gwork;          // 3 fine grids: FFT outputs / spread accumulators
+    FftPlan fft3;                  // batched 3 x C2C 3-D on the fine grid
+    // projection-space workspace (largest geometry seen), with its 2-D plan
+    DevBuf<float2> pbuf;
+    FftPlan fft2;
+    int64_t f2_np = -1, f2_nr = -1, f2_nc = -1;
+
+    NufftPlan(Dims3 d, double eps);
+    int64_t nf() const { return nf1 * nf2 * nf3; }
+    void ensure_proj(const Geom &g, cudaStream_t s);
+
+    // --- operators (device pointers; volumes are 3 contiguous components) ---
+    // forward projection (src/projection.cpp:42-77)
+    void forward(const Geom &g, const float *m3, float *proj, cudaStream_t s);
+    // adjoint (src/projection.cpp:90-126); accumulate adds into m3
+    void adjoint(const Geom &g, const float *proj, float *m3, bool accumulate, cudaStream_t s);
+    // sum over geometries of sysmat (src/gradient.cpp:34-89), NUFFT form
+    void normal(const std::vector<const Geom *> &gs, const float *x3, float *y3, cudaStream_t s);
+    // raw transforms on one geometry (FINUFFT-level boundary, complex data)
+    void type2(const Geom &g, const float2 *modes, float2 *c, cudaStream_t s);
+    void type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_t s);
+
+    // internals
+    void pad_real(const float *x3, int ncomp, cudaStream_t s);
+    void pad_complex(const float2 *f, cudaStream_t s);
+    void fft_fine(int sign, int ncomp, cudaStream_t s);
+    void extract_real(float *y3, int ncomp, float scale, bool accumulate, cudaStream_t s);
+};
+
+}  // namespace lamino

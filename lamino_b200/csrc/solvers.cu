@@ -1,0 +1,546 @@
+// Solver kernels and loops for the laminography reconstructions (sm_100a).
+//
+// Arithmetic follows the reference's float expressions element by element
+// (including where it promotes to double); reductions use FP64 accumulation
+// with warp-shuffle trees instead of the reference's serial float sums.
+#include <cmath>
+#include <vector>
+
+#include "solvers.cuh"
+
+namespace lamino {
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+
+Reducer::Reducer(int n) : cap(n) {
+    LAMINO_CUDA(cudaMalloc((void **)&d, sizeof(double) * n));
+    LAMINO_CUDA(cudaMallocHost((void **)&h, sizeof(double) * n));
+}
+Reducer::~Reducer() {
+    if (d) cudaFree(d);
+    if (h) cudaFreeHost(h);
+}
+void Reducer::zero(int n, cudaStream_t s) { LAMINO_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, s)); }
+void Reducer::fetch(int n, cudaStream_t s) {
+    LAMINO_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double ws[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) ws[wid] = v;
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? ws[threadIdx.x] : 0.0;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+__global__ void k_dot(const float *__restrict__ x, const float *__restrict__ y, int64_t n, double *out) {
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += (double)x[i] * (double)y[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+__global__ void k_sqdist3(const float *__restrict__ x, const float *__restrict__ y, int64_t V, double *out3) {
+    const int c = blockIdx.y;
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = y ? (x[c * V + i] - y[c * V + i]) : x[c * V + i];
+        s += (double)v * (double)v;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) atomicAdd(out3 + c, s);
+}
+
+__device__ __forceinline__ int float_key(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+
+__global__ void k_max(const float *__restrict__ x, int64_t n, int *out) {
+    int m = INT_MIN;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, float_key(x[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void k_key_to_double(const int *key, double *out) {
+    int k = *key;
+    int i = k >= 0 ? k : k ^ 0x7fffffff;
+    *out = (double)__int_as_float(i);
+}
+
+void vec_dot(const float *x, const float *y, int64_t n, double *out, cudaStream_t s) {
+    k_dot<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(x, y, n, out);
+    LAMINO_LAUNCH("k_dot");
+}
+void vec_sqdist3(const float *x, const float *y, int64_t V, double *out3, cudaStream_t s) {
+    dim3 g(grid_for(V, 256, 148 * 4), 3);
+    k_sqdist3<<<g, 256, 0, s>>>(x, y, V, out3);
+    LAMINO_LAUNCH("k_sqdist3");
+}
+void vec_max(const float *x, int64_t n, double *out, cudaStream_t s) {
+    static_assert(sizeof(double) >= sizeof(int), "slot size");
+    int *key = reinterpret_cast<int *>(out);  // use the slot's storage for the int key
+    int init = INT_MIN;
+    LAMINO_CUDA(cudaMemcpyAsync(key, &init, sizeof(int), cudaMemcpyHostToDevice, s));
+    k_max<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(x, n, key);
+    LAMINO_LAUNCH("k_max");
+    k_key_to_double<<<1, 1, 0, s>>>(key, out);
+    LAMINO_LAUNCH("k_key_to_double");
+    LAMINO_CUDA(cudaStreamSynchronize(s));  // `init` lives on this stack frame
+}
+
+__global__ void k_lin2(float *__restrict__ out, float a, const float *__restrict__ x, float b,
+                       const float *__restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a * x[i] + (y ? b * y[i] : 0.f);
+}
+void vec_lin2(float *out, float a, const float *x, float b, const float *y, int64_t n, cudaStream_t s) {
+    k_lin2<<<grid_for(n, 256), 256, 0, s>>>(out, a, x, b, y, n);
+    LAMINO_LAUNCH("k_lin2");
+}
+void vec_scale(float *out, float a, const float *x, int64_t n, cudaStream_t s) { vec_lin2(out, a, x, 0.f, nullptr, n, s); }
+
+// ---------------------------------------------------------------------------
+// qGGMRF (src/qggmrf.cpp:25-95)
+// ---------------------------------------------------------------------------
+
+__constant__ float c_qggmrf_w[27] = {0.0302f, 0.037f, 0.0302f, 0.037f, 0.0523f, 0.037f, 0.0302f, 0.037f, 0.0302f,
+                                     0.037f,  0.0523f, 0.037f, 0.0532f, 0.f,     0.0523f, 0.037f, 0.0523f, 0.037f,
+                                     0.0302f, 0.037f, 0.0302f, 0.037f, 0.0523f, 0.037f, 0.0302f, 0.037f, 0.0302f};
+
+// rho'(delta) with q = 2, C = 0.001, evaluated with the reference's float/double mix
+__device__ __forceinline__ float d_potential(float delta, float sigma_q, float sigma_qp, float p) {
+    const double Q = 2.0, Cd = 0.001;
+    const float C = (float)Cd;
+    float ad = fabsf(delta);
+    float t1 = (float)(pow((double)ad, Q - (double)p) / (double)sigma_qp);
+    float t3 = C + t1;
+    if (ad > 0.f) {
+        float a = delta / (t3 * sigma_q);
+        return (float)((double)a * (Q - ((Q - (double)p) * (double)t1) / (double)t3));
+    }
+    return (float)(Q / ((double)sigma_q * Cd));
+}
+
+__global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2, int n3, float sigma_q,
+                         float sigma_qp, float p) {
+    const int64_t ni = (int64_t)(n1 - 2) * (n2 - 2) * (n3 - 2);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ni; t += (int64_t)gridDim.x * blockDim.x) {
+        int k = (int)(t % (n3 - 2)) + 1;
+        int64_t r = t / (n3 - 2);
+        int j = (int)(r % (n2 - 2)) + 1;
+        int i = (int)(r / (n2 - 2)) + 1;
+        int64_t c = ((int64_t)i * n2 + j) * n3 + k;
+        float u = x[c];
+        float sum = 0.f;
+#pragma unroll
+        for (int dx = -1; dx < 2; ++dx)
+#pragma unroll
+            for (int dy = -1; dy < 2; ++dy)
+#pragma unroll
+                for (int dz = -1; dz < 2; ++dz) {
+                    if (dx == 0 && dy == 0 && dz == 0) continue;
+                    float v = x[c + ((int64_t)dx * n2 + dy) * n3 + dz];
+                    float w = c_qggmrf_w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
+                    sum += w * d_potential(v - u, sigma_q, sigma_qp, p);
+                }
+        g[c] += sum;
+    }
+}
+
+void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStream_t s) {
+    if (d.n1 < 3 || d.n2 < 3 || d.n3 < 3) return;  // no interior voxels
+    float sigma_q = std::pow(sigma, 2.0f);
+    float sigma_qp = std::pow(sigma, 2.0f - p);
+    int64_t ni = (d.n1 - 2) * (d.n2 - 2) * (d.n3 - 2);
+    k_qggmrf<<<grid_for(ni, 256), 256, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, sigma_q, sigma_qp, p);
+    LAMINO_LAUNCH("k_qggmrf");
+}
+
+// ---------------------------------------------------------------------------
+// finite differences (src/finitediff.cpp:8-71, include/bregman.h:34-36)
+// ---------------------------------------------------------------------------
+
+struct Idx3 {
+    int i, j, k;
+};
+__device__ __forceinline__ Idx3 unravel(int64_t idx, int n2, int n3) {
+    Idx3 r;
+    r.k = (int)(idx % n3);
+    int64_t q = idx / n3;
+    r.j = (int)(q % n2);
+    r.i = (int)(q / n2);
+    return r;
+}
+__device__ __forceinline__ bool interior(int i, int j, int k, int n1, int n2, int n3) {
+    return i >= 1 && i < n1 - 1 && j >= 1 && j < n2 - 1 && k >= 1 && k < n3 - 1;
+}
+
+// grad along dim `dim` at (i,j,k): (u[+] - u[-]) / 2.0 on interior, else 0 (float result)
+__device__ __forceinline__ float gdir(const float *__restrict__ u, int i, int j, int k, int n1, int n2, int n3,
+                                      int dim) {
+    if (!interior(i, j, k, n1, n2, n3)) return 0.f;
+    int64_t c = ((int64_t)i * n2 + j) * n3 + k;
+    int64_t st = dim == 0 ? (int64_t)n2 * n3 : (dim == 1 ? n3 : 1);
+    return (float)((double)(u[c + st] - u[c - st]) / 2.0);
+}
+
+__global__ void k_grad_u(const float *__restrict__ u, int n1, int n2, int n3, float *__restrict__ out3) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
+        Idx3 p = unravel(t, n2, n3);
+        for (int dim = 0; dim < 3; ++dim) out3[dim * V + t] = gdir(u, p.i, p.j, p.k, n1, n2, n3, dim);
+    }
+}
+
+// negative divergence of a 3-field given by an accessor
+template <class F>
+__device__ __forceinline__ float neg_div(const F &f, int i, int j, int k, int n1, int n2, int n3) {
+    if (!interior(i, j, k, n1, n2, n3)) return 0.f;
+    double a = -(double)(f(0, i + 1, j, k) - f(0, i - 1, j, k)) / 2.0;
+    double b = (double)(f(1, i, j + 1, k) - f(1, i, j - 1, k)) / 2.0;
+    double c = (double)(f(2, i, j, k + 1) - f(2, i, j, k - 1)) / 2.0;
+    return (float)(a - b - c);
+}
+
+__global__ void k_divergence(const float *__restrict__ du3, int n1, int n2, int n3, float *__restrict__ out) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    auto f = [&](int dim, int i, int j, int k) { return du3[dim * V + ((int64_t)i * n2 + j) * n3 + k]; };
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
+        Idx3 p = unravel(t, n2, n3);
+        out[t] = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
+    }
+}
+
+// y += mu * divergence(grad_u(u)) for NC contiguous components
+__global__ void k_laplacian_axpy(float *__restrict__ y, float mu, const float *__restrict__ u, int n1, int n2,
+                                 int n3) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    const int comp = blockIdx.y;
+    const float *uc = u + comp * V;
+    auto f = [&](int dim, int i, int j, int k) { return gdir(uc, i, j, k, n1, n2, n3, dim); };
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
+        Idx3 p = unravel(t, n2, n3);
+        float l = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
+        y[comp * V + t] += l * mu;
+    }
+}
+
+__global__ void k_sb_rhs(const float *__restrict__ yT, const float *__restrict__ d9, const float *__restrict__ b9,
+                         float mu, int n1, int n2, int n3, float *__restrict__ rhs) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    const int comp = blockIdx.y;
+    const float *dc = d9 + 3 * comp * V, *bc = b9 + 3 * comp * V;
+    auto f = [&](int dim, int i, int j, int k) {
+        int64_t c = dim * V + ((int64_t)i * n2 + j) * n3 + k;
+        return dc[c] - bc[c];
+    };
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
+        Idx3 p = unravel(t, n2, n3);
+        float dv = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
+        rhs[comp * V + t] = yT[comp * V + t] + dv * mu;
+    }
+}
+
+__global__ void k_sb_shrink(const float *__restrict__ x3, float *__restrict__ d9, float *__restrict__ b9, float lam,
+                            float mu, int n1, int n2, int n3) {
+    const int64_t V = (int64_t)n1 * n2 * n3;
+    const float eps = 1e-8f;
+    const float thr = lam / mu;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
+        Idx3 p = unravel(t, n2, n3);
+        float gx[9], tb[9];
+        float sk = 1.0f * eps;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                gx[i * 3 + j] = gdir(x3 + i * V, p.i, p.j, p.k, n1, n2, n3, j);
+                tb[i * 3 + j] = gx[i * 3 + j] + b9[(i * 3 + j) * V + t];
+                sk += tb[i * 3 + j] * tb[i * 3 + j];
+            }
+        sk = sqrtf(sk);
+        float m = fmaxf(sk - thr, 0.f);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            float dv = m * (tb[q] / sk);
+            d9[q * V + t] = dv;
+            b9[q * V + t] += gx[q] - dv;
+        }
+    }
+}
+
+void grad_u(const float *u, Dims3 d, float *out3, cudaStream_t s) {
+    k_grad_u<<<grid_for(d.size(), 256), 256, 0, s>>>(u, (int)d.n1, (int)d.n2, (int)d.n3, out3);
+    LAMINO_LAUNCH("k_grad_u");
+}
+void divergence(const float *du3, Dims3 d, float *out, cudaStream_t s) {
+    k_divergence<<<grid_for(d.size(), 256), 256, 0, s>>>(du3, (int)d.n1, (int)d.n2, (int)d.n3, out);
+    LAMINO_LAUNCH("k_divergence");
+}
+void laplacian_axpy(float *y, float mu, const float *u, Dims3 d, cudaStream_t s) {
+    dim3 g(grid_for(d.size(), 256), 3);
+    k_laplacian_axpy<<<g, 256, 0, s>>>(y, mu, u, (int)d.n1, (int)d.n2, (int)d.n3);
+    LAMINO_LAUNCH("k_laplacian_axpy");
+}
+void sb_rhs(const float *yT3, const float *d9, const float *b9, float mu, Dims3 dims, float *rhs3, cudaStream_t s) {
+    dim3 g(grid_for(dims.size(), 256), 3);
+    k_sb_rhs<<<g, 256, 0, s>>>(yT3, d9, b9, mu, (int)dims.n1, (int)dims.n2, (int)dims.n3, rhs3);
+    LAMINO_LAUNCH("k_sb_rhs");
+}
+void sb_shrink(const float *x3, float *d9, float *b9, float lam, float mu, Dims3 dims, cudaStream_t s) {
+    k_sb_shrink<<<grid_for(dims.size(), 256), 256, 0, s>>>(x3, d9, b9, lam, mu, (int)dims.n1, (int)dims.n2,
+                                                           (int)dims.n3);
+    LAMINO_LAUNCH("k_sb_shrink");
+}
+
+// ---------------------------------------------------------------------------
+// ramp preconditioner (include/precond.h:33-87)
+// ---------------------------------------------------------------------------
+
+__global__ void k_filter_mul(float2 *__restrict__ S, const float *__restrict__ f, int64_t plane, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float w = f[i % plane];
+        S[i].x *= w;
+        S[i].y *= w;
+    }
+}
+
+RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
+    int64_t n2 = d.n2, n3 = d.n3, h3 = n3 / 2 + 1;
+    std::vector<float> xf(h3), yf(n2), f(n2 * h3);
+    for (int64_t i = 0; i < h3; ++i) xf[i] = (float)i / (float)n3;
+    for (int64_t i = 0; i < n2; ++i) yf[i] = (i <= n2 / 2) ? (float)i / (float)n2 : (float)(i - n2) / (float)n2;
+    // the 1/(n2 n3) normalisation of the c2r is folded into the filter
+    float scale = (float)(1.0 / (double)(n2 * n3));
+    for (int64_t j = 0; j < n2; ++j)
+        for (int64_t i = 0; i < h3; ++i) f[j * h3 + i] = std::sqrt(xf[i] * xf[i] + yf[j] * yf[j]) * scale;
+    filt.alloc(n2 * h3);
+    LAMINO_CUDA(cudaMemcpy(filt.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    spec.alloc(3 * d.n1 * n2 * h3);
+    int n[2] = {(int)n2, (int)n3};
+    LAMINO_CUFFT(cufftPlanMany(&r2c.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, (int)(3 * d.n1)));
+    r2c.valid = true;
+    LAMINO_CUFFT(cufftPlanMany(&c2r.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, (int)(3 * d.n1)));
+    c2r.valid = true;
+}
+
+void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
+    int64_t h3 = d.n3 / 2 + 1, plane = d.n2 * h3;
+    LAMINO_CUFFT(cufftSetStream(r2c.h, s));
+    LAMINO_CUFFT(cufftSetStream(c2r.h, s));
+    LAMINO_CUFFT(cufftExecR2C(r2c.h, const_cast<float *>(r3), (cufftComplex *)spec.p));
+    k_filter_mul<<<grid_for(3 * d.n1 * plane, 256), 256, 0, s>>>(spec.p, filt.p, plane, 3 * d.n1 * plane);
+    LAMINO_LAUNCH("k_filter_mul");
+    LAMINO_CUFFT(cufftExecC2R(c2r.h, (cufftComplex *)spec.p, z3));
+}
+
+// ---------------------------------------------------------------------------
+// CG (src/conjgrad.cpp:37-117)
+// ---------------------------------------------------------------------------
+
+__global__ void k_cg_update(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
+                            const float *__restrict__ Ap, float alpha, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += p[i] * alpha;
+        r[i] -= Ap[i] * alpha;
+    }
+}
+__global__ void k_cg_dir(float *__restrict__ p, const float *__restrict__ z, float beta, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + p[i] * beta;
+}
+
+CgStats cgsolver(const OpFn &A, const float *y3, float *x3, Dims3 d, int max_iter, float tol, cudaStream_t s) {
+    const int64_t n = 3 * d.size();
+    DevBuf<float> r(n), p(n), z(n), Ap(n);
+    RampPrecond M(d);
+    Reducer red(4);
+    CgStats st;
+    A(x3, Ap.p, s);
+    vec_lin2(r.p, 1.f, y3, -1.f, Ap.p, n, s);
+    M.apply3(r.p, z.p, s);
+    LAMINO_CUDA(cudaMemcpyAsync(p.p, z.p, n * 4, cudaMemcpyDeviceToDevice, s));
+    red.zero(1, s);
+    vec_dot(z.p, r.p, n, red.d, s);
+    red.fetch(1, s);
+    double rs_old = red.h[0];
+    for (int it = 0; it < max_iter; ++it) {
+        A(p.p, Ap.p, s);
+        red.zero(2, s);
+        vec_dot(p.p, Ap.p, n, red.d, s);
+        red.fetch(1, s);
+        double pAp = red.h[0];
+        if (std::fabs(pAp) < 1e-10) break;
+        float alpha = (float)(rs_old / pAp);
+        k_cg_update<<<grid_for(n, 256), 256, 0, s>>>(x3, r.p, p.p, Ap.p, alpha, n);
+        LAMINO_LAUNCH("k_cg_update");
+        M.apply3(r.p, z.p, s);
+        red.zero(1, s);
+        vec_dot(z.p, r.p, n, red.d, s);
+        red.fetch(1, s);
+        double rs_new = red.h[0];
+        st.iters = it + 1;
+        st.last_res = std::sqrt(std::fabs(rs_new));
+        if (std::sqrt(std::fabs(rs_new)) < tol) break;
+        float beta = (float)(rs_new / rs_old);
+        k_cg_dir<<<grid_for(n, 256), 256, 0, s>>>(p.p, z.p, beta, n);
+        LAMINO_LAUNCH("k_cg_dir");
+        rs_old = rs_new;
+    }
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// split Bregman (src/bregman.cpp:39-134)
+// ---------------------------------------------------------------------------
+
+int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam, float mu, int outer_max,
+                  int inner_max, float tol, float xtol, cudaStream_t s) {
+    const int64_t V = d.size(), n = 3 * V;
+    DevBuf<float> xold(n), dd(9 * V), bb(9 * V), rhs(n);
+    LAMINO_CUDA(cudaMemcpyAsync(xold.p, x3, n * 4, cudaMemcpyDeviceToDevice, s));
+    LAMINO_CUDA(cudaMemsetAsync(dd.p, 0, dd.bytes(), s));
+    LAMINO_CUDA(cudaMemsetAsync(bb.p, 0, bb.bytes(), s));
+    OpFn Ap = [&](const float *u, float *out, cudaStream_t st) {
+        A(u, out, st);
+        laplacian_axpy(out, mu, u, d, st);
+    };
+    Reducer red(8);
+    int it = 0;
+    for (; it < outer_max; ++it) {
+        sb_rhs(yT3, dd.p, bb.p, mu, d, rhs.p, s);
+        // x = cgsolver(Ap, rhs, x_old, ...)
+        LAMINO_CUDA(cudaMemcpyAsync(x3, xold.p, n * 4, cudaMemcpyDeviceToDevice, s));
+        cgsolver(Ap, rhs.p, x3, d, inner_max, tol, s);
+        sb_shrink(x3, dd.p, bb.p, lam, mu, d, s);
+        red.zero(6, s);
+        vec_sqdist3(x3, xold.p, V, red.d, s);
+        vec_sqdist3(xold.p, nullptr, V, red.d + 3, s);
+        red.fetch(6, s);
+        double nd = 0.0;
+        for (int i = 0; i < 3; ++i) nd += std::sqrt(red.h[i]) / (std::sqrt(red.h[3 + i]) + 1e-8);
+        LAMINO_CUDA(cudaMemcpyAsync(xold.p, x3, n * 4, cudaMemcpyDeviceToDevice, s));
+        if (nd < xtol) { ++it; break; }
+    }
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    return it;
+}
+
+// ---------------------------------------------------------------------------
+// Nesterov (src/nagopt.cpp:116-209)
+// ---------------------------------------------------------------------------
+
+__global__ void k_extrap(float *__restrict__ y, const float *__restrict__ x, const float *__restrict__ xo, float beta,
+                         int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = x[i] + (x[i] - xo[i]) * beta;
+}
+
+int nagopt(const GradFn &grad, const LossFn &loss, float *x, Dims3 d, int max_iters, float lipschitz, float tol,
+           float xtol, int max_inner, cudaStream_t s) {
+    const int64_t V = d.size(), n = 3 * V;
+    DevBuf<float> xold(n), y(n), g(n);
+    LAMINO_CUDA(cudaMemcpyAsync(xold.p, x, n * 4, cudaMemcpyDeviceToDevice, s));
+    Reducer red(8);
+    double t = 1, tnew = 1;
+    float step = (float)(0.1 / lipschitz), step_prev = step;
+    double xerr = 1e300;
+    int it = 0;
+    for (; it < max_iters; ++it) {
+        for (int inner = 0; inner < max_inner; ++inner) {
+            float beta = (float)(tnew * (1.0 / t - 1.0));
+            tnew = 0.5 * (std::sqrt(std::pow(t, 4) + 4 * std::pow(t, 2)) - std::pow(t, 2));
+            k_extrap<<<grid_for(n, 256), 256, 0, s>>>(y.p, x, xold.p, beta, n);
+            LAMINO_LAUNCH("k_extrap");
+            grad(y.p, g.p, s);
+            vec_lin2(x, 1.f, y.p, -step, g.p, n, s);
+            double ex = loss(x, s);
+            double ey = loss(y.p, s);
+            red.zero(3, s);
+            vec_sqdist3(g.p, nullptr, V, red.d, s);
+            red.fetch(3, s);
+            double gy = 0.0;
+            for (int i = 0; i < 3; ++i) gy += std::sqrt(red.h[i]);
+            gy *= 0.5 * step;
+            if (ex > ey + gy) {
+                step *= 0.9f;
+            } else {
+                step = step_prev;
+                t = tnew;
+                red.zero(6, s);
+                vec_sqdist3(x, xold.p, V, red.d, s);
+                vec_sqdist3(x, nullptr, V, red.d + 3, s);
+                red.fetch(6, s);
+                double xe = 0, xn = 0;
+                for (int i = 0; i < 3; ++i) { xe += std::sqrt(red.h[i]); xn += std::sqrt(red.h[3 + i]); }
+                xerr = xe / xn;
+                if (xerr < xtol) return it + 1;
+                LAMINO_CUDA(cudaMemcpyAsync(xold.p, x, n * 4, cudaMemcpyDeviceToDevice, s));
+                break;
+            }
+        }
+        double e = loss(x, s);
+        if (e < tol) { ++it; break; }
+    }
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    return it;
+}
+
+// ---------------------------------------------------------------------------
+// power iteration
+// ---------------------------------------------------------------------------
+
+__global__ void k_uniform(float *__restrict__ x, int64_t n, unsigned long long seed) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        x[i] = (float)((z >> 40) * (1.0 / 16777216.0));
+    }
+}
+
+double lipschitz(const OpFn &A, Dims3 d, int max_iters, double tol, unsigned long long seed, cudaStream_t s) {
+    const int64_t n = 3 * d.size();
+    DevBuf<float> x(n), Ax(n);
+    Reducer red(2);
+    k_uniform<<<grid_for(n, 256), 256, 0, s>>>(x.p, n, seed);
+    LAMINO_LAUNCH("k_uniform");
+    red.zero(1, s);
+    vec_dot(x.p, x.p, n, red.d, s);
+    red.fetch(1, s);
+    vec_scale(x.p, (float)(1.0 / std::sqrt(red.h[0])), x.p, n, s);
+    double L = 0.0;
+    for (int i = 0; i < max_iters; ++i) {
+        A(x.p, Ax.p, s);
+        red.zero(1, s);
+        vec_dot(Ax.p, Ax.p, n, red.d, s);
+        red.fetch(1, s);
+        double nA = std::sqrt(red.h[0]);
+        if (nA < 1e-12) return 0.0;
+        vec_scale(x.p, (float)(1.0 / nA), Ax.p, n, s);
+        if (std::fabs(nA - L) < tol) { L = nA; break; }
+        L = nA;
+    }
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    return L;
+}
+
+}  // namespace lamino

@@ -1,0 +1,74 @@
+// Solver kernels and host-side solver loops (CG, split-Bregman, NAG, power
+// iteration) over packed 3-component volumes [3][n1][n2][n3].
+#pragma once
+
+#include <functional>
+
+#include "common.cuh"
+
+namespace lamino {
+
+using OpFn = std::function<void(const float *x3, float *y3, cudaStream_t)>;
+
+// Device scalar scratch for FP64 reductions (pinned host mirror).
+struct Reducer {
+    double *d = nullptr;   // device accumulators
+    double *h = nullptr;   // pinned host copy
+    int cap = 0;
+    explicit Reducer(int n = 16);
+    ~Reducer();
+    Reducer(const Reducer &) = delete;
+    Reducer &operator=(const Reducer &) = delete;
+    void zero(int n, cudaStream_t s);
+    void fetch(int n, cudaStream_t s);  // copies and synchronises
+};
+
+// ---- vector kernels (n = element count) ----
+void vec_lin2(float *out, float a, const float *x, float b, const float *y, int64_t n, cudaStream_t s);
+void vec_scale(float *out, float a, const float *x, int64_t n, cudaStream_t s);
+// out[slot] += sum (double) x*y
+void vec_dot(const float *x, const float *y, int64_t n, double *out, cudaStream_t s);
+// out[slot+c] += sum_c (x_c - y_c)^2 per component c of 3 (y may be null)
+void vec_sqdist3(const float *x, const float *y, int64_t V, double *out3, cudaStream_t s);
+// max element (as double, via ordered-int trick on floats)
+void vec_max(const float *x, int64_t n, double *out, cudaStream_t s);
+
+// ---- regularisers / finite differences (one component of dims d) ----
+void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStream_t s);
+void grad_u(const float *u, Dims3 d, float *out3, cudaStream_t s);
+void divergence(const float *du3, Dims3 d, float *out, cudaStream_t s);
+void laplacian_axpy(float *y, float mu, const float *u, Dims3 d, cudaStream_t s);  // y += mu*lap(u)
+// rhs_i = yT_i + mu * divergence(d_i - b_i), i = 0..2 (d, b: [3][3][V])
+void sb_rhs(const float *yT3, const float *d9, const float *b9, float mu, Dims3 dims, float *rhs3, cudaStream_t s);
+// isotropic shrink + Bregman update from grad_u(x_i) computed on the fly
+void sb_shrink(const float *x3, float *d9, float *b9, float lam, float mu, Dims3 dims, cudaStream_t s);
+
+// ---- ramp preconditioner (include/precond.h:33-87) ----
+struct RampPrecond {
+    Dims3 d;
+    FftPlan r2c, c2r;
+    DevBuf<float2> spec;
+    DevBuf<float> filt;
+    explicit RampPrecond(Dims3 d);
+    void apply3(const float *r3, float *z3, cudaStream_t s);  // all 3 components
+};
+
+// ---- solver loops (host control flow mirrors the reference) ----
+struct CgStats { int iters = 0; double last_res = 0; };
+// src/conjgrad.cpp:37-117.  x3 holds x0 on entry and the solution on exit.
+CgStats cgsolver(const OpFn &A, const float *y3, float *x3, Dims3 d, int max_iter, float tol, cudaStream_t s);
+
+// src/bregman.cpp:39-134.  x3 in/out.
+int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam, float mu, int outer_max,
+                  int inner_max, float tol, float xtol, cudaStream_t s);
+
+// src/nagopt.cpp:116-209 (vector form); grad and loss are closures.
+using GradFn = std::function<void(const float *x3, float *g3, cudaStream_t)>;
+using LossFn = std::function<double(const float *x3, cudaStream_t)>;
+int nagopt(const GradFn &grad, const LossFn &loss, float *x3, Dims3 d, int max_iters, float lipschitz, float tol,
+           float xtol, int max_inner, cudaStream_t s);
+
+// power iteration for ||A|| (src/lipschitz.cpp:31-53, made to work: seeded start, FP64 norms)
+double lipschitz(const OpFn &A, Dims3 d, int max_iters, double tol, unsigned long long seed, cudaStream_t s);
+
+}  // namespace lamino

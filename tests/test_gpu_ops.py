@@ -1,0 +1,173 @@
+"""GPU parity tests for the operator path, through the C ABI (ctypes).
+
+Tolerances: single operator applies within relative L2 1e-5 of the oracle
+(FP64, eps 1e-12, the reference's float coordinates); the Toeplitz FP16
+storage variant within 2e-3 of the FP32 one.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def test_geometry_points_bitexact(L, gold_ref):
+    for tag in ("odd", "even"):
+        th = gold_ref[f"grid_{tag}_theta"]
+        _, nr, nc, g = gold_ref[f"grid_{tag}_meta"]
+        pg = L.PolarGrid(th, int(nr), int(nc), np.float32(g))
+        x, y, z = pg.points()
+        gx, gy, gz = gold_ref[f"grid_{tag}_xyz"]
+        assert np.array_equal(x, gx) and np.array_equal(y, gy) and np.array_equal(z, gz)
+
+
+def _golden_grid(L, gold_orc):
+    th = gold_orc["op_theta"]
+    nr, nc, g = gold_orc["op_meta"]
+    return L.PolarGrid(th, int(nr), int(nc), np.float32(g)), np.float32(g)
+
+
+def test_nufft_vs_golden_nudft(L, gold_orc):
+    pg, _ = _golden_grid(L, gold_orc)
+    assert rel(L.nufft3d2(gold_orc["op_f"], pg), gold_orc["op_nudft2"]) < TOL
+    assert rel(L.nufft3d1(gold_orc["op_c"], pg, (9, 5, 11)), gold_orc["op_nudft1"]) < TOL
+
+
+def test_operators_vs_golden(L, gold_orc):
+    pg, g = _golden_grid(L, gold_orc)
+    assert rel(L.forward(gold_orc["op_m"], pg, g), gold_orc["op_forward"]) < TOL
+    assert rel(L.adjoint(gold_orc["op_proj"], pg, (9, 5, 11), g), gold_orc["op_adjoint"]) < TOL
+    assert rel(L.sysmat(gold_orc["op_m"], pg, g), gold_orc["op_sysmat"]) < TOL
+
+
+CASES = [
+    # volume dims, [(nproj, nrows, ncols, gamma)]
+    ((22, 6, 20), [(7, 31, 29, 0.0), (5, 31, 29, np.pi / 4)]),
+    ((17, 9, 24), [(6, 26, 34, 1.1)]),
+]
+
+
+@pytest.mark.parametrize("dims,geoms", CASES)
+def test_operators_vs_oracle(L, O, dims, geoms):
+    rng = np.random.default_rng(11)
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    pgs, opgs = [], []
+    for np_, nr, nc, g in geoms:
+        th = rng.uniform(0, 2 * np.pi, np_).astype(np.float32)
+        pgs.append(L.PolarGrid(th, nr, nc, np.float32(g)))
+        opgs.append(O.PolarGrid(th, nr, nc, np.float32(g)))
+    m = O.synthetic_magnetization(dims, seed=5, sigma=1.5)
+    for pg, opg in zip(pgs, opgs):
+        assert rel(L.forward(m, pg), O.forward(m, opg, opg.gamma, plan_o)) < TOL
+        proj = rng.standard_normal(opg.dims()).astype(np.float32)
+        assert rel(L.adjoint(proj, pg, dims), O.adjoint(proj, opg, dims, opg.gamma, plan_o)) < TOL
+    want = O.normal(m, opgs, [p.gamma for p in opgs], plan_o)
+    assert rel(L.sysmat(m, pgs), want) < TOL
+    # random (white) input exercises high frequencies
+    xr = rng.standard_normal((3,) + dims).astype(np.float32)
+    assert rel(L.sysmat(xr, pgs), O.normal(xr, opgs, [p.gamma for p in opgs], plan_o)) < TOL
+
+
+@pytest.mark.parametrize("dims,geoms", CASES)
+def test_toeplitz_vs_oracle(L, O, dims, geoms):
+    rng = np.random.default_rng(12)
+    pgs, opgs, ths = [], [], []
+    for np_, nr, nc, g in geoms:
+        th = rng.uniform(0, 2 * np.pi, np_).astype(np.float32)
+        ths.append(th)
+        pgs.append(L.PolarGrid(th, nr, nc, np.float32(g)))
+        opgs.append(O.PolarGrid(th, nr, nc, np.float32(g)))
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    T = L.ToeplitzNormal(pgs, dims, "fp32")
+    for x in (O.synthetic_magnetization(dims, seed=6, sigma=1.5),
+              rng.standard_normal((3,) + dims).astype(np.float32)):
+        want = O.normal(x, opgs, [p.gamma for p in opgs], plan_o)
+        assert rel(T(x), want) < TOL
+        assert rel(T(x), L.sysmat(x, pgs)) < TOL
+    T16 = L.ToeplitzNormal(pgs, dims, "fp16")
+    x = O.synthetic_magnetization(dims, seed=7, sigma=1.5)
+    assert rel(T16(x), T(x)) < 2e-3
+
+
+def test_toeplitz_matches_analytic_oracle(L, O):
+    rng = np.random.default_rng(13)
+    dims = (9, 4, 8)
+    ths = [rng.uniform(0, 6.28, 5).astype(np.float32), rng.uniform(0, 6.28, 3).astype(np.float32)]
+    gms = [0.0, 0.9]
+    T = L.ToeplitzNormal([L.PolarGrid(t, 12, 11, g) for t, g in zip(ths, gms)], dims)
+    Tk = O.toeplitz_kernel(dims, [t.astype(np.float64) for t in ths],
+                           [float(np.float32(g)) for g in gms], 12, 11)
+    x = rng.standard_normal((3,) + dims).astype(np.float32)
+    assert rel(T(x), O.toeplitz_apply(x.astype(np.float64), Tk)) < TOL
+
+
+def test_edge_sizes(L, O):
+    """Degenerate shapes: single projection, single row, thin volume."""
+    rng = np.random.default_rng(14)
+    dims = (3, 1, 2)
+    th = np.array([0.3], np.float32)
+    pg = L.PolarGrid(th, 1, 3, 0.5)
+    opg = O.PolarGrid(th, 1, 3, np.float32(0.5))
+    pe = O.NufftPlan(dims, exact=True)
+    m = rng.standard_normal((3,) + dims).astype(np.float32)
+    assert rel(L.forward(m, pg), O.forward(m, opg, opg.gamma, pe)) < TOL
+    assert rel(L.sysmat(m, pg), O.sysmat(m, opg, opg.gamma, pe)) < TOL
+    T = L.ToeplitzNormal([pg], dims)
+    assert rel(T(m), O.sysmat(m, opg, opg.gamma, pe)) < TOL
+
+
+def test_invalid_arguments_raise(L):
+    with pytest.raises(L.LaminoError) as e:
+        L.PolarGrid(np.zeros(0, np.float32), 5, 5, 0.0)
+    assert e.value.code == 1
+    with pytest.raises(L.LaminoError):
+        L.NufftPlan((0, 4, 4))
+    pg = L.PolarGrid([0.1], 4, 4, 0.0)
+    with pytest.raises(L.LaminoError):
+        L.ToeplitzNormal([pg], (4, -1, 4))
+
+
+def test_device_tensors_in_place(L, O):
+    """torch CUDA tensors go through the same C ABI without host staging."""
+    import torch
+    dims = (12, 5, 10)
+    th = np.linspace(0, 3, 6, dtype=np.float32)
+    pg = L.PolarGrid(th, 17, 15, 0.4)
+    x = O.synthetic_magnetization(dims, seed=3, sigma=1.5)
+    xd = torch.from_numpy(x).cuda()
+    T = L.ToeplitzNormal([pg], dims)
+    yd = T(xd)
+    torch.cuda.synchronize()
+    assert yd.is_cuda
+    assert rel(yd.cpu().numpy(), T(x)) < 1e-6
+
+
+def test_full_size_toeplitz_properties(L):
+    """51x511x511 reconstruction size (padded 721x71x721), 4 gammas x 361 angles,
+    1233x1233 padded projections: symmetry, linearity, agreement with the NUFFT form."""
+    import torch
+    dims = (721, 71, 721)
+    rng = np.random.default_rng(15)
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, 361).astype(np.float32), 1233, 1233, g)
+           for g in np.deg2rad([0.0, 45.0, 90.0, 135.0]).astype(np.float32)]
+    T = L.ToeplitzNormal(pgs, dims, "fp32")
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((3,) + dims, device="cuda", generator=g)
+    y = torch.randn((3,) + dims, device="cuda", generator=g)
+    Ax, Ay = T(x), T(y)
+    lhs = torch.sum(Ax.double() * y.double()).item()
+    rhs = torch.sum(x.double() * Ay.double()).item()
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+    assert torch.sum(x.double() * Ax.double()).item() > 0
+    Axy = T(2.0 * x - 0.5 * y)
+    assert (torch.linalg.norm(Axy - (2.0 * Ax - 0.5 * Ay)) / torch.linalg.norm(Axy)).item() < 1e-5
+    # smooth input: agreement with the NUFFT-form sum_gamma sysmat
+    k = torch.arange(721, device="cuda", dtype=torch.float32)
+    s = torch.exp(-((k - 360) / 120.0) ** 2)
+    xs = (s[:, None, None] * torch.ones(71, device="cuda")[None, :, None] * s[None, None, :])
+    xs = torch.stack([xs, 0.5 * xs, -0.25 * xs]).contiguous()
+    ys = T(xs)
+    yn = L.sysmat(xs, pgs)
+    assert (torch.linalg.norm(ys - yn) / torch.linalg.norm(yn)).item() < TOL

@@ -1,0 +1,105 @@
+"""GPU parity tests for the solver path (regularisers, CG, split Bregman, NAG,
+power iteration, MBIR drivers), through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def test_qggmrf_vs_reference(L, gold_ref):
+    g = gold_ref["qg_g0"].copy()
+    L.opt.qggmrf(g, gold_ref["qg_x"], 1000.0, 1.2)
+    assert rel(g, gold_ref["qg_g"]) < 1e-6
+
+
+def test_finite_differences_vs_reference(L, gold_ref):
+    assert np.allclose(L.opt.grad_u(gold_ref["fd_u"]), gold_ref["fd_grad"], rtol=0, atol=1e-6)
+    assert np.allclose(L.opt.divergence(gold_ref["fd_du"]), gold_ref["fd_div"], rtol=0, atol=1e-6)
+    assert np.allclose(L.opt.laplacian(gold_ref["fd_u"]), gold_ref["fd_lap"], rtol=0, atol=2e-6)
+
+
+def test_ramp_preconditioner_vs_oracle(L, O):
+    rng = np.random.default_rng(1)
+    dims = (5, 9, 12)
+    r = rng.standard_normal((3,) + dims).astype(np.float32)
+    M = O.RampPreconditioner(dims)
+    want = np.stack([M.apply(r[i]) for i in range(3)])
+    assert rel(L.opt.ramp_precond(r), want) < 1e-5
+
+
+def _problem(L, O, dims=(14, 6, 12), geoms=((8, 21, 19, 0.0), (6, 21, 19, 0.7)), seed=2):
+    rng = np.random.default_rng(seed)
+    pgs, opgs = [], []
+    for np_, nr, nc, g in geoms:
+        th = rng.uniform(0, 2 * np.pi, np_).astype(np.float32)
+        pgs.append(L.PolarGrid(th, nr, nc, np.float32(g)))
+        opgs.append(O.PolarGrid(th, nr, nc, np.float32(g)))
+    return pgs, opgs
+
+
+def test_cgsolver_vs_oracle(L, O):
+    dims = (14, 6, 12)
+    pgs, opgs = _problem(L, O, dims)
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    A_o = lambda v: O.normal(v, opgs, [p.gamma for p in opgs], plan_o)
+    xt = O.synthetic_magnetization(dims, seed=9, sigma=1.5).astype(np.float64)
+    y = A_o(xt)
+    want = O.cgsolver(A_o, y, np.zeros_like(y), 8, 1e-12)
+    T = L.ToeplitzNormal(pgs, dims)
+    got = L.opt.cgsolver(T, y.astype(np.float32), np.zeros_like(y, np.float32), 8, 1e-12)
+    assert rel(got, want) < 1e-4
+    got_n = L.opt.cgsolver((L.NufftPlan(dims), pgs), y.astype(np.float32), np.zeros_like(y, np.float32), 8, 1e-12)
+    assert rel(got_n, want) < 1e-4
+
+
+def test_split_bregman_vs_oracle(L, O):
+    dims = (14, 6, 12)
+    pgs, opgs = _problem(L, O, dims)
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    A_o = lambda v: O.normal(v, opgs, [p.gamma for p in opgs], plan_o)
+    yT = A_o(O.synthetic_magnetization(dims, seed=10, sigma=1.5).astype(np.float64))
+    want = O.split_bregman(A_o, yT, np.zeros_like(yT), 0.1, 10.0, 4, 3, 1e-12, 1e-12)
+    got = L.opt.split_bregman(L.ToeplitzNormal(pgs, dims), yT.astype(np.float32),
+                              np.zeros_like(yT, np.float32), 0.1, 10.0, 4, 3, 1e-12, 1e-12)
+    assert rel(got, want) < 1e-4
+
+
+def test_lipschitz_vs_oracle(L, O):
+    dims = (14, 6, 12)
+    pgs, opgs = _problem(L, O, dims)
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    A_o = lambda v: O.normal(v, opgs, [p.gamma for p in opgs], plan_o)
+    Lo = O.lipschitz(A_o, (3,) + dims, max_iters=60, tol=1e-9)
+    Lg = L.opt.lipschitz(L.ToeplitzNormal(pgs, dims), dims, max_iters=60, tol=1e-9)
+    assert Lg == pytest.approx(Lo, rel=1e-3)
+
+
+def _datasets(L, O, recon=(8, 5, 9), nproj=(6, 5), det=(9, 11), gammas=(0.0, 0.8), seed=3):
+    """Synthetic projections from the oracle forward model on the padded grid."""
+    rng = np.random.default_rng(seed)
+    m = O.synthetic_magnetization(recon, seed=seed, sigma=1.0).astype(np.float64)
+    plan = O.NufftPlan(recon, exact=True)
+    data = []
+    for n, g in zip(nproj, gammas):
+        th = rng.uniform(0, 2 * np.pi, n).astype(np.float32)
+        pg = O.PolarGrid(th, det[0], det[1], np.float32(g))
+        proj = O.forward(m, pg, pg.gamma, plan) + 0.05
+        data.append((proj.astype(np.float32), th, np.float32(g)))
+    return data
+
+
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_mbir_vs_oracle(L, O, method):
+    recon = (8, 5, 9)
+    data = _datasets(L, O, recon)
+    po = O.ReconParams(maxIters=4, innerIters=2)
+    fn_o = {1: O.MBIR1, 2: O.MBIR2, 3: O.MBIR3}[method]
+    want = fn_o(data, recon, po, exact=True)
+    for kind in ("toeplitz", "nufft"):
+        pl = L.ReconParams(maxIters=4, innerIters=2, op_kind=kind)
+        fn = {1: L.MBIR1, 2: L.MBIR2, 3: L.MBIR3}[method]
+        got = fn(data, recon, pl)
+        assert got.shape == (3,) + recon
+        assert rel(got, want) < 1e-4, kind
