@@ -85,6 +85,24 @@ int lamino_gradient(lamino_plan_t p, lamino_geom_t g, const float *f3, const flo
 int lamino_residual(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float yTy, double *out,
                     void *stream);
 
+/* Allocation-free variant of lamino_residual (no counterpart in the reference).
+ * For callers that cannot allocate device memory: a service overlapping several
+ * reconstructions on one GPU evaluates this residual (the MBIR3 loss) inside its
+ * line search, where a cudaMalloc/cudaFree would stall the other requests
+ * (cudaFree waits for the whole device), and a caller whose device memory is
+ * owned by another allocator may get none at all.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine: A f and the FP64 reduction slots live
+ * in a 96 MiB static device array, held by every GPU that loads this library
+ * until exit, so the volume may hold at most 8,388,586 voxels (n1*n2*n3);
+ * larger volumes are rejected with LAMINO_ERR_ARG.  f3 and yT3 must be device
+ * pointers (host pointers are rejected); res is host memory.  The first call on
+ * a device resolves the array's device address (with that device current) and
+ * should come before any stream capture.  Every call shares the array and it
+ * keeps the last call's contents (the reduction slots are cleared at the start
+ * of each call); calls that overlap on the GPU, on any stream, race. */
+int lamino_residual_noalloc(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float yTy,
+                            double *res, void *stream);
+
 /* ---- Toeplitz normal operator ----------------------------------------------
  * sum_gamma sysmat as a 3x3 block convolution (no reference counterpart; it
  * replaces the MBIR `A` closures src/mbir_cg.cpp:97-105, src/mbir_sb.cpp:89-97).

@@ -2,6 +2,7 @@
 // converts C++ exceptions into status codes plus a thread-local message, and
 // stages host buffers through device memory when it is given host pointers.
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -528,6 +529,82 @@ int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *p
     Out<float> o(out3, 3 * rd.size(), S(stream));
     mbir(method, data, rd, prm, o.d, S(stream));
     o.finish(S(stream));
+    API_END
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual.
+//
+// Callers that cannot allocate device memory use lamino_residual_noalloc: a
+// reconstruction service that overlaps several requests on one GPU evaluates
+// this residual (the MBIR3 loss) inside its Nesterov line search, and a
+// cudaMalloc/cudaFree there would stall every other request (cudaFree waits
+// for the whole device); a caller whose device memory is owned by another
+// allocator (a framework's caching allocator that has reserved most of HBM)
+// may not be able to obtain fresh device memory at all.  Its scratch -- A f
+// (3 volumes) and the six FP64 reduction slots -- lives in the static array
+// below, of fixed size on every GPU that loads this library until exit.
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr size_t kNoAllocScratchBytes = (size_t)96 << 20;  // 96 MiB
+constexpr size_t kNoAllocHeader = 256;                      // 6 doubles, padded to 256 B
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void *g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+
+// Device address of the static scratch for the current device, resolved once
+// per device with that device current.
+void *noalloc_scratch() {
+    int dev = 0;
+    LAMINO_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw Error(ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            throw Error(ERR_CUDA, std::string("cudaGetSymbolAddress of the static scratch failed: ") +
+                                      cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+extern "C" int lamino_residual_noalloc(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3,
+                                       float yTy, double *res, void *stream) {
+    API_BEGIN
+    if (!p || !g || !res) throw Error(ERR_ARG, "null argument");
+    const int64_t V = p->p->vol.size();
+    const size_t need = kNoAllocHeader + (size_t)3 * V * sizeof(float);
+    if (need > kNoAllocScratchBytes)
+        throw Error(ERR_ARG, "lamino_residual_noalloc: volume of " + std::to_string(V) +
+                                 " voxels exceeds the static scratch (at most " +
+                                 std::to_string((kNoAllocScratchBytes - kNoAllocHeader) / 12) + " voxels)");
+    if (!is_device_ptr(f3) || !is_device_ptr(yT3))
+        throw Error(ERR_ARG, "lamino_residual_noalloc needs device pointers for f and yT");
+    cudaStream_t s = S(stream);
+    unsigned char *base = static_cast<unsigned char *>(noalloc_scratch());
+    double *acc = reinterpret_cast<double *>(base);
+    float *Ax = reinterpret_cast<float *>(base + kNoAllocHeader);
+    LAMINO_CUDA(cudaMemsetAsync(acc, 0, 6 * sizeof(double), s));  // slots keep the last call's sums
+    const Geom *gp = g->g.get();
+    p->p->normal_ptrs(&gp, 1, f3, Ax, s);
+    for (int i = 0; i < 3; ++i) {
+        vec_dot(f3 + i * V, Ax + i * V, V, acc + i, s);
+        vec_dot(f3 + i * V, yT3 + i * V, V, acc + 3 + i, s);
+    }
+    double h[6];
+    LAMINO_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    double e = 0;
+    for (int i = 0; i < 3; ++i) e += std::sqrt(h[i] - 2.0 * h[3 + i] + (double)yTy);
+    *res = e;
     API_END
 }
 

@@ -540,6 +540,29 @@ void NufftPlan::normal(const std::vector<const Geom *> &gs, const float *x3, flo
     LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
 }
 
+void NufftPlan::normal_ptrs(const Geom *const *gs, int ng, const float *x3, float *y3, cudaStream_t s) {
+    if (!gs || ng <= 0) throw Error(ERR_ARG, "normal operator needs at least one geometry");
+    for (int i = 0; i < ng; ++i)
+        if (gs[i]->npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    pad_real(x3, 3, s);
+    fft_fine(-1, 3, s);
+    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
+    Fine F = fine_of(*this);
+    for (int i = 0; i < ng; ++i) {
+        GeomView gv = gs[i]->view();
+        unsigned grid = grid_for(gs[i]->npts(), 256, 148LL * 16 * 8);
+        float inv_scale = 1.0f / (float)(gs[i]->nrows * gs[i]->ncols);
+        LAMINO_W_DISPATCH(w, k_sysmat_points, grid, 256, s, gv, gwork.p, gin.p, nf(), F, inv_scale);
+        LAMINO_LAUNCH("k_sysmat_points");
+    }
+    LAMINO_CUFFT(cufftSetStream(fft3.h, s));
+    for (int c = 0; c < 3; ++c)
+        LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gin.p + c * nf()),
+                                  (cufftComplex *)(gwork.p + c * nf()), CUFFT_INVERSE));
+    extract_real(y3, 3, 1.0f, false, s);
+    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
+}
+
 void NufftPlan::type2(const Geom &g, const float2 *modes, float2 *c, cudaStream_t s) {
     if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
     pad_complex(modes, s);

@@ -43,6 +43,8 @@ struct NufftPlan {
     void adjoint(const Geom &g, const float *proj, float *m3, bool accumulate, cudaStream_t s);
     // sum over geometries of sysmat (src/gradient.cpp:34-89), NUFFT form
     void normal(const std::vector<const Geom *> &gs, const float *x3, float *y3, cudaStream_t s);
+    // same sum over geometries given as a pointer array (no host containers)
+    void normal_ptrs(const Geom *const *gs, int ng, const float *x3, float *y3, cudaStream_t s);
     // raw transforms on one geometry (FINUFFT-level boundary, complex data)
     void type2(const Geom &g, const float2 *modes, float2 *c, cudaStream_t s);
     void type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_t s);
