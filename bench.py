@@ -34,6 +34,9 @@ PADDED = (721, 71, 721)             # internal (W, T, H) after MBIR2 padding
 GAMMAS_DEG = (0.0, 45.0, 90.0, 135.0)
 NPROJ = 361
 DET_PADDED = 1233
+# smaller cases of the same geometry, for profiler captures only (not bench lines)
+SCALES = {"full": ((721, 71, 721), 361, 1233), "half": ((361, 36, 361), 181, 617),
+          "quarter": ((181, 18, 181), 91, 309)}
 
 
 def workload_config(precision: str, n: int):
@@ -250,13 +253,14 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     L.lib()
 
+    dims, nproj, det = SCALES[args.scale]
     rng = np.random.default_rng(2026)
-    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, NPROJ).astype(np.float32), DET_PADDED, DET_PADDED,
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, nproj).astype(np.float32), det, det,
                        np.float32(np.deg2rad(g))) for g in GAMMAS_DEG]
     t0 = time.perf_counter()
-    op = L.ToeplitzNormal(pgs, PADDED, args.precision)
+    op = L.ToeplitzNormal(pgs, dims, args.precision)
     build_s = time.perf_counter() - t0
-    x = synthetic_magnetization_gpu(torch, PADDED)
+    x = synthetic_magnetization_gpu(torch, dims)
     y = torch.empty_like(x)
     stream = torch.cuda.current_stream()
 
@@ -334,7 +338,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded smoothed unit-vector magnetization, "
                                                      "seeded angles)",
-        "config": workload_config(args.precision, world),
+        "config": workload_config(args.precision, world) if args.scale == "full" else
+        {"workload": f"profiling case {args.scale}: padded {dims}, 4 gammas x {nproj} angles, {det}^2"},
         "e2e": {"value": world * k_e2e / (ms_e2e / 1e3), "unit": "applies/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes},
         "gpu_launches": kpa * args.steps,
@@ -362,6 +367,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", choices=sorted(SCALES), default="full",
+                    help="smaller cases of the same geometry for profiler captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
