@@ -36,7 +36,9 @@ NPROJ = 361
 DET_PADDED = 1233
 # smaller cases of the same geometry, for profiler captures only (not bench lines)
 SCALES = {"full": ((721, 71, 721), 361, 1233), "half": ((361, 36, 361), 181, 617),
-          "quarter": ((181, 18, 181), 91, 309)}
+          "quarter": ((181, 18, 181), 91, 309),
+          # same n1 (FFT length 1458) as the full case, thin in n2/n3: > L2 but < 1 GB
+          "pencil": ((721, 18, 360), 45, 309)}
 
 
 def workload_config(precision: str, n: int):

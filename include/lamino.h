@@ -121,7 +121,8 @@ int lamino_normal_destroy(lamino_normal_t op);
  * up to max_applies subsequent applies. */
 int lamino_normal_profile(lamino_normal_t op, int enable, int max_applies);
 /* Stage timings accumulated since lamino_normal_profile: nstages (<= 8) stages in
- * the order pad, r2c, multiply, c2r, crop; ms[k] summed milliseconds; bytes[k] the
+ * the order r2c_rows, dim2_fwd, pencil, dim2_inv, c2r_rows (one kernel each);
+ * ms[k] summed milliseconds; bytes[k] the
  * algorithmic bytes of one apply of stage k; napplies profiled applies;
  * kernels_per_apply this library's kernel launches in one apply.  Any output
  * pointer except nstages may be NULL. */

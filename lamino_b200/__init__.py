@@ -326,7 +326,7 @@ class ToeplitzNormal:
         na, kp = ctypes.c_int(), ctypes.c_int()
         _check(lib().lamino_normal_stage_times(self._h, ctypes.byref(n), ms, by, ctypes.byref(na),
                                                ctypes.byref(kp)))
-        names = ["pad", "r2c", "multiply", "c2r", "crop", "s5", "s6", "s7"]
+        names = ["r2c_rows", "dim2_fwd", "pencil", "dim2_inv", "c2r_rows", "s5", "s6", "s7"]
         return ({names[k]: (ms[k], by[k]) for k in range(n.value)}, na.value, kp.value)
 
     def info(self):

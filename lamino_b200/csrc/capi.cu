@@ -336,9 +336,7 @@ int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes) {
     if (!op) throw Error(ERR_ARG, "null operator");
     const Toeplitz &t = *op->t;
     if (L) { L[0] = t.L1; L[1] = t.L2; L[2] = t.L3; }
-    if (bytes)
-        *bytes = (int64_t)(t.K.bytes() + t.Kh.bytes() + t.Kscale.bytes() + t.xpad.bytes() + t.xhat.bytes() +
-                           t.ypad.bytes());
+    if (bytes) *bytes = (int64_t)t.device_bytes();
     API_END
 }
 

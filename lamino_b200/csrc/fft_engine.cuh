@@ -1,0 +1,236 @@
+// Shared-memory mixed-radix FFT engine for the Toeplitz apply (sm_100a).
+//
+// A length-n transform (n = product of radices in {2,3,4,5,8,9}) runs as
+// in-place decimation-in-frequency stages: stage s with radix r and block size
+// B_s = n / (r_0 ... r_{s-1}) combines the r elements base + m j (m = B_s / r),
+// applies an r-point DFT and the twiddles w_{B_s}^{n1 k}.  The output is left in
+// digit-reversed position order, which is never undone: the Toeplitz spectra
+// are stored in the same position order, and the inverse ("undo") runs the
+// stages backwards (conjugate twiddles, then an inverse r-point DFT), taking
+// positions back to natural order and returning n x (unnormalised).
+//
+// Transforms of zero-padded data (input length <= n/2) start with a radix-2
+// stage whose second input is zero; it is folded into the load, and the matching
+// last undo stage (outputs < n/2 only) into the store.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace lamino {
+
+constexpr int FFT_MAX_STAGES = 16;
+
+struct FftLen {  // POD, passed by value to kernels
+    int n, ns;
+    int radix[FFT_MAX_STAGES];
+    int bsz[FFT_MAX_STAGES];
+    const float2 *tw;  // exp(-2 pi i e / n), e in [0, n)
+};
+
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 c_mulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 c_rot(float2 a) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft3(float2 &x0, float2 &x1, float2 &x2) {
+    const float c = -0.5f, s = 0.86602540378443864676f;
+    float2 t = c_add(x1, x2);
+    float2 d = c_sub(x1, x2);
+    float2 y0 = c_add(x0, t);
+    float2 m = make_float2(fmaf(c, t.x, x0.x), fmaf(c, t.y, x0.y));
+    float2 r = c_rot<INV>(c_scale(d, s));  // -i s d (fwd) / +i s d (inv)
+    x0 = y0;
+    x1 = c_add(m, r);
+    x2 = c_sub(m, r);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &x0, float2 &x1, float2 &x2, float2 &x3) {
+    float2 a = c_add(x0, x2), b = c_sub(x0, x2);
+    float2 c = c_add(x1, x3), d = c_rot<INV>(c_sub(x1, x3));
+    x0 = c_add(a, c);
+    x2 = c_sub(a, c);
+    x1 = c_add(b, d);
+    x3 = c_sub(b, d);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft5(float2 (&v)[5]) {
+    const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
+    const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+    float2 a1 = c_add(v[1], v[4]), b1 = c_sub(v[1], v[4]);
+    float2 a2 = c_add(v[2], v[3]), b2 = c_sub(v[2], v[3]);
+    float2 y0 = c_add(v[0], c_add(a1, a2));
+    float2 m1 = make_float2(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    float2 m2 = make_float2(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    // -i (s1 b1 + s2 b2) and -i (s2 b1 - s1 b2) for the forward transform
+    float2 r1 = c_rot<INV>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+    float2 r2 = c_rot<INV>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+    v[0] = y0;
+    v[1] = c_add(m1, r1);
+    v[4] = c_sub(m1, r1);
+    v[2] = c_add(m2, r2);
+    v[3] = c_sub(m2, r2);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(float2 (&v)[8]) {
+    // y[k] = E[k mod 4] + W8^k O[k mod 4], E/O = 4-point DFTs of even/odd inputs
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    const float h = 0.70710678118654752440f;
+    // W8^1 = (1 - i)/sqrt2 (fwd), (1 + i)/sqrt2 (inv); W8^2 = -i / +i; W8^3 = (-1 - i)/sqrt2 / (-1 + i)/sqrt2
+    float2 t1 = INV ? make_float2(h * (o1.x - o1.y), h * (o1.x + o1.y)) : make_float2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    float2 t2 = c_rot<INV>(o2);
+    float2 t3 = INV ? make_float2(-h * (o3.x + o3.y), h * (o3.x - o3.y)) : make_float2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+    v[0] = c_add(e0, o0);
+    v[4] = c_sub(e0, o0);
+    v[1] = c_add(e1, t1);
+    v[5] = c_sub(e1, t1);
+    v[2] = c_add(e2, t2);
+    v[6] = c_sub(e2, t2);
+    v[3] = c_add(e3, t3);
+    v[7] = c_sub(e3, t3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft9(float2 (&v)[9]) {
+    // j = j1 + 3 j2, k = 3 k1 + k2: inner 3-point DFTs over j2, twiddle W9^{j1 k2}, outer over j1
+    float2 a[3][3];
+#pragma unroll
+    for (int j1 = 0; j1 < 3; ++j1) {
+        a[j1][0] = v[j1];
+        a[j1][1] = v[j1 + 3];
+        a[j1][2] = v[j1 + 6];
+        dft3<INV>(a[j1][0], a[j1][1], a[j1][2]);
+    }
+    const float c1 = 0.76604444311897803520f, s1 = 0.64278760968653932632f;   // W9^1
+    const float c2 = 0.17364817766693034885f, s2 = 0.98480775301220805936f;   // W9^2
+    const float c4 = -0.93969262078590838405f, s4 = 0.34202014332566873304f;  // W9^4
+    const float sg = INV ? 1.f : -1.f;
+    a[1][1] = c_mul(a[1][1], make_float2(c1, sg * s1));
+    a[1][2] = c_mul(a[1][2], make_float2(c2, sg * s2));
+    a[2][1] = c_mul(a[2][1], make_float2(c2, sg * s2));
+    a[2][2] = c_mul(a[2][2], make_float2(c4, sg * s4));
+#pragma unroll
+    for (int k2 = 0; k2 < 3; ++k2) {
+        float2 y0 = a[0][k2], y1 = a[1][k2], y2 = a[2][k2];
+        dft3<INV>(y0, y1, y2);
+        v[k2] = y0;
+        v[3 + k2] = y1;
+        v[6 + k2] = y2;
+    }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_small(float2 (&v)[R]) {
+    if constexpr (R == 2) {
+        float2 a = v[0];
+        v[0] = c_add(a, v[1]);
+        v[1] = c_sub(a, v[1]);
+    } else if constexpr (R == 3) {
+        dft3<INV>(v[0], v[1], v[2]);
+    } else if constexpr (R == 4) {
+        dft4<INV>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 5) {
+        dft5<INV>(v);
+    } else if constexpr (R == 8) {
+        dft8<INV>(v);
+    } else {
+        static_assert(R == 9, "unsupported radix");
+        dft9<INV>(v);
+    }
+}
+
+// One stage over P pencils of length n (pencil stride ps) in shared memory.
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(float2 *__restrict__ data, int P, int ps, int n, int B,
+                                          const float2 *__restrict__ tw, int tid, int nth) {
+    const int m = B / R;
+    const int nb = n / R;
+    const int ts = n / B;
+    const int total = P * nb;
+    for (int t = tid; t < total; t += nth) {
+        int pen = t / nb;
+        int u = t - pen * nb;
+        int b = u / m;
+        int n1 = u - b * m;
+        float2 *base = data + pen * ps + b * B + n1;
+        float2 v[R];
+        if constexpr (!INV) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[j] = base[m * j];
+            dft_small<R, false>(v);
+            if (n1 != 0) {
+#pragma unroll
+                for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], __ldg(tw + n1 * k * ts));
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) base[m * k] = v[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < R; ++k) v[k] = base[m * k];
+            if (n1 != 0) {
+#pragma unroll
+                for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], __ldg(tw + n1 * k * ts));
+            }
+            dft_small<R, true>(v);
+#pragma unroll
+            for (int j = 0; j < R; ++j) base[m * j] = v[j];
+        }
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void fft_stage_rt(int r, float2 *data, int P, int ps, int n, int B, const float2 *tw,
+                                             int tid, int nth) {
+    switch (r) {
+        case 2: fft_stage<2, INV>(data, P, ps, n, B, tw, tid, nth); break;
+        case 3: fft_stage<3, INV>(data, P, ps, n, B, tw, tid, nth); break;
+        case 4: fft_stage<4, INV>(data, P, ps, n, B, tw, tid, nth); break;
+        case 5: fft_stage<5, INV>(data, P, ps, n, B, tw, tid, nth); break;
+        case 8: fft_stage<8, INV>(data, P, ps, n, B, tw, tid, nth); break;
+        default: fft_stage<9, INV>(data, P, ps, n, B, tw, tid, nth); break;
+    }
+}
+
+// forward DIF stages s_begin .. ns-1 (caller synchronises before the call)
+__device__ __forceinline__ void fft_forward(float2 *data, int P, int ps, const FftLen &F, int s_begin, int tid,
+                                            int nth) {
+    for (int s = s_begin; s < F.ns; ++s) {
+        fft_stage_rt<false>(F.radix[s], data, P, ps, F.n, F.bsz[s], F.tw, tid, nth);
+        __syncthreads();
+    }
+}
+
+// undo stages ns-1 .. s_end (caller synchronises before the call)
+__device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const FftLen &F, int s_end, int tid,
+                                            int nth) {
+    for (int s = F.ns - 1; s >= s_end; --s) {
+        fft_stage_rt<true>(F.radix[s], data, P, ps, F.n, F.bsz[s], F.tw, tid, nth);
+        __syncthreads();
+    }
+}
+
+// ---- host-side schedule ----
+// Radix schedule for length n; lead2 puts a radix-2 stage first (zero-padded data).
+std::vector<int> fft_schedule(int n, bool lead2);
+// natural frequency k -> DIF output position
+std::vector<int> fft_positions(int n, const std::vector<int> &radix);
+
+}  // namespace lamino

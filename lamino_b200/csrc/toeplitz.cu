@@ -9,8 +9,14 @@
 //   D_n(s) = sin(pi s) / sin(pi s / n),
 // which is real and even, so its spectrum on an even embedding grid is real.
 // The kernel is evaluated in closed form (FP64 phase reduction, float sinpi),
-// never by spreading points, then transformed once; each apply is a zero-padded
-// R2C, a 3x3 symmetric multiply with 6 real spectra and a C2R plus crop.
+// never by spreading points, and transformed once (cuFFT, build only).  Each
+// apply is five kernels of this file over the zero-padded embedding, with the
+// padding never materialised: R2C rows along n3, a pruned FFT along n2, one
+// kernel per (k2, k3) pencil doing the n1 transform, the 3x3 multiply with the
+// 6 real spectra and the inverse n1 transform in shared memory, then the two
+// inverse passes.  Spectra and intermediates stay in digit-reversed position
+// order (fft_engine.cuh), so no pass reorders data.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -83,19 +89,30 @@ __global__ void __launch_bounds__(256) k_toeplitz_kernel(
     }
 }
 
-// K_q = Re(spectrum) * norm
-__global__ void k_take_real(const float2 *__restrict__ S, int64_t n, float norm, float *__restrict__ K) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        K[i] = S[i].x * norm;
+// ---------------------------------------------------------------------------
+// spectra in apply order
+// ---------------------------------------------------------------------------
+
+// K[(pen * 6 + q) * L1 + p1] = Re(S[(nat1[p1] * L2 + nat2[p2]) * L3h + k3]) * norm, pen = p2 * L3h + k3
+__global__ void k_take_real_perm(const float2 *__restrict__ S, int L1, int L2, int L3h, const int *__restrict__ nat1,
+                                 const int *__restrict__ nat2, int q, float norm, float *__restrict__ K) {
+    const int64_t total = (int64_t)L1 * L2 * L3h;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        int p1 = (int)(i % L1);
+        int64_t pen = i / L1;
+        int k3 = (int)(pen % L3h);
+        int p2 = (int)(pen / L3h);
+        float v = S[((int64_t)nat1[p1] * L2 + nat2[p2]) * L3h + k3].x * norm;
+        K[(pen * 6 + q) * L1 + p1] = v;
+    }
 }
 
-// per-k1-plane max |K| over the 6 spectra -> power-of-two scale; then fp16 store
-__global__ void k_plane_scale(const float *__restrict__ K, int64_t L1, int64_t plane, float *__restrict__ scale) {
-    int64_t k1 = blockIdx.x;
+// per-pencil max |K| over its 6 x L1 values -> power-of-two scale; fp16 store
+__global__ void k_pencil_scale(const float *__restrict__ K, int L1, float *__restrict__ scale) {
+    const int64_t pen = blockIdx.x;
+    const float *Kp = K + pen * 6 * L1;
     float m = 0.f;
-    for (int q = 0; q < 6; ++q)
-        for (int64_t i = threadIdx.x; i < plane; i += blockDim.x)
-            m = fmaxf(m, fabsf(K[(q * L1 + k1) * plane + i]));
+    for (int i = threadIdx.x; i < 6 * L1; i += blockDim.x) m = fmaxf(m, fabsf(Kp[i]));
     __shared__ float red[256];
     red[threadIdx.x] = m;
     __syncthreads();
@@ -104,78 +121,226 @@ __global__ void k_plane_scale(const float *__restrict__ K, int64_t L1, int64_t p
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        // map the plane maximum to at most 2^14 (well inside fp16's 65504)
         float mx = red[0];
-        float sc = 1.f;
-        if (mx > 0.f) sc = exp2f(floorf(log2f(mx)) - 14.f);
-        scale[k1] = sc;
+        scale[pen] = mx > 0.f ? exp2f(floorf(log2f(mx)) - 14.f) : 1.f;  // max maps below 2^15
     }
 }
 
-__global__ void k_to_half(const float *__restrict__ K, int64_t L1, int64_t plane, const float *__restrict__ scale,
+__global__ void k_to_half(const float *__restrict__ K, int64_t n, int L1, const float *__restrict__ scale,
                           __half *__restrict__ Kh) {
-    int64_t n = 6 * L1 * plane;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t k1 = (i / plane) % L1;
-        Kh[i] = __float2half_rn(K[i] / scale[k1]);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        Kh[i] = __float2half_rn(K[i] / scale[i / (6 * (int64_t)L1)]);
+}
+
+// ---------------------------------------------------------------------------
+// apply kernels
+// ---------------------------------------------------------------------------
+
+// A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
+// packed-complex M3-point DIF and the even/odd split.
+__global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
+                                                  const int *__restrict__ pos3, const float2 *__restrict__ twh,
+                                                  int R, float2 *__restrict__ z1) {
+    extern __shared__ float2 sm[];
+    const int M3 = F3.n, ps = M3 + 1;
+    const int64_t row0 = (int64_t)blockIdx.x * R;
+    const int nr = (int)min((int64_t)R, nrows - row0);
+    for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
+        int r = t / M3, m = t - r * M3;
+        const float *xr = x + (row0 + r) * n3;
+        int i = 2 * m;
+        sm[r * ps + m] = make_float2(i < n3 ? xr[i] : 0.f, i + 1 < n3 ? xr[i + 1] : 0.f);
+    }
+    __syncthreads();
+    fft_forward(sm, nr, ps, F3, 0, threadIdx.x, blockDim.x);
+    for (int t = threadIdx.x; t < nr * (M3 + 1); t += blockDim.x) {
+        int r = t / (M3 + 1), k = t - r * (M3 + 1);
+        int ka = (k == M3) ? 0 : k;
+        int kb = (k == 0) ? 0 : M3 - k;
+        float2 Zk = sm[r * ps + __ldg(pos3 + ka)];
+        float2 Zm = sm[r * ps + __ldg(pos3 + kb)];
+        Zm.y = -Zm.y;
+        float2 sum = c_add(Zk, Zm), dif = c_sub(Zk, Zm);
+        float2 wd = c_mul(__ldg(twh + k), dif);
+        // X = (sum - i w dif) / 2
+        z1[(row0 + r) * (M3 + 1) + k] = make_float2(0.5f * (sum.x + wd.y), 0.5f * (sum.y - wd.x));
     }
 }
 
-__global__ void k_pad3(const float *__restrict__ x, int n1, int n2, int n3, float *__restrict__ xp, int64_t L2,
-                       int64_t L3, int64_t LS) {
-    const int comp = blockIdx.y;
-    const int64_t V = (int64_t)n1 * n2 * n3;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        int i3 = (int)(idx % n3);
-        int64_t r = idx / n3;
-        int i2 = (int)(r % n2);
-        int i1 = (int)(r / n2);
-        xp[comp * LS + ((int64_t)i1 * L2 + i2) * L3 + i3] = x[comp * V + idx];
+// A2: columns along n2 (zero-padded to L2), KB k3 values per CTA; output pencil-major
+// xa[((c L2 + p2) L3h + k3) n1 + i1].
+__global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, FftLen F2,
+                                                  const float2 *__restrict__ tw2, int KB, float2 *__restrict__ xa) {
+    extern __shared__ float2 sm[];
+    const int i1 = blockIdx.x, k3b = blockIdx.y * KB, c = blockIdx.z;
+    const int nk = min(KB, L3h - k3b);
+    const int L2 = F2.n, ps = L2 + 1, half = L2 / 2;
+    const float2 *src = z1 + ((int64_t)c * n1 + i1) * n2 * L3h + k3b;
+    for (int t = threadIdx.x; t < half * nk; t += blockDim.x) {
+        int i2 = t / nk, kk = t - i2 * nk;
+        float2 v = i2 < n2 ? src[(int64_t)i2 * L3h + kk] : make_float2(0.f, 0.f);
+        sm[kk * ps + i2] = v;
+        sm[kk * ps + i2 + half] = c_mul(v, __ldg(tw2 + i2));
+    }
+    __syncthreads();
+    fft_forward(sm, nk, ps, F2, 1, threadIdx.x, blockDim.x);
+    for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
+        int p2 = t / nk, kk = t - p2 * nk;
+        xa[(((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1 + i1] = sm[kk * ps + p2];
     }
 }
 
-__global__ void k_crop3(const float *__restrict__ yp, int n1, int n2, int n3, int64_t L2, int64_t L3, int64_t LS,
-                        float *__restrict__ y) {
-    const int comp = blockIdx.y;
-    const int64_t V = (int64_t)n1 * n2 * n3;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < V;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        int i3 = (int)(idx % n3);
-        int64_t r = idx / n3;
-        int i2 = (int)(r % n2);
-        int i1 = (int)(r / n2);
-        y[comp * V + idx] = yp[comp * LS + ((int64_t)i1 * L2 + i2) * L3 + i3];
+// B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
+// symmetric multiply with the spectra (same position order), undo, first n1 kept.
+// In place on xa.
+template <bool HALF>
+__global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1, int L2, int L3h, FftLen F1,
+                                                const float2 *__restrict__ tw1, const float *__restrict__ K,
+                                                const __half *__restrict__ Kh, const float *__restrict__ kscale) {
+    extern __shared__ float2 sm[];
+    const int64_t pen = blockIdx.x;
+    const int p2 = (int)(pen / L3h), k3 = (int)(pen - (int64_t)p2 * L3h);
+    const int L1 = F1.n, half = L1 / 2;
+    const int64_t cs = (int64_t)L2 * L3h * n1;  // component stride in xa
+    float2 *pv = xa + ((int64_t)p2 * L3h + k3) * n1;
+    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
+        int c = t / half, i1 = t - c * half;
+        float2 v = i1 < n1 ? pv[c * cs + i1] : make_float2(0.f, 0.f);
+        sm[c * L1 + i1] = v;
+        sm[c * L1 + i1 + half] = c_mul(v, __ldg(tw1 + i1));
+    }
+    __syncthreads();
+    fft_forward(sm, 3, L1, F1, 1, threadIdx.x, blockDim.x);
+    const float sc = HALF ? kscale[pen] : 1.f;
+    for (int p1 = threadIdx.x; p1 < L1; p1 += blockDim.x) {
+        float k00, k11, k22, k01, k02, k12;
+        if (HALF) {
+            const __half *Kp = Kh + pen * 6 * L1 + p1;
+            k00 = __half2float(Kp[0]) * sc; k11 = __half2float(Kp[L1]) * sc; k22 = __half2float(Kp[2 * L1]) * sc;
+            k01 = __half2float(Kp[3 * L1]) * sc; k02 = __half2float(Kp[4 * L1]) * sc; k12 = __half2float(Kp[5 * L1]) * sc;
+        } else {
+            const float *Kp = K + pen * 6 * L1 + p1;
+            k00 = Kp[0]; k11 = Kp[L1]; k22 = Kp[2 * L1]; k01 = Kp[3 * L1]; k02 = Kp[4 * L1]; k12 = Kp[5 * L1];
+        }
+        float2 a = sm[p1], b = sm[L1 + p1], c = sm[2 * L1 + p1];
+        sm[p1] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
+        sm[L1 + p1] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
+        sm[2 * L1 + p1] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+    }
+    __syncthreads();
+    fft_inverse(sm, 3, L1, F1, 1, threadIdx.x, blockDim.x);
+    for (int t = threadIdx.x; t < 3 * n1; t += blockDim.x) {
+        int c = t / n1, i1 = t - c * n1;
+        pv[c * cs + i1] = c_add(sm[c * L1 + i1], c_mulc(sm[c * L1 + i1 + half], __ldg(tw1 + i1)));
     }
 }
 
-__global__ void k_mul_fp32(float2 *__restrict__ X, int64_t S, const float *__restrict__ K) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < S; i += (int64_t)gridDim.x * blockDim.x) {
-        float2 a = X[i], b = X[S + i], c = X[2 * S + i];
-        float k00 = K[i], k11 = K[S + i], k22 = K[2 * S + i];
-        float k01 = K[3 * S + i], k02 = K[4 * S + i], k12 = K[5 * S + i];
-        X[i] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
-        X[S + i] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
-        X[2 * S + i] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+// C2: undo along k2 (positions -> natural), first n2 rows kept, back into z1 rows
+__global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, FftLen F2,
+                                                  const float2 *__restrict__ tw2, int KB, float2 *__restrict__ z1) {
+    extern __shared__ float2 sm[];
+    const int i1 = blockIdx.x, k3b = blockIdx.y * KB, c = blockIdx.z;
+    const int nk = min(KB, L3h - k3b);
+    const int L2 = F2.n, ps = L2 + 1, half = L2 / 2;
+    for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
+        int p2 = t / nk, kk = t - p2 * nk;
+        sm[kk * ps + p2] = xa[(((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1 + i1];
+    }
+    __syncthreads();
+    fft_inverse(sm, nk, ps, F2, 1, threadIdx.x, blockDim.x);
+    float2 *dst = z1 + ((int64_t)c * n1 + i1) * n2 * L3h + k3b;
+    for (int t = threadIdx.x; t < n2 * nk; t += blockDim.x) {
+        int i2 = t / nk, kk = t - i2 * nk;
+        dst[(int64_t)i2 * L3h + kk] = c_add(sm[kk * ps + i2], c_mulc(sm[kk * ps + i2 + half], __ldg(tw2 + i2)));
     }
 }
 
-__global__ void k_mul_fp16(float2 *__restrict__ X, int64_t S, int64_t plane, const __half *__restrict__ K,
-                           const float *__restrict__ scale) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < S; i += (int64_t)gridDim.x * blockDim.x) {
-        float sc = scale[i / plane];
-        float2 a = X[i], b = X[S + i], c = X[2 * S + i];
-        float k00 = __half2float(K[i]) * sc, k11 = __half2float(K[S + i]) * sc, k22 = __half2float(K[2 * S + i]) * sc;
-        float k01 = __half2float(K[3 * S + i]) * sc, k02 = __half2float(K[4 * S + i]) * sc,
-              k12 = __half2float(K[5 * S + i]) * sc;
-        X[i] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
-        X[S + i] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
-        X[2 * S + i] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+// C1: half spectrum k3 in [0, M3] -> real rows (first n3 kept), the inverse of A1
+// returning L3 x (unnormalised; the 1/(L1 L2 L3) lives in the spectra).
+__global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1, int64_t nrows, int n3, FftLen F3,
+                                                  const int *__restrict__ pos3, const float2 *__restrict__ twh, int R,
+                                                  float *__restrict__ y) {
+    extern __shared__ float2 sm[];
+    const int M3 = F3.n, ps = M3 + 1;
+    const int64_t row0 = (int64_t)blockIdx.x * R;
+    const int nr = (int)min((int64_t)R, nrows - row0);
+    for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
+        int r = t / M3, k = t - r * M3;
+        const float2 *Xr = z1 + (row0 + r) * (M3 + 1);
+        float2 Xk = Xr[k], Xm = Xr[M3 - k];
+        Xm.y = -Xm.y;
+        float2 E = c_add(Xk, Xm);
+        float2 O = c_mulc(c_sub(Xk, Xm), __ldg(twh + k));
+        sm[r * ps + __ldg(pos3 + k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
     }
+    __syncthreads();
+    fft_inverse(sm, nr, ps, F3, 0, threadIdx.x, blockDim.x);
+    for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
+        int r = t / M3, m = t - r * M3;
+        float2 z = sm[r * ps + m];
+        float *yr = y + (row0 + r) * n3;
+        int i = 2 * m;
+        if (i < n3) yr[i] = z.x;
+        if (i + 1 < n3) yr[i + 1] = z.y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+std::vector<int> fft_schedule(int n, bool lead2) {
+    std::vector<int> r;
+    int m = n;
+    for (int q : {9, 8, 5, 4, 3, 2})
+        while (m % q == 0 && m > 1) { r.push_back(q); m /= q; }
+    if (m != 1) throw Error(ERR_ARG, "FFT length must be 2,3,5-smooth");
+    if (lead2) {
+        if (n % 2) throw Error(ERR_ARG, "zero-padded FFT length must be even");
+        auto it = std::find(r.begin(), r.end(), 2);
+        if (it != r.end()) r.erase(it);
+        else if ((it = std::find(r.begin(), r.end(), 4)) != r.end()) *it = 2;
+        else if ((it = std::find(r.begin(), r.end(), 8)) != r.end()) *it = 4;
+        r.insert(r.begin(), 2);
+    }
+    if ((int)r.size() > FFT_MAX_STAGES) throw Error(ERR_ARG, "FFT length has too many stages");
+    return r;
+}
+
+std::vector<int> fft_positions(int n, const std::vector<int> &radix) {
+    std::vector<int> pos(n, 0);
+    if (radix.empty()) return pos;
+    int r = radix[0], m = n / r;
+    std::vector<int> sub = fft_positions(m, std::vector<int>(radix.begin() + 1, radix.end()));
+    for (int k = 0; k < n; ++k) pos[k] = m * (k % r) + sub[k / r];
+    return pos;
+}
+
+static FftLen make_len(int n, bool lead2, DevBuf<float2> &tw, std::vector<int> *radix_out) {
+    std::vector<int> r = fft_schedule(n, lead2);
+    FftLen F{};
+    F.n = n;
+    F.ns = (int)r.size();
+    int b = n;
+    for (int s = 0; s < F.ns; ++s) {
+        F.radix[s] = r[s];
+        F.bsz[s] = b;
+        b /= r[s];
+    }
+    std::vector<float2> h(n);
+    for (int e = 0; e < n; ++e) {
+        double a = -2.0 * M_PI * (double)e / (double)n;
+        h[e] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    tw.alloc(n);
+    LAMINO_CUDA(cudaMemcpy(tw.p, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    F.tw = tw.p;
+    if (radix_out) *radix_out = r;
+    return F;
 }
 
 static int64_t embed_len(int64_t n) {
-    // smallest even 2,3,5-smooth L >= 2n  (L >= 2n-1 suffices for a linear convolution)
+    // smallest even 2,3,5-smooth L >= 2n (L >= 2n-1 suffices for a linear convolution)
     return next_smooth_even(2 * n);
 }
 
@@ -187,7 +352,36 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     L2 = embed_len(d.n2);
     L3 = embed_len(d.n3);
     L3h = L3 / 2 + 1;
+    M3 = L3 / 2;
     if (Lsize() > (int64_t)INT32_MAX) throw Error(ERR_ARG, "volume too large for the Toeplitz embedding");
+    if (3 * L1 * (int64_t)sizeof(float2) > 227 * 1024) throw Error(ERR_ARG, "n1 too large for the pencil kernel");
+
+    // FFT schedules, twiddles and position maps
+    std::vector<int> r1, r2, r3;
+    f1 = make_len((int)L1, true, tw1, &r1);
+    f2 = make_len((int)L2, true, tw2, &r2);
+    f3 = make_len((int)M3, false, tw3, &r3);
+    {
+        std::vector<float2> h(M3 + 1);
+        for (int64_t k = 0; k <= M3; ++k) {
+            double a = -2.0 * M_PI * (double)k / (double)L3;
+            h[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        twh3.alloc(M3 + 1);
+        LAMINO_CUDA(cudaMemcpy(twh3.p, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        std::vector<int> p3 = fft_positions((int)M3, r3);
+        pos3.alloc(M3);
+        LAMINO_CUDA(cudaMemcpy(pos3.p, p3.data(), M3 * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    std::vector<int> nat1(L1), nat2(L2);
+    {
+        std::vector<int> p1 = fft_positions((int)L1, r1), p2 = fft_positions((int)L2, r2);
+        for (int k = 0; k < (int)L1; ++k) nat1[p1[k]] = k;
+        for (int k = 0; k < (int)L2; ++k) nat2[p2[k]] = k;
+    }
+    DevBuf<int> dnat1(L1), dnat2(L2);
+    LAMINO_CUDA(cudaMemcpy(dnat1.p, nat1.data(), L1 * sizeof(int), cudaMemcpyHostToDevice));
+    LAMINO_CUDA(cudaMemcpy(dnat2.p, nat2.data(), L2 * sizeof(int), cudaMemcpyHostToDevice));
 
     // geometry tables in double
     std::vector<TGam> hg;
@@ -227,42 +421,57 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
         T.p, L1, L2, L3, (int)d.n1, (int)d.n2, (int)d.n3, dg.p, (int)hg.size(), dp.p);
     LAMINO_LAUNCH("k_toeplitz_kernel");
 
+    // one-off uniform R2C per pair (cuFFT), real part stored in apply order
+    FftPlan r2c;
     int n[3] = {(int)L1, (int)L2, (int)L3};
     LAMINO_CUFFT(cufftPlanMany(&r2c.h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, 1));
     r2c.valid = true;
-    LAMINO_CUFFT(cufftPlanMany(&c2r.h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 1));
-    c2r.valid = true;
     LAMINO_CUFFT(cufftSetStream(r2c.h, s));
-    LAMINO_CUFFT(cufftSetStream(c2r.h, s));
-
-    xhat.alloc(3 * Ssize());
+    DevBuf<float2> spec(Ssize());
     K.alloc(6 * Ssize());
     float norm = (float)(1.0 / ((double)L1 * L2 * L3));
     for (int q = 0; q < 6; ++q) {
-        LAMINO_CUFFT(cufftExecR2C(r2c.h, T.p + q * Lsize(), (cufftComplex *)xhat.p));
-        k_take_real<<<grid_for(Ssize(), 256), 256, 0, s>>>(xhat.p, Ssize(), norm, K.p + q * Ssize());
-        LAMINO_LAUNCH("k_take_real");
+        LAMINO_CUFFT(cufftExecR2C(r2c.h, T.p + q * Lsize(), (cufftComplex *)spec.p));
+        k_take_real_perm<<<grid_for(Ssize(), 256), 256, 0, s>>>(spec.p, (int)L1, (int)L2, (int)L3h, dnat1.p,
+                                                                 dnat2.p, q, norm, K.p);
+        LAMINO_LAUNCH("k_take_real_perm");
     }
     if (precision == PREC_FP16) {
         Kh.alloc(6 * Ssize());
-        Kscale.alloc(L1);
-        k_plane_scale<<<(unsigned)L1, 256, 0, s>>>(K.p, L1, L2 * L3h, Kscale.p);
-        LAMINO_LAUNCH("k_plane_scale");
-        k_to_half<<<grid_for(6 * Ssize(), 256), 256, 0, s>>>(K.p, L1, L2 * L3h, Kscale.p, Kh.p);
+        Kscale.alloc(L2 * L3h);
+        k_pencil_scale<<<(unsigned)(L2 * L3h), 256, 0, s>>>(K.p, (int)L1, Kscale.p);
+        LAMINO_LAUNCH("k_pencil_scale");
+        k_to_half<<<grid_for(6 * Ssize(), 256), 256, 0, s>>>(K.p, 6 * Ssize(), (int)L1, Kscale.p, Kh.p);
         LAMINO_LAUNCH("k_to_half");
-        LAMINO_CUDA(cudaStreamSynchronize(s));
-        K.release();
     }
     LAMINO_CUDA(cudaStreamSynchronize(s));
+    if (precision == PREC_FP16) K.release();
     T.release();
-    xpad.alloc(3 * Lsize());
-    LAMINO_CUDA(cudaMemsetAsync(xpad.p, 0, xpad.bytes(), s));
-    ypad.alloc(3 * Lsize());
-    LAMINO_CUDA(cudaStreamSynchronize(s));
+    spec.release();
+
+    // intermediates and launch shapes
+    z1.alloc(3 * d.n1 * d.n2 * L3h);
+    xa.alloc(3 * L2 * L3h * d.n1);
+    rows1 = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / (L3h * (int64_t)sizeof(float2))));
+    kb2 = (int)std::max<int64_t>(1, std::min<int64_t>(32, (64 * 1024) / ((L2 + 1) * (int64_t)sizeof(float2))));
+    const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
+    const int smem_d2 = kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
+    LAMINO_CUDA(cudaFuncSetAttribute(k_r2c_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
+    LAMINO_CUDA(cudaFuncSetAttribute(k_c2r_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
+    LAMINO_CUDA(cudaFuncSetAttribute(k_dim2_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_d2));
+    LAMINO_CUDA(cudaFuncSetAttribute(k_dim2_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_d2));
+    LAMINO_CUDA(cudaFuncSetAttribute(k_pencil<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_pen));
+    LAMINO_CUDA(cudaFuncSetAttribute(k_pencil<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_pen));
 }
 
 Toeplitz::~Toeplitz() {
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
+size_t Toeplitz::device_bytes() const {
+    return K.bytes() + Kh.bytes() + Kscale.bytes() + z1.bytes() + xa.bytes() + tw1.bytes() + tw2.bytes() +
+           tw3.bytes() + twh3.bytes() + pos3.bytes();
 }
 
 void Toeplitz::set_profiling(bool on, int max_applies) {
@@ -290,47 +499,51 @@ int Toeplitz::stage_times(double *ms) {
 }
 
 const char *Toeplitz::stage_name(int i) {
-    static const char *names[NSTAGE] = {"pad", "r2c", "multiply", "c2r", "crop"};
+    static const char *names[NSTAGE] = {"r2c_rows", "dim2_fwd", "pencil", "dim2_inv", "c2r_rows"};
     return (i >= 0 && i < NSTAGE) ? names[i] : "";
 }
 
 void Toeplitz::stage_bytes(int64_t *b) const {
-    const int64_t V = vol.size(), S = Ssize(), L = Lsize();
+    const int64_t V = vol.size();
+    const int64_t Z = 3 * vol.n1 * vol.n2 * L3h * 8;   // z1 bytes
+    const int64_t X = 3 * L2 * L3h * vol.n1 * 8;        // xa bytes
     const int64_t bk = precision == PREC_FP16 ? 2 : 4;
-    b[0] = 3 * V * 4 * 2;                    // read x, write the data box of xpad
-    b[1] = 3 * (L * 4 + S * 8);              // one pass: read real grid, write half-spectrum
-    b[2] = 3 * S * 8 * 2 + 6 * S * bk;       // read + write 3 spectra, read 6 kernel spectra
-    b[3] = 3 * (S * 8 + L * 4);              // one pass: read half-spectrum, write real grid
-    b[4] = 3 * V * 4 * 2;                    // read the data box of ypad, write y
+    b[0] = 3 * V * 4 + Z;                               // read x, write z1
+    b[1] = Z + X;                                       // read z1, write xa
+    b[2] = 2 * X + 6 * L2 * L3h * L1 * bk;              // read + write xa, read the 6 spectra
+    b[3] = X + Z;                                       // read xa, write z1
+    b[4] = Z + 3 * V * 4;                               // read z1, write y
 }
 
 void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
     const bool prof = profiling && (size_t)(nprof + 1) * (NSTAGE + 1) <= ev.size();
     cudaEvent_t *E = prof ? &ev[(size_t)nprof * (NSTAGE + 1)] : nullptr;
+    const int64_t nrows = 3 * vol.n1 * vol.n2;
+    const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
+    const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
+    const int smem_d2 = kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
+    const dim3 gd2((unsigned)vol.n1, (unsigned)((L3h + kb2 - 1) / kb2), 3);
     if (prof) LAMINO_CUDA(cudaEventRecord(E[0], s));
-    dim3 g3(grid_for(vol.size(), 256), 3);
-    k_pad3<<<g3, 256, 0, s>>>(x3, (int)vol.n1, (int)vol.n2, (int)vol.n3, xpad.p, L2, L3, Lsize());
-    LAMINO_LAUNCH("k_pad3");
+    k_r2c_rows<<<grows, 256, smem_rows, s>>>(x3, nrows, (int)vol.n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    LAMINO_LAUNCH("k_r2c_rows");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[1], s));
-    LAMINO_CUFFT(cufftSetStream(r2c.h, s));
-    LAMINO_CUFFT(cufftSetStream(c2r.h, s));
-    for (int c = 0; c < 3; ++c)
-        LAMINO_CUFFT(cufftExecR2C(r2c.h, xpad.p + c * Lsize(), (cufftComplex *)(xhat.p + c * Ssize())));
+    k_dim2_fwd<<<gd2, 256, smem_d2, s>>>(z1.p, (int)vol.n1, (int)vol.n2, (int)L3h, f2, tw2.p, kb2, xa.p);
+    LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
-    if (precision == PREC_FP16) {
-        k_mul_fp16<<<grid_for(Ssize(), 256), 256, 0, s>>>(xhat.p, Ssize(), L2 * L3h, Kh.p, Kscale.p);
-        LAMINO_LAUNCH("k_mul_fp16");
-    } else {
-        k_mul_fp32<<<grid_for(Ssize(), 256), 256, 0, s>>>(xhat.p, Ssize(), K.p);
-        LAMINO_LAUNCH("k_mul_fp32");
-    }
+    if (precision == PREC_FP16)
+        k_pencil<true><<<(unsigned)(L2 * L3h), 256, smem_pen, s>>>(xa.p, (int)vol.n1, (int)L2, (int)L3h, f1, tw1.p,
+                                                                   nullptr, Kh.p, Kscale.p);
+    else
+        k_pencil<false><<<(unsigned)(L2 * L3h), 256, smem_pen, s>>>(xa.p, (int)vol.n1, (int)L2, (int)L3h, f1, tw1.p,
+                                                                    K.p, nullptr, nullptr);
+    LAMINO_LAUNCH("k_pencil");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[3], s));
-    for (int c = 0; c < 3; ++c)
-        LAMINO_CUFFT(cufftExecC2R(c2r.h, (cufftComplex *)(xhat.p + c * Ssize()), ypad.p + c * Lsize()));
+    k_dim2_inv<<<gd2, 256, smem_d2, s>>>(xa.p, (int)vol.n1, (int)vol.n2, (int)L3h, f2, tw2.p, kb2, z1.p);
+    LAMINO_LAUNCH("k_dim2_inv");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[4], s));
-    dim3 gc(grid_for(vol.size(), 256), 3);
-    k_crop3<<<gc, 256, 0, s>>>(ypad.p, (int)vol.n1, (int)vol.n2, (int)vol.n3, L2, L3, Lsize(), y3);
-    LAMINO_LAUNCH("k_crop3");
+    k_c2r_rows<<<grows, 256, smem_rows, s>>>(z1.p, nrows, (int)vol.n3, f3, pos3.p, twh3.p, rows1, y3);
+    LAMINO_LAUNCH("k_c2r_rows");
     if (prof) {
         LAMINO_CUDA(cudaEventRecord(E[5], s));
         ++nprof;

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fft_engine.cuh"
 #include "geometry.cuh"
 
 namespace lamino {
@@ -15,18 +16,25 @@ enum Precision : int { PREC_FP32 = 0, PREC_FP16 = 1 };
 
 struct Toeplitz {
     Dims3 vol;
-    int64_t L1, L2, L3, L3h;     // embedding grid (even, 2,3,5-smooth, >= 2n) and L3/2+1
+    int64_t L1, L2, L3, L3h;     // embedding grid (even, 2,3,5-smooth, >= 2n); L3h = L3/2 + 1
+    int64_t M3;                  // L3 / 2 (packed-complex length of the real transform)
     int precision = PREC_FP32;
-    DevBuf<float> K;             // 6 real half-spectra (fp32), pair order 00,11,22,01,02,12
+    // spectra in apply order: [(p2 * L3h + k3) * 6 + q][p1], p = DIF position of k
+    DevBuf<float> K;             // fp32 storage
     DevBuf<__half> Kh;           // fp16 storage variant
-    DevBuf<float> Kscale;        // per-k1-plane power-of-two scales of Kh
-    DevBuf<float> xpad;          // 3 zero-padded real grids (zero outside the data box)
-    DevBuf<float2> xhat;         // 3 half-spectra
-    DevBuf<float> ypad;          // 3 real grids (C2R outputs)
-    FftPlan r2c, c2r;
+    DevBuf<float> Kscale;        // power-of-two scale per (p2, k3) pencil of Kh
+    // FFT schedules and twiddles: dim 1 (length L1), dim 2 (L2), dim 3 (packed, M3)
+    FftLen f1, f2, f3;
+    DevBuf<float2> tw1, tw2, tw3, twh3;  // twh3: exp(-2 pi i k / L3), k <= M3
+    DevBuf<int> pos3;                    // natural k -> DIF position, length M3
+    // intermediates
+    DevBuf<float2> z1;           // [3][n1][n2][L3h]   after the R2C along n3 (and before C2R)
+    DevBuf<float2> xa;           // [3][L2][L3h][n1]   spectra after dim 2, pencil-major
+    int kb2 = 32;                // k3 values per CTA in the dim-2 kernels
+    int rows1 = 8;               // rows per CTA in the dim-3 kernels
 
     // optional per-stage timing with CUDA events on the launching stream
-    static constexpr int NSTAGE = 5;  // pad, r2c, multiply, c2r, crop
+    static constexpr int NSTAGE = 5;  // r2c rows, dim2 fwd, pencil (fwd x K inv), dim2 inv, c2r rows
     bool profiling = false;
     std::vector<cudaEvent_t> ev;      // NSTAGE+1 events per profiled apply
     int nprof = 0;
@@ -43,7 +51,8 @@ struct Toeplitz {
     void stage_bytes(int64_t *b) const;
     static const char *stage_name(int i);
     // number of this library's kernels launched per apply
-    static int kernels_per_apply() { return 3; }
+    static int kernels_per_apply() { return NSTAGE; }
+    size_t device_bytes() const;
 };
 
 }  // namespace lamino
