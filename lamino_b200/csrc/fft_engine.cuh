@@ -227,6 +227,111 @@ __device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const F
     }
 }
 
+// ---- compile-time schedules for the lengths of the common problem sizes ----
+// (729 = packed n3 transform and 1458 = n1 transform of a 721-voxel axis; 144 =
+// n2 transform of a 71-voxel axis).  Other lengths use the runtime path above.
+template <int N>
+struct CtSched {
+    static constexpr int ns = 0;
+    static constexpr int r[4] = {0, 0, 0, 0};
+};
+template <>
+struct CtSched<729> {
+    static constexpr int ns = 3;
+    static constexpr int r[4] = {9, 9, 9, 0};
+};
+template <>
+struct CtSched<1458> {
+    static constexpr int ns = 4;
+    static constexpr int r[4] = {2, 9, 9, 9};
+};
+template <>
+struct CtSched<144> {
+    static constexpr int ns = 3;
+    static constexpr int r[4] = {2, 9, 8, 0};
+};
+
+template <int N>
+__host__ __device__ constexpr int ct_block(int s) {
+    int b = N;
+    for (int i = 0; i < s; ++i) b /= CtSched<N>::r[i];
+    return b;
+}
+
+// one stage with compile-time radix, length and block size
+template <int R, int N, int B, bool INV>
+__device__ __forceinline__ void fft_stage_fixed(float2 *__restrict__ data, int P, int ps,
+                                                const float2 *__restrict__ tw, int tid, int nth) {
+    constexpr int m = B / R;
+    constexpr int nb = N / R;
+    constexpr int ts = N / B;
+    const int total = P * nb;
+    for (int t = tid; t < total; t += nth) {
+        const int pen = t / nb;
+        const int u = t - pen * nb;
+        const int b = u / m;
+        const int n1 = u - b * m;
+        float2 *base = data + pen * ps + b * B + n1;
+        float2 v[R];
+        if constexpr (!INV) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[j] = base[m * j];
+            dft_small<R, false>(v);
+            if constexpr (m > 1) {
+                if (n1 != 0) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], __ldg(tw + n1 * k * ts));
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) base[m * k] = v[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < R; ++k) v[k] = base[m * k];
+            if constexpr (m > 1) {
+                if (n1 != 0) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], __ldg(tw + n1 * k * ts));
+                }
+            }
+            dft_small<R, true>(v);
+#pragma unroll
+            for (int j = 0; j < R; ++j) base[m * j] = v[j];
+        }
+    }
+}
+
+template <int N, int S>
+__device__ __forceinline__ void ct_forward(float2 *data, int P, int ps, const float2 *tw, int tid, int nth) {
+    if constexpr (S < CtSched<N>::ns) {
+        fft_stage_fixed<CtSched<N>::r[S], N, ct_block<N>(S), false>(data, P, ps, tw, tid, nth);
+        __syncthreads();
+        ct_forward<N, S + 1>(data, P, ps, tw, tid, nth);
+    }
+}
+
+// undo stages S, S-1, ..., S_END
+template <int N, int S, int S_END>
+__device__ __forceinline__ void ct_inverse(float2 *data, int P, int ps, const float2 *tw, int tid, int nth) {
+    if constexpr (S >= S_END) {
+        fft_stage_fixed<CtSched<N>::r[S], N, ct_block<N>(S), true>(data, P, ps, tw, tid, nth);
+        __syncthreads();
+        ct_inverse<N, S - 1, S_END>(data, P, ps, tw, tid, nth);
+    }
+}
+
+// Forward / inverse with a compile-time schedule when N != 0, else the runtime one.
+template <int N, int S_BEGIN>
+__device__ __forceinline__ void fft_fwd_any(float2 *data, int P, int ps, const FftLen &F, int tid, int nth) {
+    if constexpr (N == 0) fft_forward(data, P, ps, F, S_BEGIN, tid, nth);
+    else ct_forward<N, S_BEGIN>(data, P, ps, F.tw, tid, nth);
+}
+template <int N, int S_END>
+__device__ __forceinline__ void fft_inv_any(float2 *data, int P, int ps, const FftLen &F, int tid, int nth) {
+    if constexpr (N == 0) fft_inverse(data, P, ps, F, S_END, tid, nth);
+    else ct_inverse<N, CtSched<N>::ns - 1, S_END>(data, P, ps, F.tw, tid, nth);
+}
+
 // ---- host-side schedule ----
 // Radix schedule for length n; lead2 puts a radix-2 stage first (zero-padded data).
 std::vector<int> fft_schedule(int n, bool lead2);

@@ -137,12 +137,14 @@ __global__ void k_to_half(const float *__restrict__ K, int64_t n, int L1, const 
 // ---------------------------------------------------------------------------
 
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
-// packed-complex M3-point DIF and the even/odd split.
+// packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
+template <int N3>
 __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh,
                                                   int R, float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
-    const int M3 = F3.n, ps = M3 + 1;
+    const int M3 = N3 ? N3 : F3.n;
+    const int ps = M3 + 1;
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
     for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, i
         sm[r * ps + m] = make_float2(i < n3 ? xr[i] : 0.f, i + 1 < n3 ? xr[i + 1] : 0.f);
     }
     __syncthreads();
-    fft_forward(sm, nr, ps, F3, 0, threadIdx.x, blockDim.x);
+    fft_fwd_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
     for (int t = threadIdx.x; t < nr * (M3 + 1); t += blockDim.x) {
         int r = t / (M3 + 1), k = t - r * (M3 + 1);
         int ka = (k == M3) ? 0 : k;
@@ -167,42 +169,62 @@ __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, i
     }
 }
 
-// A2: columns along n2 (zero-padded to L2), KB k3 values per CTA; output pencil-major
-// xa[((c L2 + p2) L3h + k3) n1 + i1].
-__global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, FftLen F2,
-                                                  const float2 *__restrict__ tw2, int KB, float2 *__restrict__ xa) {
+// Tiles of the n2 passes: 8 consecutive i1 x KB consecutive k3 per CTA.  Shared
+// pencil p = ii * KB + kk has stride L2 + 1 (odd).  xa pencils have stride n1p
+// (a multiple of 8), so each thread moves its 8 i1 values as 64 aligned bytes.
+constexpr int D2_IB = 8;
+
+// A2: columns along n2 (zero-padded to L2) -> pencil-major xa[((c L2 + p2) L3h + k3) n1p + i1]
+template <int N2>
+__global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, int n1p,
+                                                  FftLen F2, const float2 *__restrict__ tw2, int KB,
+                                                  float2 *__restrict__ xa) {
     extern __shared__ float2 sm[];
-    const int i1 = blockIdx.x, k3b = blockIdx.y * KB, c = blockIdx.z;
+    const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
-    const int L2 = F2.n, ps = L2 + 1, half = L2 / 2;
-    const float2 *src = z1 + ((int64_t)c * n1 + i1) * n2 * L3h + k3b;
-    for (int t = threadIdx.x; t < half * nk; t += blockDim.x) {
-        int i2 = t / nk, kk = t - i2 * nk;
-        float2 v = i2 < n2 ? src[(int64_t)i2 * L3h + kk] : make_float2(0.f, 0.f);
-        sm[kk * ps + i2] = v;
-        sm[kk * ps + i2 + half] = c_mul(v, __ldg(tw2 + i2));
+    const int L2 = N2 ? N2 : F2.n;
+    const int ps = L2 + 1, half = L2 / 2;
+    // load: kk fastest (coalesced along k3)
+    for (int t = threadIdx.x; t < D2_IB * half * KB; t += blockDim.x) {
+        int kk = t % KB;
+        int r = t / KB;
+        int i2 = r % half;
+        int ii = r / half;
+        int i1 = i1b + ii;
+        float2 v = make_float2(0.f, 0.f);
+        if (kk < nk && i2 < n2 && i1 < n1) v = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
+        float2 *pp = sm + (ii * KB + kk) * ps;
+        pp[i2] = v;
+        pp[i2 + half] = c_mul(v, __ldg(tw2 + i2));
     }
     __syncthreads();
-    fft_forward(sm, nk, ps, F2, 1, threadIdx.x, blockDim.x);
+    fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
+    // store: one thread per (p2, kk) writes its 8 i1 values (64 B)
     for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
-        int p2 = t / nk, kk = t - p2 * nk;
-        xa[(((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1 + i1] = sm[kk * ps + p2];
+        int kk = t % nk, p2 = t / nk;
+        float4 *dst = reinterpret_cast<float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
+#pragma unroll
+        for (int h = 0; h < D2_IB / 2; ++h) {
+            float2 a = sm[((2 * h) * KB + kk) * ps + p2];
+            float2 b = sm[((2 * h + 1) * KB + kk) * ps + p2];
+            dst[h] = make_float4(a.x, a.y, b.x, b.y);
+        }
     }
 }
 
 // B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
 // symmetric multiply with the spectra (same position order), undo, first n1 kept.
-// In place on xa.
-template <bool HALF>
-__global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1, int L2, int L3h, FftLen F1,
+// In place on xa.  N1: compile-time L1 or 0.
+template <bool HALF, int N1>
+__global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
                                                 const float2 *__restrict__ tw1, const float *__restrict__ K,
                                                 const __half *__restrict__ Kh, const float *__restrict__ kscale) {
     extern __shared__ float2 sm[];
     const int64_t pen = blockIdx.x;
-    const int p2 = (int)(pen / L3h), k3 = (int)(pen - (int64_t)p2 * L3h);
-    const int L1 = F1.n, half = L1 / 2;
-    const int64_t cs = (int64_t)L2 * L3h * n1;  // component stride in xa
-    float2 *pv = xa + ((int64_t)p2 * L3h + k3) * n1;
+    const int L1 = N1 ? N1 : F1.n;
+    const int half = L1 / 2;
+    const int64_t cs = (int64_t)L2 * L3h * n1p;  // component stride in xa
+    float2 *pv = xa + pen * n1p;
     for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
         int c = t / half, i1 = t - c * half;
         float2 v = i1 < n1 ? pv[c * cs + i1] : make_float2(0.f, 0.f);
@@ -210,7 +232,7 @@ __global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1,
         sm[c * L1 + i1 + half] = c_mul(v, __ldg(tw1 + i1));
     }
     __syncthreads();
-    fft_forward(sm, 3, L1, F1, 1, threadIdx.x, blockDim.x);
+    fft_fwd_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
     const float sc = HALF ? kscale[pen] : 1.f;
     for (int p1 = threadIdx.x; p1 < L1; p1 += blockDim.x) {
         float k00, k11, k22, k01, k02, k12;
@@ -228,7 +250,7 @@ __global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1,
         sm[2 * L1 + p1] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
     }
     __syncthreads();
-    fft_inverse(sm, 3, L1, F1, 1, threadIdx.x, blockDim.x);
+    fft_inv_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
     for (int t = threadIdx.x; t < 3 * n1; t += blockDim.x) {
         int c = t / n1, i1 = t - c * n1;
         pv[c * cs + i1] = c_add(sm[c * L1 + i1], c_mulc(sm[c * L1 + i1 + half], __ldg(tw1 + i1)));
@@ -236,32 +258,58 @@ __global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1,
 }
 
 // C2: undo along k2 (positions -> natural), first n2 rows kept, back into z1 rows
-__global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, FftLen F2,
-                                                  const float2 *__restrict__ tw2, int KB, float2 *__restrict__ z1) {
+template <int N2>
+__global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, int n1p,
+                                                  FftLen F2, const float2 *__restrict__ tw2, int KB,
+                                                  float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
-    const int i1 = blockIdx.x, k3b = blockIdx.y * KB, c = blockIdx.z;
+    const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
-    const int L2 = F2.n, ps = L2 + 1, half = L2 / 2;
-    for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
-        int p2 = t / nk, kk = t - p2 * nk;
-        sm[kk * ps + p2] = xa[(((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1 + i1];
+    const int L2 = N2 ? N2 : F2.n;
+    const int ps = L2 + 1, half = L2 / 2;
+    // load: one thread per (p2, kk) reads its 8 i1 values (64 B)
+    for (int t = threadIdx.x; t < L2 * KB; t += blockDim.x) {
+        int kk = t % KB, p2 = t / KB;
+        if (kk < nk) {
+            const float4 *src =
+                reinterpret_cast<const float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
+#pragma unroll
+            for (int h = 0; h < D2_IB / 2; ++h) {
+                float4 q = src[h];
+                sm[((2 * h) * KB + kk) * ps + p2] = make_float2(q.x, q.y);
+                sm[((2 * h + 1) * KB + kk) * ps + p2] = make_float2(q.z, q.w);
+            }
+        } else {
+#pragma unroll
+            for (int ii = 0; ii < D2_IB; ++ii) sm[(ii * KB + kk) * ps + p2] = make_float2(0.f, 0.f);
+        }
     }
     __syncthreads();
-    fft_inverse(sm, nk, ps, F2, 1, threadIdx.x, blockDim.x);
-    float2 *dst = z1 + ((int64_t)c * n1 + i1) * n2 * L3h + k3b;
-    for (int t = threadIdx.x; t < n2 * nk; t += blockDim.x) {
-        int i2 = t / nk, kk = t - i2 * nk;
-        dst[(int64_t)i2 * L3h + kk] = c_add(sm[kk * ps + i2], c_mulc(sm[kk * ps + i2 + half], __ldg(tw2 + i2)));
+    fft_inv_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
+    // store: kk fastest (coalesced along k3)
+    for (int t = threadIdx.x; t < D2_IB * n2 * nk; t += blockDim.x) {
+        int kk = t % nk;
+        int r = t / nk;
+        int i2 = r % n2;
+        int ii = r / n2;
+        int i1 = i1b + ii;
+        if (i1 < n1) {
+            const float2 *pp = sm + (ii * KB + kk) * ps;
+            z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] =
+                c_add(pp[i2], c_mulc(pp[i2 + half], __ldg(tw2 + i2)));
+        }
     }
 }
 
 // C1: half spectrum k3 in [0, M3] -> real rows (first n3 kept), the inverse of A1
 // returning L3 x (unnormalised; the 1/(L1 L2 L3) lives in the spectra).
+template <int N3>
 __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh, int R,
                                                   float *__restrict__ y) {
     extern __shared__ float2 sm[];
-    const int M3 = F3.n, ps = M3 + 1;
+    const int M3 = N3 ? N3 : F3.n;
+    const int ps = M3 + 1;
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
     for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
@@ -274,7 +322,7 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
         sm[r * ps + __ldg(pos3 + k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
     }
     __syncthreads();
-    fft_inverse(sm, nr, ps, F3, 0, threadIdx.x, blockDim.x);
+    fft_inv_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
     for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
         int r = t / M3, m = t - r * M3;
         float2 z = sm[r * ps + m];
@@ -450,19 +498,33 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     spec.release();
 
     // intermediates and launch shapes
+    n1p = (d.n1 + D2_IB - 1) / D2_IB * D2_IB;
     z1.alloc(3 * d.n1 * d.n2 * L3h);
-    xa.alloc(3 * L2 * L3h * d.n1);
+    xa.alloc(3 * L2 * L3h * n1p);
     rows1 = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / (L3h * (int64_t)sizeof(float2))));
-    kb2 = (int)std::max<int64_t>(1, std::min<int64_t>(32, (64 * 1024) / ((L2 + 1) * (int64_t)sizeof(float2))));
+    kb2 = (int)std::min<int64_t>(8, (160 * 1024) / (D2_IB * (L2 + 1) * (int64_t)sizeof(float2)));
+    if (kb2 < 1) throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
+    ct1 = L1 == 1458 ? 1458 : 0;
+    ct2 = L2 == 144 ? 144 : 0;
+    ct3 = M3 == 729 ? 729 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * (int)(L2 + 1) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
-    LAMINO_CUDA(cudaFuncSetAttribute(k_r2c_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
-    LAMINO_CUDA(cudaFuncSetAttribute(k_c2r_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
-    LAMINO_CUDA(cudaFuncSetAttribute(k_dim2_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_d2));
-    LAMINO_CUDA(cudaFuncSetAttribute(k_dim2_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_d2));
-    LAMINO_CUDA(cudaFuncSetAttribute(k_pencil<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_pen));
-    LAMINO_CUDA(cudaFuncSetAttribute(k_pencil<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_pen));
+    auto attr = [](const void *f, int bytes) {
+        LAMINO_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    };
+    attr((const void *)k_r2c_rows<0>, smem_rows);
+    attr((const void *)k_r2c_rows<729>, smem_rows);
+    attr((const void *)k_c2r_rows<0>, smem_rows);
+    attr((const void *)k_c2r_rows<729>, smem_rows);
+    attr((const void *)k_dim2_fwd<0>, smem_d2);
+    attr((const void *)k_dim2_fwd<144>, smem_d2);
+    attr((const void *)k_dim2_inv<0>, smem_d2);
+    attr((const void *)k_dim2_inv<144>, smem_d2);
+    attr((const void *)k_pencil<false, 0>, smem_pen);
+    attr((const void *)k_pencil<true, 0>, smem_pen);
+    attr((const void *)k_pencil<false, 1458>, smem_pen);
+    attr((const void *)k_pencil<true, 1458>, smem_pen);
 }
 
 Toeplitz::~Toeplitz() {
@@ -506,7 +568,7 @@ const char *Toeplitz::stage_name(int i) {
 void Toeplitz::stage_bytes(int64_t *b) const {
     const int64_t V = vol.size();
     const int64_t Z = 3 * vol.n1 * vol.n2 * L3h * 8;   // z1 bytes
-    const int64_t X = 3 * L2 * L3h * vol.n1 * 8;        // xa bytes
+    const int64_t X = 3 * L2 * L3h * vol.n1 * 8;        // xa bytes (the n1p padding is not counted)
     const int64_t bk = precision == PREC_FP16 ? 2 : 4;
     b[0] = 3 * V * 4 + Z;                               // read x, write z1
     b[1] = Z + X;                                       // read z1, write xa
@@ -521,28 +583,37 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
     const int64_t nrows = 3 * vol.n1 * vol.n2;
     const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * (int)(L2 + 1) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
-    const dim3 gd2((unsigned)vol.n1, (unsigned)((L3h + kb2 - 1) / kb2), 3);
+    const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
+    const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
+    const unsigned gpen = (unsigned)(L2 * L3h);
     if (prof) LAMINO_CUDA(cudaEventRecord(E[0], s));
-    k_r2c_rows<<<grows, 256, smem_rows, s>>>(x3, nrows, (int)vol.n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    if (ct3) k_r2c_rows<729><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[1], s));
-    k_dim2_fwd<<<gd2, 256, smem_d2, s>>>(z1.p, (int)vol.n1, (int)vol.n2, (int)L3h, f2, tw2.p, kb2, xa.p);
+    if (ct2) k_dim2_fwd<144><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
-    if (precision == PREC_FP16)
-        k_pencil<true><<<(unsigned)(L2 * L3h), 256, smem_pen, s>>>(xa.p, (int)vol.n1, (int)L2, (int)L3h, f1, tw1.p,
-                                                                   nullptr, Kh.p, Kscale.p);
+    const bool h = precision == PREC_FP16;
+    if (ct1 && h)
+        k_pencil<true, 1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
+    else if (ct1)
+        k_pencil<false, 1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
+    else if (h)
+        k_pencil<true, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
     else
-        k_pencil<false><<<(unsigned)(L2 * L3h), 256, smem_pen, s>>>(xa.p, (int)vol.n1, (int)L2, (int)L3h, f1, tw1.p,
-                                                                    K.p, nullptr, nullptr);
+        k_pencil<false, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
     LAMINO_LAUNCH("k_pencil");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[3], s));
-    k_dim2_inv<<<gd2, 256, smem_d2, s>>>(xa.p, (int)vol.n1, (int)vol.n2, (int)L3h, f2, tw2.p, kb2, z1.p);
+    if (ct2) k_dim2_inv<144><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
+    else k_dim2_inv<0><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
     LAMINO_LAUNCH("k_dim2_inv");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[4], s));
-    k_c2r_rows<<<grows, 256, smem_rows, s>>>(z1.p, nrows, (int)vol.n3, f3, pos3.p, twh3.p, rows1, y3);
+    if (ct3) k_c2r_rows<729><<<grows, 256, smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
+    else k_c2r_rows<0><<<grows, 256, smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
     LAMINO_LAUNCH("k_c2r_rows");
     if (prof) {
         LAMINO_CUDA(cudaEventRecord(E[5], s));

@@ -29,9 +29,11 @@ struct Toeplitz {
     DevBuf<int> pos3;                    // natural k -> DIF position, length M3
     // intermediates
     DevBuf<float2> z1;           // [3][n1][n2][L3h]   after the R2C along n3 (and before C2R)
-    DevBuf<float2> xa;           // [3][L2][L3h][n1]   spectra after dim 2, pencil-major
-    int kb2 = 32;                // k3 values per CTA in the dim-2 kernels
+    DevBuf<float2> xa;           // [3][L2][L3h][n1p]  spectra after dim 2, pencil-major
+    int64_t n1p = 0;             // pencil stride: n1 rounded up to a multiple of 8
+    int kb2 = 8;                 // k3 values per CTA in the dim-2 kernels (x 8 i1 values)
     int rows1 = 8;               // rows per CTA in the dim-3 kernels
+    int ct1 = 0, ct2 = 0, ct3 = 0;  // compile-time FFT lengths in use (0 = runtime schedule)
 
     // optional per-stage timing with CUDA events on the launching stream
     static constexpr int NSTAGE = 5;  // r2c rows, dim2 fwd, pencil (fwd x K inv), dim2 inv, c2r rows

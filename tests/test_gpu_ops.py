@@ -175,3 +175,21 @@ def test_full_size_toeplitz_properties(L):
     ys = T(xs)
     yn = L.sysmat(xs, pgs)
     assert (torch.linalg.norm(ys - yn) / torch.linalg.norm(yn)).item() < 1e-4
+
+
+@pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721)])
+def test_toeplitz_compiled_fft_lengths(L, O, dims):
+    """Thin volumes whose FFT lengths hit the compile-time schedules (n1 = 721 ->
+    1458, n2 = 71 -> 144, n3 = 721 -> packed 729) against the oracle.  The
+    Toeplitz form evaluates the exact lattice, so the oracle here uses FP64
+    points (the reference's double path): with white input on a 721-long axis
+    the float32 points of the float path move the highest modes' phases by about
+    k * ulp and differ from it by 2.5e-5."""
+    rng = np.random.default_rng(16)
+    th = rng.uniform(0, 2 * np.pi, 4).astype(np.float32)
+    pg = L.PolarGrid(th, 13, 11, np.float32(0.7))
+    opg = O.PolarGrid(th, 13, 11, np.float32(0.7), dtype=np.float64)
+    x = rng.standard_normal((3,) + dims).astype(np.float32)
+    want = O.sysmat(x, opg, opg.gamma, O.NufftPlan(dims, exact=True))
+    assert rel(L.ToeplitzNormal([pg], dims)(x), want) < TOL
+    assert rel(L.ToeplitzNormal([pg], dims, "fp16")(x), want) < 2e-3
