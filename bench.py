@@ -38,7 +38,11 @@ DET_PADDED = 1233
 SCALES = {"full": ((721, 71, 721), 361, 1233), "half": ((361, 36, 361), 181, 617),
           "quarter": ((181, 18, 181), 91, 309),
           # same n1 (FFT length 1458) as the full case, thin in n2/n3: > L2 but < 1 GB
-          "pencil": ((721, 18, 360), 45, 309)}
+          "pencil": ((721, 18, 360), 45, 309),
+          # n1 = 721, n2 = 71 as the full case (compile-time n1 / n2 FFT lengths), n3 thin: < 2 GB
+          "pencil2": ((721, 71, 180), 45, 309),
+          # n2 = 71, n3 = 721 as the full case (compile-time n2 / n3 lengths), n1 thin: < 2 GB
+          "rows": ((181, 71, 721), 45, 309)}
 
 
 def workload_config(precision: str, n: int):

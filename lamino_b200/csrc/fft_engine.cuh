@@ -137,6 +137,22 @@ __device__ __forceinline__ void dft9(float2 (&v)[9]) {
     }
 }
 
+// w^k for k = 1..R-1 from two table loads (w = tw[e], w4 = tw[4e] when R > 4),
+// every power at most two complex products away from a loaded value.
+template <int R>
+__device__ __forceinline__ void twiddle_powers(const float2 *__restrict__ tw, int e, float2 (&w)[R]) {
+    w[1] = __ldg(tw + e);
+    if constexpr (R > 2) w[2] = c_mul(w[1], w[1]);
+    if constexpr (R > 3) w[3] = c_mul(w[2], w[1]);
+    if constexpr (R > 4) {
+        w[4] = __ldg(tw + 4 * e);
+        if constexpr (R > 5) w[5] = c_mul(w[4], w[1]);
+        if constexpr (R > 6) w[6] = c_mul(w[4], w[2]);
+        if constexpr (R > 7) w[7] = c_mul(w[4], w[3]);
+        if constexpr (R > 8) w[8] = c_mul(w[4], w[4]);
+    }
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft_small(float2 (&v)[R]) {
     if constexpr (R == 2) {
@@ -248,7 +264,7 @@ struct CtSched<1458> {
 template <>
 struct CtSched<144> {
     static constexpr int ns = 3;
-    static constexpr int r[4] = {2, 9, 8, 0};
+    static constexpr int r[4] = {2, 8, 9, 0};
 };
 
 template <int N>
@@ -279,8 +295,10 @@ __device__ __forceinline__ void fft_stage_fixed(float2 *__restrict__ data, int P
             dft_small<R, false>(v);
             if constexpr (m > 1) {
                 if (n1 != 0) {
+                    float2 w[R];
+                    twiddle_powers<R>(tw, n1 * ts, w);
 #pragma unroll
-                    for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], __ldg(tw + n1 * k * ts));
+                    for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], w[k]);
                 }
             }
 #pragma unroll
@@ -290,8 +308,10 @@ __device__ __forceinline__ void fft_stage_fixed(float2 *__restrict__ data, int P
             for (int k = 0; k < R; ++k) v[k] = base[m * k];
             if constexpr (m > 1) {
                 if (n1 != 0) {
+                    float2 w[R];
+                    twiddle_powers<R>(tw, n1 * ts, w);
 #pragma unroll
-                    for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], __ldg(tw + n1 * k * ts));
+                    for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], w[k]);
                 }
             }
             dft_small<R, true>(v);

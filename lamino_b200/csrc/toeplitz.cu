@@ -169,10 +169,13 @@ __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, i
     }
 }
 
-// Tiles of the n2 passes: 8 consecutive i1 x KB consecutive k3 per CTA.  Shared
-// pencil p = ii * KB + kk has stride L2 + 1 (odd).  xa pencils have stride n1p
-// (a multiple of 8), so each thread moves its 8 i1 values as 64 aligned bytes.
+// Tiles of the n2 passes: 8 consecutive i1 x KB (8) consecutive k3 per CTA.  Shared
+// pencil p = ii * KB + kk has stride ps = L2 + pad with ps = 2 (mod 16), so the 16
+// lanes of each 8-byte shared access phase (8 kk x 2 rows) hit distinct banks in the
+// load, FFT and transpose phases.  xa pencils have stride n1p (a multiple of 8), so
+// each thread moves its 8 i1 values as 64 aligned bytes.
 constexpr int D2_IB = 8;
+__host__ __device__ constexpr int d2_stride(int L2) { return L2 + (((2 - L2) % 16) + 16) % 16; }
 
 // A2: columns along n2 (zero-padded to L2) -> pencil-major xa[((c L2 + p2) L3h + k3) n1p + i1]
 template <int N2>
@@ -183,19 +186,35 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
     const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
-    const int ps = L2 + 1, half = L2 / 2;
-    // load: kk fastest (coalesced along k3)
-    for (int t = threadIdx.x; t < D2_IB * half * KB; t += blockDim.x) {
-        int kk = t % KB;
-        int r = t / KB;
-        int i2 = r % half;
-        int ii = r / half;
-        int i1 = i1b + ii;
-        float2 v = make_float2(0.f, 0.f);
-        if (kk < nk && i2 < n2 && i1 < n1) v = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
-        float2 *pp = sm + (ii * KB + kk) * ps;
-        pp[i2] = v;
-        pp[i2 + half] = c_mul(v, __ldg(tw2 + i2));
+    const int ps = d2_stride(L2), half = L2 / 2;
+    // load: kk fastest (coalesced along k3); 4 independent loads in flight per thread
+    const int total = D2_IB * half * KB;
+    for (int t0 = threadIdx.x; t0 < total; t0 += 4 * blockDim.x) {
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int t = t0 + u * blockDim.x;
+            int kk = t % KB;
+            int r = t / KB;
+            int i2 = r % half;
+            int i1 = i1b + r / half;
+            v[u] = make_float2(0.f, 0.f);
+            if (t < total && kk < nk && i2 < n2 && i1 < n1)
+                v[u] = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int t = t0 + u * blockDim.x;
+            if (t < total) {
+                int kk = t % KB;
+                int r = t / KB;
+                int i2 = r % half;
+                int ii = r / half;
+                float2 *pp = sm + (ii * KB + kk) * ps;
+                pp[i2] = v[u];
+                pp[i2 + half] = c_mul(v[u], __ldg(tw2 + i2));
+            }
+        }
     }
     __syncthreads();
     fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
@@ -266,7 +285,7 @@ __global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa,
     const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
-    const int ps = L2 + 1, half = L2 / 2;
+    const int ps = d2_stride(L2), half = L2 / 2;
     // load: one thread per (p2, kk) reads its 8 i1 values (64 B)
     for (int t = threadIdx.x; t < L2 * KB; t += blockDim.x) {
         int kk = t % KB, p2 = t / KB;
@@ -349,8 +368,11 @@ std::vector<int> fft_schedule(int n, bool lead2) {
         if (it != r.end()) r.erase(it);
         else if ((it = std::find(r.begin(), r.end(), 4)) != r.end()) *it = 2;
         else if ((it = std::find(r.begin(), r.end(), 8)) != r.end()) *it = 4;
-        r.insert(r.begin(), 2);
     }
+    // even radices first, odd ones last: the last stages read with stride = radix,
+    // which is conflict-free in 8-byte shared-memory banks only when it is odd
+    std::stable_sort(r.begin(), r.end(), [](int a, int b) { return (a % 2 == 0) && (b % 2 == 1); });
+    if (lead2) r.insert(r.begin(), 2);
     if ((int)r.size() > FFT_MAX_STAGES) throw Error(ERR_ARG, "FFT length has too many stages");
     return r;
 }
@@ -502,13 +524,13 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     z1.alloc(3 * d.n1 * d.n2 * L3h);
     xa.alloc(3 * L2 * L3h * n1p);
     rows1 = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / (L3h * (int64_t)sizeof(float2))));
-    kb2 = (int)std::min<int64_t>(8, (160 * 1024) / (D2_IB * (L2 + 1) * (int64_t)sizeof(float2)));
+    kb2 = (int)std::min<int64_t>(8, (160 * 1024) / (D2_IB * d2_stride((int)L2) * (int64_t)sizeof(float2)));
     if (kb2 < 1) throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
     ct1 = L1 == 1458 ? 1458 : 0;
     ct2 = L2 == 144 ? 144 : 0;
     ct3 = M3 == 729 ? 729 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     auto attr = [](const void *f, int bytes) {
         LAMINO_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -583,7 +605,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
     const int64_t nrows = 3 * vol.n1 * vol.n2;
     const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * (int)(L2 + 1) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
