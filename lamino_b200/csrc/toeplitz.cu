@@ -136,6 +136,9 @@ __global__ void k_to_half(const float *__restrict__ K, int64_t n, int L1, const 
 // apply kernels
 // ---------------------------------------------------------------------------
 
+// independent global loads kept in flight per thread in the load phases
+constexpr int LD_BATCH = 8;
+
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
@@ -147,11 +150,27 @@ __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, i
     const int ps = M3 + 1;
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
-    for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
-        int r = t / M3, m = t - r * M3;
-        const float *xr = x + (row0 + r) * n3;
-        int i = 2 * m;
-        sm[r * ps + m] = make_float2(i < n3 ? xr[i] : 0.f, i + 1 < n3 ? xr[i + 1] : 0.f);
+    {
+        const int total = nr * M3;
+        const float *xb = x + row0 * n3;
+        for (int t0 = threadIdx.x; t0 < total; t0 += LD_BATCH * blockDim.x) {
+            float2 v[LD_BATCH];
+#pragma unroll
+            for (int u = 0; u < LD_BATCH; ++u) {
+                int t = t0 + u * blockDim.x;
+                int r = t / M3, m = t - r * M3, i = 2 * m;
+                v[u].x = (t < total && i < n3) ? xb[(int64_t)r * n3 + i] : 0.f;
+                v[u].y = (t < total && i + 1 < n3) ? xb[(int64_t)r * n3 + i + 1] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < LD_BATCH; ++u) {
+                int t = t0 + u * blockDim.x;
+                if (t < total) {
+                    int r = t / M3;
+                    sm[r * ps + (t - r * M3)] = v[u];
+                }
+            }
+        }
     }
     __syncthreads();
     fft_fwd_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
@@ -175,7 +194,11 @@ __global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, i
 // load, FFT and transpose phases.  xa pencils have stride n1p (a multiple of 8), so
 // each thread moves its 8 i1 values as 64 aligned bytes.
 constexpr int D2_IB = 8;
-__host__ __device__ constexpr int d2_stride(int L2) { return L2 + (((2 - L2) % 16) + 16) % 16; }
+// shared pencil stride for KB k3 values per tile: ps = 16 / KB (mod 16)
+__host__ __device__ constexpr int d2_stride(int L2, int KB) {
+    return L2 + ((((16 / KB) - L2) % 16) + 16) % 16;
+}
+
 
 // A2: columns along n2 (zero-padded to L2) -> pencil-major xa[((c L2 + p2) L3h + k3) n1p + i1]
 template <int N2>
@@ -186,13 +209,13 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
     const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
-    const int ps = d2_stride(L2), half = L2 / 2;
-    // load: kk fastest (coalesced along k3); 4 independent loads in flight per thread
+    const int ps = d2_stride(L2, KB), half = L2 / 2;
+    // load: kk fastest (coalesced along k3); LD_BATCH independent loads in flight per thread
     const int total = D2_IB * half * KB;
-    for (int t0 = threadIdx.x; t0 < total; t0 += 4 * blockDim.x) {
-        float2 v[4];
+    for (int t0 = threadIdx.x; t0 < total; t0 += LD_BATCH * blockDim.x) {
+        float2 v[LD_BATCH];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < LD_BATCH; ++u) {
             int t = t0 + u * blockDim.x;
             int kk = t % KB;
             int r = t / KB;
@@ -203,7 +226,7 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
                 v[u] = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < LD_BATCH; ++u) {
             int t = t0 + u * blockDim.x;
             if (t < total) {
                 int kk = t % KB;
@@ -244,29 +267,57 @@ __global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1,
     const int half = L1 / 2;
     const int64_t cs = (int64_t)L2 * L3h * n1p;  // component stride in xa
     float2 *pv = xa + pen * n1p;
-    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
-        int c = t / half, i1 = t - c * half;
-        float2 v = i1 < n1 ? pv[c * cs + i1] : make_float2(0.f, 0.f);
-        sm[c * L1 + i1] = v;
-        sm[c * L1 + i1 + half] = c_mul(v, __ldg(tw1 + i1));
+    for (int t0 = threadIdx.x; t0 < 3 * half; t0 += LD_BATCH * blockDim.x) {
+        float2 v[LD_BATCH];
+#pragma unroll
+        for (int u = 0; u < LD_BATCH; ++u) {
+            int t = t0 + u * blockDim.x;
+            int c = t / half, i1 = t - c * half;
+            v[u] = (t < 3 * half && i1 < n1) ? pv[c * cs + i1] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < LD_BATCH; ++u) {
+            int t = t0 + u * blockDim.x;
+            if (t < 3 * half) {
+                int c = t / half, i1 = t - c * half;
+                sm[c * L1 + i1] = v[u];
+                sm[c * L1 + i1 + half] = c_mul(v[u], __ldg(tw1 + i1));
+            }
+        }
     }
     __syncthreads();
     fft_fwd_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
     const float sc = HALF ? kscale[pen] : 1.f;
-    for (int p1 = threadIdx.x; p1 < L1; p1 += blockDim.x) {
-        float k00, k11, k22, k01, k02, k12;
-        if (HALF) {
-            const __half *Kp = Kh + pen * 6 * L1 + p1;
-            k00 = __half2float(Kp[0]) * sc; k11 = __half2float(Kp[L1]) * sc; k22 = __half2float(Kp[2 * L1]) * sc;
-            k01 = __half2float(Kp[3 * L1]) * sc; k02 = __half2float(Kp[4 * L1]) * sc; k12 = __half2float(Kp[5 * L1]) * sc;
-        } else {
-            const float *Kp = K + pen * 6 * L1 + p1;
-            k00 = Kp[0]; k11 = Kp[L1]; k22 = Kp[2 * L1]; k01 = Kp[3 * L1]; k02 = Kp[4 * L1]; k12 = Kp[5 * L1];
+    constexpr int KU = 2;  // p1 values whose 6 spectra are in flight together
+    for (int q0 = threadIdx.x; q0 < L1; q0 += KU * blockDim.x) {
+        float kv[KU][6];
+#pragma unroll
+        for (int u = 0; u < KU; ++u) {
+            int p1 = q0 + u * blockDim.x;
+            if (p1 < L1) {
+                if (HALF) {
+                    const __half *Kp = Kh + pen * 6 * L1 + p1;
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) kv[u][q] = __half2float(Kp[q * L1]) * sc;
+                } else {
+                    const float *Kp = K + pen * 6 * L1 + p1;
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) kv[u][q] = Kp[q * L1];
+                }
+            }
         }
-        float2 a = sm[p1], b = sm[L1 + p1], c = sm[2 * L1 + p1];
-        sm[p1] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
-        sm[L1 + p1] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
-        sm[2 * L1 + p1] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+#pragma unroll
+        for (int u = 0; u < KU; ++u) {
+            int p1 = q0 + u * blockDim.x;
+            if (p1 < L1) {
+                const float k00 = kv[u][0], k11 = kv[u][1], k22 = kv[u][2], k01 = kv[u][3], k02 = kv[u][4],
+                            k12 = kv[u][5];
+                float2 a = sm[p1], b = sm[L1 + p1], c = sm[2 * L1 + p1];
+                sm[p1] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
+                sm[L1 + p1] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
+                sm[2 * L1 + p1] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+            }
+        }
     }
     __syncthreads();
     fft_inv_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
@@ -285,22 +336,35 @@ __global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa,
     const int i1b = blockIdx.x * D2_IB, k3b = blockIdx.y * KB, c = blockIdx.z;
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
-    const int ps = d2_stride(L2), half = L2 / 2;
-    // load: one thread per (p2, kk) reads its 8 i1 values (64 B)
-    for (int t = threadIdx.x; t < L2 * KB; t += blockDim.x) {
-        int kk = t % KB, p2 = t / KB;
-        if (kk < nk) {
-            const float4 *src =
-                reinterpret_cast<const float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
+    const int ps = d2_stride(L2, KB), half = L2 / 2;
+    // load: one thread per (p2, kk) reads its 8 i1 values (64 B); two tasks in flight
+    for (int t0 = threadIdx.x; t0 < L2 * KB; t0 += 2 * blockDim.x) {
+        float4 q[2][D2_IB / 2];
 #pragma unroll
-            for (int h = 0; h < D2_IB / 2; ++h) {
-                float4 q = src[h];
-                sm[((2 * h) * KB + kk) * ps + p2] = make_float2(q.x, q.y);
-                sm[((2 * h + 1) * KB + kk) * ps + p2] = make_float2(q.z, q.w);
+        for (int u = 0; u < 2; ++u) {
+            int t = t0 + u * blockDim.x;
+            int kk = t % KB, p2 = t / KB;
+            if (t < L2 * KB && kk < nk) {
+                const float4 *src =
+                    reinterpret_cast<const float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
+#pragma unroll
+                for (int h = 0; h < D2_IB / 2; ++h) q[u][h] = src[h];
+            } else {
+#pragma unroll
+                for (int h = 0; h < D2_IB / 2; ++h) q[u][h] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-        } else {
+        }
 #pragma unroll
-            for (int ii = 0; ii < D2_IB; ++ii) sm[(ii * KB + kk) * ps + p2] = make_float2(0.f, 0.f);
+        for (int u = 0; u < 2; ++u) {
+            int t = t0 + u * blockDim.x;
+            if (t < L2 * KB) {
+                int kk = t % KB, p2 = t / KB;
+#pragma unroll
+                for (int h = 0; h < D2_IB / 2; ++h) {
+                    sm[((2 * h) * KB + kk) * ps + p2] = make_float2(q[u][h].x, q[u][h].y);
+                    sm[((2 * h + 1) * KB + kk) * ps + p2] = make_float2(q[u][h].z, q[u][h].w);
+                }
+            }
         }
     }
     __syncthreads();
@@ -331,14 +395,29 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
     const int ps = M3 + 1;
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
-    for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
-        int r = t / M3, k = t - r * M3;
-        const float2 *Xr = z1 + (row0 + r) * (M3 + 1);
-        float2 Xk = Xr[k], Xm = Xr[M3 - k];
-        Xm.y = -Xm.y;
-        float2 E = c_add(Xk, Xm);
-        float2 O = c_mulc(c_sub(Xk, Xm), __ldg(twh + k));
-        sm[r * ps + __ldg(pos3 + k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+    for (int t0 = threadIdx.x; t0 < nr * M3; t0 += LD_BATCH * blockDim.x) {
+        float2 Xk[LD_BATCH], Xm[LD_BATCH];
+#pragma unroll
+        for (int u = 0; u < LD_BATCH; ++u) {
+            int t = t0 + u * blockDim.x;
+            int r = t / M3, k = t - r * M3;
+            if (t < nr * M3) {
+                const float2 *Xr = z1 + (row0 + r) * (M3 + 1);
+                Xk[u] = Xr[k];
+                Xm[u] = Xr[M3 - k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LD_BATCH; ++u) {
+            int t = t0 + u * blockDim.x;
+            if (t < nr * M3) {
+                int r = t / M3, k = t - r * M3;
+                float2 xm = make_float2(Xm[u].x, -Xm[u].y);
+                float2 E = c_add(Xk[u], xm);
+                float2 O = c_mulc(c_sub(Xk[u], xm), __ldg(twh + k));
+                sm[r * ps + __ldg(pos3 + k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+            }
+        }
     }
     __syncthreads();
     fft_inv_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
@@ -524,13 +603,15 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     z1.alloc(3 * d.n1 * d.n2 * L3h);
     xa.alloc(3 * L2 * L3h * n1p);
     rows1 = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / (L3h * (int64_t)sizeof(float2))));
-    kb2 = (int)std::min<int64_t>(8, (160 * 1024) / (D2_IB * d2_stride((int)L2) * (int64_t)sizeof(float2)));
-    if (kb2 < 1) throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
+    kb2 = 4;
+    while (kb2 > 1 && D2_IB * kb2 * d2_stride((int)L2, kb2) * (int64_t)sizeof(float2) > 160 * 1024) kb2 /= 2;
+    if (D2_IB * kb2 * d2_stride((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
+        throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
     ct1 = L1 == 1458 ? 1458 : 0;
     ct2 = L2 == 144 ? 144 : 0;
     ct3 = M3 == 729 ? 729 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     auto attr = [](const void *f, int bytes) {
         LAMINO_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -605,7 +686,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
     const int64_t nrows = 3 * vol.n1 * vol.n2;
     const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2) * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
