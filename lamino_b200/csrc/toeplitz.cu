@@ -142,7 +142,7 @@ constexpr int LD_BATCH = 8;
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
-__global__ void __launch_bounds__(256) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
+__global__ void __launch_bounds__(256, 6) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh,
                                                   int R, float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
@@ -210,12 +210,13 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
     const int ps = d2_stride(L2, KB), half = L2 / 2;
-    // load: kk fastest (coalesced along k3); LD_BATCH independent loads in flight per thread
+    // load: kk fastest (coalesced along k3); D2_BATCH independent loads in flight per thread
+    constexpr int D2_BATCH = 4;
     const int total = D2_IB * half * KB;
-    for (int t0 = threadIdx.x; t0 < total; t0 += LD_BATCH * blockDim.x) {
-        float2 v[LD_BATCH];
+    for (int t0 = threadIdx.x; t0 < total; t0 += D2_BATCH * blockDim.x) {
+        float2 v[D2_BATCH];
 #pragma unroll
-        for (int u = 0; u < LD_BATCH; ++u) {
+        for (int u = 0; u < D2_BATCH; ++u) {
             int t = t0 + u * blockDim.x;
             int kk = t % KB;
             int r = t / KB;
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
                 v[u] = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
         }
 #pragma unroll
-        for (int u = 0; u < LD_BATCH; ++u) {
+        for (int u = 0; u < D2_BATCH; ++u) {
             int t = t0 + u * blockDim.x;
             if (t < total) {
                 int kk = t % KB;
