@@ -106,10 +106,12 @@ int lamino_residual_noalloc(lamino_plan_t p, lamino_geom_t g, const float *f3, c
 /* ---- Toeplitz normal operator ----------------------------------------------
  * sum_gamma sysmat as a 3x3 block convolution (no reference counterpart; it
  * replaces the MBIR `A` closures src/mbir_cg.cpp:97-105, src/mbir_sb.cpp:89-97).
- * precision: 0 = FP32 spectra, 1 = FP16 spectra with per-plane power-of-two scales.
+ * precision: 0 = FP32 spectra, 1 = FP16 spectra with a power-of-two scale per
+ * (k2, k3) pencil, 2 = both.
  */
 #define LAMINO_PREC_FP32 0
 #define LAMINO_PREC_FP16 1
+#define LAMINO_PREC_MIXED 2 /* both spectra; lamino_normal_apply uses the FP32 ones */
 int lamino_normal_create(const lamino_geom_t *geoms, int ngeom, int64_t n1, int64_t n2, int64_t n3, int precision,
                          lamino_normal_t *out, void *stream);
 int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *stream);
@@ -165,13 +167,16 @@ int lamino_lipschitz(lamino_op_t A, int64_t n1, int64_t n2, int64_t n3, int max_
  * tomocam::MBIR1 / MBIR2 / MBIR3 (include/tomocam.h:101-154; src/mbir_cg.cpp:48-128,
  * src/mbir_sb.cpp:47-114, src/mbir3.cpp:47-135).  Fields default as
  * tomocam::ReconParams (include/config.h:146-158); lamino_recon_params_default fills them.
- * op_kind: 0 Toeplitz FP32, 1 Toeplitz FP16 spectra, 2 NUFFT form.
+ * op_kind: 0 Toeplitz FP32, 1 Toeplitz FP16 spectra, 2 NUFFT form, 3 mixed (FP16
+ * correction solves inside `refinements` FP32-residual refinement cycles per
+ * linear solve; MBIR1 and MBIR2).
  */
 typedef struct {
     int max_iters, inner_iters;
     float sigma, p, lambda, mu, tol, xtol, pad_factor;
     int op_kind;
     double eps;
+    int refinements;
 } lamino_recon_params;
 void lamino_recon_params_default(lamino_recon_params *p);
 /* method 1, 2 or 3.  projs[i]: [proj_dims[3i]][proj_dims[3i+1]][proj_dims[3i+2]];

@@ -298,7 +298,7 @@ class ToeplitzNormal:
         self.grids = list(grids)
         gp, keep = _geom_array(self.grids)
         h = ctypes.c_void_p()
-        prec = {"fp32": 0, "fp16": 1}[precision]
+        prec = {"fp32": 0, "fp16": 1, "mixed": 2}[precision]
         _check(lib().lamino_normal_create(gp, len(self.grids), *self.dims, prec, ctypes.byref(h),
                                           stream or ctypes.c_void_p(0)))
         self._h = h
@@ -446,12 +446,14 @@ class _ReconParamsC(ctypes.Structure):
     _fields_ = [("max_iters", ctypes.c_int), ("inner_iters", ctypes.c_int),
                 ("sigma", ctypes.c_float), ("p", ctypes.c_float), ("lam", ctypes.c_float),
                 ("mu", ctypes.c_float), ("tol", ctypes.c_float), ("xtol", ctypes.c_float),
-                ("pad_factor", ctypes.c_float), ("op_kind", ctypes.c_int), ("eps", ctypes.c_double)]
+                ("pad_factor", ctypes.c_float), ("op_kind", ctypes.c_int), ("eps", ctypes.c_double),
+                ("refinements", ctypes.c_int)]
 
 
 class ReconParams:
     """tomocam::ReconParams defaults (include/config.h:146-158) plus the operator
-    form: op_kind 'toeplitz' (FP32 spectra), 'toeplitz_fp16' or 'nufft'."""
+    form: op_kind 'toeplitz' (FP32 spectra), 'toeplitz_fp16', 'nufft' or 'mixed'
+    (FP16 correction solves in `refinements` FP32-residual cycles)."""
 
     def __init__(self, **kw):
         c = _ReconParamsC()
@@ -459,15 +461,15 @@ class ReconParams:
         self.maxIters, self.innerIters = c.max_iters, c.inner_iters
         self.sigma, self.p, self.lam, self.mu = c.sigma, c.p, c.lam, c.mu
         self.tol, self.xtol, self.PAD_FACTOR = c.tol, c.xtol, c.pad_factor
-        self.op_kind, self.eps = "toeplitz", c.eps
+        self.op_kind, self.eps, self.refinements = "toeplitz", c.eps, c.refinements
         for k, v in kw.items():
             setattr(self, k, v)
 
     def _c(self):
-        kind = {"toeplitz": 0, "toeplitz_fp16": 1, "nufft": 2}[self.op_kind]
+        kind = {"toeplitz": 0, "toeplitz_fp16": 1, "nufft": 2, "mixed": 3}[self.op_kind]
         return _ReconParamsC(int(self.maxIters), int(self.innerIters), float(self.sigma), float(self.p),
                              float(self.lam), float(self.mu), float(self.tol), float(self.xtol),
-                             float(self.PAD_FACTOR), kind, float(self.eps))
+                             float(self.PAD_FACTOR), kind, float(self.eps), int(self.refinements))
 
 
 def _mbir(method, datasets, recon_dims, params):

@@ -496,6 +496,7 @@ void lamino_recon_params_default(lamino_recon_params *p) {
     p->pad_factor = d.pad_factor;
     p->op_kind = d.op_kind;
     p->eps = d.eps;
+    p->refinements = d.refinements;
 }
 
 int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *pdims, const float *const *angles,
@@ -516,6 +517,7 @@ int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *p
     prm.pad_factor = params->pad_factor;
     prm.op_kind = params->op_kind;
     prm.eps = params->eps;
+    prm.refinements = params->refinements;
     std::vector<std::unique_ptr<In<float>>> ins;
     std::vector<Dataset> data;
     for (int i = 0; i < nds; ++i) {

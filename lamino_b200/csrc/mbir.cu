@@ -4,6 +4,7 @@
 // operations and its quirks (different projection padding for MBIR1 vs 2/3,
 // yT subtracted once per gamma in the MBIR3 gradient, `mu` passed as the
 // Lipschitz constant, per-component square roots in the MBIR3 loss).
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -104,20 +105,29 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
 
     // normal operator sum_gamma sysmat
     std::unique_ptr<Toeplitz> T;
-    OpFn A;
+    OpFn A, A_lo;
+    const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
     if (prm.op_kind == OP_NUFFT) {
         A = [&](const float *x, float *y, cudaStream_t st) { plan.normal(gptr, x, y, st); };
     } else {
-        T.reset(new Toeplitz(gptr, od, prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : PREC_FP32, s));
-        A = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st); };
+        int prec = prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : (mixed ? PREC_MIXED : PREC_FP32);
+        T.reset(new Toeplitz(gptr, od, prec, s));
+        A = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st, false); };
+        if (mixed) A_lo = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st, true); };
     }
 
     DevBuf<float> x(n);
     LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));
     if (method == 1) {
-        cgsolver(A, yT.p, x.p, od, prm.max_iters, prm.tol, s);
+        if (mixed) {
+            int R = std::max(1, prm.refinements);
+            cgsolver_refined(A, A_lo, yT.p, x.p, od, std::max(1, prm.max_iters / R), R, prm.tol, s);
+        } else {
+            cgsolver(A, yT.p, x.p, od, prm.max_iters, prm.tol, s);
+        }
     } else if (method == 2) {
-        split_bregman(A, yT.p, x.p, od, prm.lambda, prm.mu, prm.max_iters, prm.inner_iters, prm.tol, prm.xtol, s);
+        split_bregman_refined(A, A_lo, mixed ? std::max(1, prm.refinements) : 0, yT.p, x.p, od, prm.lambda, prm.mu,
+                              prm.max_iters, prm.inner_iters, prm.tol, prm.xtol, s);
     } else {
         // per-gamma operators for the loss (sum over gamma of per-component sqrt terms)
         std::vector<std::unique_ptr<Toeplitz>> Tg;

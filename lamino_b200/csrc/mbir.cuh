@@ -12,7 +12,9 @@
 
 namespace lamino {
 
-enum OpKind : int { OP_TOEPLITZ_FP32 = 0, OP_TOEPLITZ_FP16 = 1, OP_NUFFT = 2 };
+// Toeplitz with FP32 spectra, with FP16 spectra, the NUFFT form, or Toeplitz with
+// both spectra (FP16 correction solves inside FP32-residual refinement cycles).
+enum OpKind : int { OP_TOEPLITZ_FP32 = 0, OP_TOEPLITZ_FP16 = 1, OP_NUFFT = 2, OP_TOEPLITZ_MIXED = 3 };
 
 struct ReconParams {  // include/config.h:146-158 defaults
     int max_iters = 50;
@@ -21,6 +23,7 @@ struct ReconParams {  // include/config.h:146-158 defaults
     float pad_factor = 1.4142f;
     int op_kind = OP_TOEPLITZ_FP32;
     double eps = 1.2e-6;
+    int refinements = 3;  // refinement cycles per linear solve with OP_TOEPLITZ_MIXED
 };
 
 struct Dataset {

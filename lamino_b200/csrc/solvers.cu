@@ -368,10 +368,18 @@ __global__ void k_cg_dir(float *__restrict__ p, const float *__restrict__ z, flo
 }
 
 CgStats cgsolver(const OpFn &A, const float *y3, float *x3, Dims3 d, int max_iter, float tol, cudaStream_t s) {
+    CgWork w(d);
+    CgStats st = cgsolver(A, y3, x3, w, max_iter, tol, s);
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    return st;
+}
+
+CgStats cgsolver(const OpFn &A, const float *y3, float *x3, CgWork &w, int max_iter, float tol, cudaStream_t s) {
+    const Dims3 d = w.d;
     const int64_t n = 3 * d.size();
-    DevBuf<float> r(n), p(n), z(n), Ap(n);
-    RampPrecond M(d);
-    Reducer red(4);
+    DevBuf<float> &r = w.r, &p = w.p, &z = w.z, &Ap = w.Ap;
+    RampPrecond &M = w.M;
+    Reducer &red = w.red;
     CgStats st;
     A(x3, Ap.p, s);
     vec_lin2(r.p, 1.f, y3, -1.f, Ap.p, n, s);
@@ -407,12 +415,49 @@ CgStats cgsolver(const OpFn &A, const float *y3, float *x3, Dims3 d, int max_ite
     return st;
 }
 
+CgStats cgsolver_refined(const OpFn &A_hi, const OpFn &A_lo, const float *y3, float *x3, Dims3 d, int inner,
+                         int refinements, float tol, cudaStream_t s) {
+    CgWork w(d);
+    CgStats st = cgsolver_refined(A_hi, A_lo, y3, x3, w, inner, refinements, tol, s);
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    return st;
+}
+
+CgStats cgsolver_refined(const OpFn &A_hi, const OpFn &A_lo, const float *y3, float *x3, CgWork &w, int inner,
+                         int refinements, float tol, cudaStream_t s) {
+    const int64_t n = 3 * w.d.size();
+    if (w.e1.n != (size_t)n) w.e1.alloc(n);
+    if (w.e2.n != (size_t)n) w.e2.alloc(n);
+    DevBuf<float> &r = w.e1, &dx = w.e2;
+    Reducer &red = w.red;
+    CgStats st;
+    for (int k = 0; k < refinements; ++k) {
+        A_hi(x3, r.p, s);
+        vec_lin2(r.p, 1.f, y3, -1.f, r.p, n, s);  // r = y - A_hi x
+        red.zero(1, s);
+        vec_dot(r.p, r.p, n, red.d, s);
+        red.fetch(1, s);
+        st.last_res = std::sqrt(red.h[0]);
+        if (st.last_res < tol) break;
+        LAMINO_CUDA(cudaMemsetAsync(dx.p, 0, dx.bytes(), s));
+        CgStats in = cgsolver(A_lo, r.p, dx.p, w, inner, tol, s);
+        st.iters += in.iters;
+        vec_lin2(x3, 1.f, x3, 1.f, dx.p, n, s);
+    }
+    return st;
+}
+
 // ---------------------------------------------------------------------------
 // split Bregman (src/bregman.cpp:39-134)
 // ---------------------------------------------------------------------------
 
 int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam, float mu, int outer_max,
                   int inner_max, float tol, float xtol, cudaStream_t s) {
+    return split_bregman_refined(A, OpFn(), 0, yT3, x3, d, lam, mu, outer_max, inner_max, tol, xtol, s);
+}
+
+int split_bregman_refined(const OpFn &A, const OpFn &A_lo, int refinements, const float *yT3, float *x3, Dims3 d,
+                          float lam, float mu, int outer_max, int inner_max, float tol, float xtol, cudaStream_t s) {
     const int64_t V = d.size(), n = 3 * V;
     DevBuf<float> xold(n), dd(9 * V), bb(9 * V), rhs(n);
     LAMINO_CUDA(cudaMemcpyAsync(xold.p, x3, n * 4, cudaMemcpyDeviceToDevice, s));
@@ -422,13 +467,21 @@ int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam
         A(u, out, st);
         laplacian_axpy(out, mu, u, d, st);
     };
+    OpFn Ap_lo = [&](const float *u, float *out, cudaStream_t st) {
+        A_lo(u, out, st);
+        laplacian_axpy(out, mu, u, d, st);
+    };
     Reducer red(8);
+    CgWork work(d);
     int it = 0;
     for (; it < outer_max; ++it) {
         sb_rhs(yT3, dd.p, bb.p, mu, d, rhs.p, s);
         // x = cgsolver(Ap, rhs, x_old, ...)
         LAMINO_CUDA(cudaMemcpyAsync(x3, xold.p, n * 4, cudaMemcpyDeviceToDevice, s));
-        cgsolver(Ap, rhs.p, x3, d, inner_max, tol, s);
+        if (A_lo && refinements > 0)
+            cgsolver_refined(Ap, Ap_lo, rhs.p, x3, work, inner_max, refinements, tol, s);
+        else
+            cgsolver(Ap, rhs.p, x3, work, inner_max, tol, s);
         sb_shrink(x3, dd.p, bb.p, lam, mu, d, s);
         red.zero(6, s);
         vec_sqdist3(x3, xold.p, V, red.d, s);

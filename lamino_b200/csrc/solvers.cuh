@@ -55,10 +55,35 @@ struct RampPrecond {
 
 // ---- solver loops (host control flow mirrors the reference) ----
 struct CgStats { int iters = 0; double last_res = 0; };
+
+// Buffers, ramp preconditioner (cuFFT plans) and reduction slots of one PCG,
+// allocated once per solve so repeated calls (split-Bregman inner solves,
+// refinement cycles) allocate and free nothing.
+struct CgWork {
+    Dims3 d;
+    DevBuf<float> r, p, z, Ap, e1, e2;  // e1, e2: refinement residual / correction
+    RampPrecond M;
+    Reducer red;
+    explicit CgWork(Dims3 dd)
+        : d(dd), r(3 * dd.size()), p(3 * dd.size()), z(3 * dd.size()), Ap(3 * dd.size()), M(dd), red(4) {}
+};
+
 // src/conjgrad.cpp:37-117.  x3 holds x0 on entry and the solution on exit.
 CgStats cgsolver(const OpFn &A, const float *y3, float *x3, Dims3 d, int max_iter, float tol, cudaStream_t s);
+CgStats cgsolver(const OpFn &A, const float *y3, float *x3, CgWork &w, int max_iter, float tol, cudaStream_t s);
 
-// src/bregman.cpp:39-134.  x3 in/out.
+// Mixed-precision PCG: `refinements` cycles of  r = y - A_hi x  (FP32 operator,
+// FP64 reductions), then `inner` PCG iterations on A_lo d = r from d = 0, x += d.
+CgStats cgsolver_refined(const OpFn &A_hi, const OpFn &A_lo, const float *y3, float *x3, Dims3 d, int inner,
+                         int refinements, float tol, cudaStream_t s);
+CgStats cgsolver_refined(const OpFn &A_hi, const OpFn &A_lo, const float *y3, float *x3, CgWork &w, int inner,
+                         int refinements, float tol, cudaStream_t s);
+
+// src/bregman.cpp:39-134.  x3 in/out.  With A_lo set, each outer iteration solves
+// its linear subproblem as x_old + d, d from PCG on A_lo against the residual of
+// A (refinement cycles as cgsolver_refined).
+int split_bregman_refined(const OpFn &A, const OpFn &A_lo, int refinements, const float *yT3, float *x3, Dims3 d,
+                          float lam, float mu, int outer_max, int inner_max, float tol, float xtol, cudaStream_t s);
 int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam, float mu, int outer_max,
                   int inner_max, float tol, float xtol, cudaStream_t s);
 

@@ -497,7 +497,8 @@ static int64_t embed_len(int64_t n) {
 Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaStream_t s) : vol(d), precision(prec) {
     if (gs.empty()) throw Error(ERR_ARG, "Toeplitz operator needs at least one geometry");
     if (d.n1 <= 0 || d.n2 <= 0 || d.n3 <= 0) throw Error(ERR_ARG, "volume dims must be positive");
-    if (prec != PREC_FP32 && prec != PREC_FP16) throw Error(ERR_ARG, "precision must be 0 (fp32) or 1 (fp16)");
+    if (prec != PREC_FP32 && prec != PREC_FP16 && prec != PREC_MIXED)
+        throw Error(ERR_ARG, "precision must be 0 (fp32), 1 (fp16) or 2 (mixed)");
     L1 = embed_len(d.n1);
     L2 = embed_len(d.n2);
     L3 = embed_len(d.n3);
@@ -586,7 +587,7 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
                                                                  dnat2.p, q, norm, K.p);
         LAMINO_LAUNCH("k_take_real_perm");
     }
-    if (precision == PREC_FP16) {
+    if (precision != PREC_FP32) {
         Kh.alloc(6 * Ssize());
         Kscale.alloc(L2 * L3h);
         k_pencil_scale<<<(unsigned)(L2 * L3h), 256, 0, s>>>(K.p, (int)L1, Kscale.p);
@@ -673,7 +674,7 @@ void Toeplitz::stage_bytes(int64_t *b) const {
     const int64_t V = vol.size();
     const int64_t Z = 3 * vol.n1 * vol.n2 * L3h * 8;   // z1 bytes
     const int64_t X = 3 * L2 * L3h * vol.n1 * 8;        // xa bytes (the n1p padding is not counted)
-    const int64_t bk = precision == PREC_FP16 ? 2 : 4;
+    const int64_t bk = precision == PREC_FP32 ? 4 : 2;
     b[0] = 3 * V * 4 + Z;                               // read x, write z1
     b[1] = Z + X;                                       // read z1, write xa
     b[2] = 2 * X + 6 * L2 * L3h * L1 * bk;              // read + write xa, read the 6 spectra
@@ -681,7 +682,7 @@ void Toeplitz::stage_bytes(int64_t *b) const {
     b[4] = Z + 3 * V * 4;                               // read z1, write y
 }
 
-void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
+void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     const bool prof = profiling && (size_t)(nprof + 1) * (NSTAGE + 1) <= ev.size();
     cudaEvent_t *E = prof ? &ev[(size_t)nprof * (NSTAGE + 1)] : nullptr;
     const int64_t nrows = 3 * vol.n1 * vol.n2;
@@ -701,7 +702,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s) {
     else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
-    const bool h = precision == PREC_FP16;
+    const bool h = precision == PREC_FP16 || (precision == PREC_MIXED && low);
     if (ct1 && h)
         k_pencil<true, 1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
     else if (ct1)

@@ -12,7 +12,9 @@
 
 namespace lamino {
 
-enum Precision : int { PREC_FP32 = 0, PREC_FP16 = 1 };
+// FP32 spectra, FP16 spectra, or both (mixed: FP32 for refinement residuals,
+// FP16 for the correction solves).
+enum Precision : int { PREC_FP32 = 0, PREC_FP16 = 1, PREC_MIXED = 2 };
 
 struct Toeplitz {
     Dims3 vol;
@@ -45,7 +47,10 @@ struct Toeplitz {
     ~Toeplitz();
     int64_t Lsize() const { return L1 * L2 * L3; }
     int64_t Ssize() const { return L1 * L2 * L3h; }
-    void apply(const float *x3, float *y3, cudaStream_t s);
+    // low = true applies with the FP16 spectra (PREC_FP16 always does; PREC_MIXED on request)
+    void apply(const float *x3, float *y3, cudaStream_t s, bool low = false);
+    bool has_fp32() const { return K.p != nullptr; }
+    bool has_fp16() const { return Kh.p != nullptr; }
     void set_profiling(bool on, int max_applies);
     // accumulated stage milliseconds over profiled applies; returns count
     int stage_times(double *ms);

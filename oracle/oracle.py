@@ -547,6 +547,18 @@ def cgsolver(A: Callable, y, x0, max_iter: int, tol: float, precond=None, log=No
     return x
 
 
+def cgsolver_refined(A_hi: Callable, A_lo: Callable, y, x0, inner: int, refinements: int, tol: float):
+    """Iterative refinement around PCG (this project's mixed-precision form):
+    r = y - A_hi x; d = PCG(A_lo, r, 0, inner); x += d, `refinements` times."""
+    x = np.array(x0, dtype=np.float64)
+    for _ in range(refinements):
+        r = y - A_hi(x)
+        if math.sqrt(float(np.sum(r * r))) < tol:
+            break
+        x += cgsolver(A_lo, r, np.zeros_like(x), inner, tol)
+    return x
+
+
 def grad_u(u):
     """src/finitediff.cpp:8-47: central differences / 2 on interior voxels, zero border."""
     g = np.zeros((3,) + u.shape, dtype=np.float64)
@@ -571,8 +583,10 @@ def laplacian(u):
     return divergence(grad_u(u))
 
 
-def split_bregman(A: Callable, yT, x0, lam, mu, outer_max, inner_max, tol, xtol, log=None):
-    """src/bregman.cpp:39-134 (isotropic TV, inner PCG on A + mu*laplacian)."""
+def split_bregman(A: Callable, yT, x0, lam, mu, outer_max, inner_max, tol, xtol, log=None,
+                  A_lo: Callable | None = None, refinements: int = 0):
+    """src/bregman.cpp:39-134 (isotropic TV, inner PCG on A + mu*laplacian).  With
+    A_lo and refinements > 0 the inner solve is cgsolver_refined (mixed form)."""
     eps = 1e-8
     x = np.array(x0, dtype=np.float64)
     x_old = x.copy()
@@ -583,9 +597,15 @@ def split_bregman(A: Callable, yT, x0, lam, mu, outer_max, inner_max, tol, xtol,
         du = A(u)
         return du + mu * np.stack([laplacian(u[i]) for i in range(3)])
 
+    def Ap_lo(u):
+        return A_lo(u) + mu * np.stack([laplacian(u[i]) for i in range(3)])
+
     for it in range(outer_max):
         rhs = np.stack([yT[i] + divergence(d[i] - b[i]) * mu for i in range(3)])
-        x = cgsolver(Ap, rhs, x_old, inner_max, tol)
+        if A_lo is not None and refinements > 0:
+            x = cgsolver_refined(Ap, Ap_lo, rhs, x_old, inner_max, refinements, tol)
+        else:
+            x = cgsolver(Ap, rhs, x_old, inner_max, tol)
         gx = np.stack([grad_u(x[i]) for i in range(3)])
         sk = np.sqrt(eps + ((gx + b) ** 2).sum(axis=(0, 1)))
         d = np.maximum(sk - lam / mu, 0.0) * ((gx + b) / sk)
@@ -742,22 +762,30 @@ def mbir_setup(datasets, recon_dims, params, proj_pad, eps=1e-12, exact=False,
     return out_dims, plan, grids, gammas, yT
 
 
-def MBIR1(datasets, recon_dims, params, eps=1e-12, exact=False):
-    """src/mbir_cg.cpp:48-128 (projections padded by PAD_FACTOR-1)."""
+def MBIR1(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
+    """src/mbir_cg.cpp:48-128 (projections padded by PAD_FACTOR-1).  refinements > 0
+    runs the mixed form's algorithm (cgsolver_refined, maxIters // refinements inner
+    iterations per cycle) with the exact operator in both roles."""
     pad = np.float32(params.PAD_FACTOR - 1.0)
     out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params, pad, eps, exact)
     A = lambda v: normal(v, grids, gammas, plan)
-    x = cgsolver(A, yT, np.zeros((3,) + out_dims), params.maxIters, params.tol)
+    if refinements > 0:
+        x = cgsolver_refined(A, A, yT, np.zeros((3,) + out_dims), max(1, params.maxIters // refinements),
+                             refinements, params.tol)
+    else:
+        x = cgsolver(A, yT, np.zeros((3,) + out_dims), params.maxIters, params.tol)
     return np.stack([crop3d(x[i], recon_dims) for i in range(3)])
 
 
-def MBIR2(datasets, recon_dims, params, eps=1e-12, exact=False):
-    """src/mbir_sb.cpp:47-114 (projections padded by PAD_FACTOR itself)."""
+def MBIR2(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
+    """src/mbir_sb.cpp:47-114 (projections padded by PAD_FACTOR itself); refinements
+    > 0 as in MBIR1 for each inner linear solve."""
     out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params,
                                                    params.PAD_FACTOR, eps, exact)
     A = lambda v: normal(v, grids, gammas, plan)
     x = split_bregman(A, yT, np.zeros((3,) + out_dims), params.lam, params.mu,
-                      params.maxIters, params.innerIters, params.tol, params.xtol)
+                      params.maxIters, params.innerIters, params.tol, params.xtol,
+                      A_lo=A if refinements > 0 else None, refinements=refinements)
     return np.stack([crop3d(x[i], recon_dims) for i in range(3)])
 
 

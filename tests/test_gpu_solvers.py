@@ -103,3 +103,21 @@ def test_mbir_vs_oracle(L, O, method):
         got = fn(data, recon, pl)
         assert got.shape == (3,) + recon
         assert rel(got, want) < 1e-4, kind
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_mbir_mixed_precision_vs_oracle(L, O, method):
+    """Mixed form (FP16 spectra in the correction solves, FP32-residual refinement
+    cycles, FP64 reductions) against the FP64 oracle running the same refined
+    algorithm with the exact operator in both roles.  Bar: 1e-4 (final volume)."""
+    recon = (8, 5, 9)
+    data = _datasets(L, O, recon)
+    R = 3
+    po = O.ReconParams(maxIters=6, innerIters=3)
+    fn_o = {1: O.MBIR1, 2: O.MBIR2}[method]
+    want = fn_o(data, recon, po, exact=True, refinements=R)
+    got = {1: L.MBIR1, 2: L.MBIR2}[method](data, recon, L.ReconParams(maxIters=6, innerIters=3, op_kind="mixed",
+                                                                        refinements=R))
+    err = rel(got, want)
+    print(f"MBIR{method} mixed vs FP64 oracle: {err:.2e}")
+    assert err < 1e-4
