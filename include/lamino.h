@@ -177,6 +177,7 @@ typedef struct {
     int op_kind;
     double eps;
     int refinements;
+    int use_graphs; /* replay each solver iteration's operator work as a CUDA graph (non-default streams) */
 } lamino_recon_params;
 void lamino_recon_params_default(lamino_recon_params *p);
 /* method 1, 2 or 3.  projs[i]: [proj_dims[3i]][proj_dims[3i+1]][proj_dims[3i+2]];
@@ -184,6 +185,33 @@ void lamino_recon_params_default(lamino_recon_params *p);
 int lamino_mbir(int method, int ndatasets, const float *const *projs, const int64_t *proj_dims,
                 const float *const *angles, const float *gammas, int64_t r1, int64_t r2, int64_t r3,
                 const lamino_recon_params *params, float *out3, void *stream);
+
+/* Estimated peak device bytes of one lamino_mbir call (used for admission control). */
+int lamino_mbir_footprint(int method, int ndatasets, const int64_t *proj_dims, int64_t r1, int64_t r2, int64_t r3,
+                          const lamino_recon_params *params, int64_t *bytes);
+
+/* ---- continuous-batching server (no reference counterpart) ----------------------
+ * Requests are MBIR1/2/3 problems as for lamino_mbir (inputs copied at submit).
+ * A request is admitted in arrival order as soon as one of `slots` workers is free
+ * and its estimated footprint fits in `budget_bytes` next to the running ones; each
+ * worker runs on its own CUDA stream, so admitted reconstructions overlap on the
+ * device and keep their iterates there until they finish.  flags & 1: dry run
+ * (workers hold each request for dry_run_ms without touching the GPU; for tests
+ * of the admission logic). */
+typedef struct lamino_server_s *lamino_server_t;
+int lamino_server_create(int64_t budget_bytes, int slots, int flags, double dry_run_ms, lamino_server_t *out);
+int lamino_server_submit(lamino_server_t srv, int method, int ndatasets, const float *const *projs,
+                         const int64_t *proj_dims, const float *const *angles, const float *gammas, int64_t r1,
+                         int64_t r2, int64_t r3, const lamino_recon_params *params, int64_t *id);
+/* Waits for request `id` (timeout_s < 0: no limit; returns LAMINO_ERR_TIMEOUT on
+ * expiry), copies the reconstruction to out3 (host, may be NULL), reports the time
+ * queued and running and the total latency in seconds, then forgets the request. */
+int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float *out3, double *queue_s,
+                       double *run_s, double *latency_s);
+/* stats[10] = submitted, completed, failed, bytes in use, peak bytes in use, budget,
+ * active, peak active, queued, slots. */
+int lamino_server_stats(lamino_server_t srv, int64_t *stats);
+int lamino_server_destroy(lamino_server_t srv);
 
 #ifdef __cplusplus
 }

@@ -19,7 +19,8 @@ import numpy as np
 __all__ = [
     "LaminoError", "lib", "PolarGrid", "NufftPlan", "ToeplitzNormal", "beam_dir_vector",
     "forward", "adjoint", "sysmat", "gradient", "residual", "nufft3d1", "nufft3d2",
-    "MBIR1", "MBIR2", "MBIR3", "ReconParams", "opt", "padded_volume_dims",
+    "MBIR1", "MBIR2", "MBIR3", "ReconParams", "opt", "padded_volume_dims", "mbir_footprint",
+    "ReconServer",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -80,6 +81,12 @@ def lib():
         "lamino_lipschitz": ([vp, i64, i64, i64, i32, f64, ctypes.c_uint64, P(f64), vp], i32),
         "lamino_recon_params_default": ([vp], None),
         "lamino_mbir": ([i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, vp, vp], i32),
+        "lamino_mbir_footprint": ([i32, i32, P(i64), i64, i64, i64, vp, P(i64)], i32),
+        "lamino_server_create": ([i64, i32, i32, f64, P(vp)], i32),
+        "lamino_server_submit": ([vp, i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, P(i64)], i32),
+        "lamino_server_wait": ([vp, i64, f64, vp, P(f64), P(f64), P(f64)], i32),
+        "lamino_server_stats": ([vp, P(i64)], i32),
+        "lamino_server_destroy": ([vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -447,13 +454,14 @@ class _ReconParamsC(ctypes.Structure):
                 ("sigma", ctypes.c_float), ("p", ctypes.c_float), ("lam", ctypes.c_float),
                 ("mu", ctypes.c_float), ("tol", ctypes.c_float), ("xtol", ctypes.c_float),
                 ("pad_factor", ctypes.c_float), ("op_kind", ctypes.c_int), ("eps", ctypes.c_double),
-                ("refinements", ctypes.c_int)]
+                ("refinements", ctypes.c_int), ("use_graphs", ctypes.c_int)]
 
 
 class ReconParams:
     """tomocam::ReconParams defaults (include/config.h:146-158) plus the operator
     form: op_kind 'toeplitz' (FP32 spectra), 'toeplitz_fp16', 'nufft' or 'mixed'
-    (FP16 correction solves in `refinements` FP32-residual cycles)."""
+    (FP16 correction solves in `refinements` FP32-residual cycles), and
+    use_graphs (replay each solver iteration's operator work as a CUDA graph)."""
 
     def __init__(self, **kw):
         c = _ReconParamsC()
@@ -462,6 +470,7 @@ class ReconParams:
         self.sigma, self.p, self.lam, self.mu = c.sigma, c.p, c.lam, c.mu
         self.tol, self.xtol, self.PAD_FACTOR = c.tol, c.xtol, c.pad_factor
         self.op_kind, self.eps, self.refinements = "toeplitz", c.eps, c.refinements
+        self.use_graphs = bool(c.use_graphs)
         for k, v in kw.items():
             setattr(self, k, v)
 
@@ -469,32 +478,126 @@ class ReconParams:
         kind = {"toeplitz": 0, "toeplitz_fp16": 1, "nufft": 2, "mixed": 3}[self.op_kind]
         return _ReconParamsC(int(self.maxIters), int(self.innerIters), float(self.sigma), float(self.p),
                              float(self.lam), float(self.mu), float(self.tol), float(self.xtol),
-                             float(self.PAD_FACTOR), kind, float(self.eps), int(self.refinements))
+                             float(self.PAD_FACTOR), kind, float(self.eps), int(self.refinements),
+                             int(bool(self.use_graphs)))
 
 
-def _mbir(method, datasets, recon_dims, params):
-    params = params or ReconParams()
+def _datasets_c(datasets):
+    """ctypes arrays (projection pointers, dims, angle pointers, gammas) of a list of
+    (projections, angles, gamma) triples, plus the arrays they point into."""
     n = len(datasets)
+    if n == 0:
+        raise ValueError("no datasets")
     keep = []
     projs = (ctypes.c_void_p * n)()
     angs = (ctypes.c_void_p * n)()
     dims = (ctypes.c_int64 * (3 * n))()
     gam = (ctypes.c_float * n)()
-    ref = None
     for i, (proj, angles, gamma) in enumerate(datasets):
         p = _as_f32(proj)
         a = np.ascontiguousarray(angles, dtype=np.float32)
+        if p.ndim != 3 or a.shape != (p.shape[0],):
+            raise ValueError("projections must be (nproj, nrows, ncols) with one angle per projection")
         keep += [p, a]
-        ref = p if ref is None else ref
         projs[i] = _ptr(p).value
         angs[i] = _ptr(a).value
         dims[3 * i:3 * i + 3] = list(p.shape)
         gam[i] = float(gamma)
+    return n, projs, dims, angs, gam, keep
+
+
+def _mbir(method, datasets, recon_dims, params):
+    params = params or ReconParams()
+    n, projs, dims, angs, gam, keep = _datasets_c(datasets)
+    ref = keep[0]
     out = _empty_like_kind(ref, (3,) + tuple(recon_dims))
     pc = params._c()
     _check(lib().lamino_mbir(method, n, projs, dims, angs, gam, *[int(d) for d in recon_dims],
                              ctypes.byref(pc), _ptr(out), _stream(ref)))
     return out
+
+
+def mbir_footprint(method: int, proj_shapes, recon_dims, params: ReconParams | None = None) -> int:
+    """Estimated peak device bytes of one MBIR{method} call with datasets of the
+    given (nproj, nrows, ncols) shapes (the server's admission figure)."""
+    params = params or ReconParams()
+    n = len(proj_shapes)
+    dims = (ctypes.c_int64 * (3 * n))(*[int(v) for sh in proj_shapes for v in sh])
+    out = ctypes.c_int64()
+    pc = params._c()
+    _check(lib().lamino_mbir_footprint(method, n, dims, *[int(d) for d in recon_dims], ctypes.byref(pc),
+                                       ctypes.byref(out)))
+    return out.value
+
+
+class ReconServer:
+    """Continuous-batching MBIR server (no reference counterpart).
+
+    Requests are admitted in arrival order while a worker slot is free and the
+    sum of their estimated device footprints stays within ``budget_bytes``; each
+    worker runs on its own CUDA stream.  ``dry_run_ms`` (not None) makes the
+    workers hold each request that long without touching the GPU, which tests
+    the admission logic on any machine."""
+
+    STAT_KEYS = ("submitted", "completed", "failed", "in_use", "peak_in_use", "budget", "active",
+                 "peak_active", "queued", "slots")
+
+    def __init__(self, budget_bytes: int, slots: int = 4, dry_run_ms: float | None = None):
+        h = ctypes.c_void_p()
+        flags = 1 if dry_run_ms is not None else 0
+        _check(lib().lamino_server_create(int(budget_bytes), int(slots), flags, float(dry_run_ms or 0.0),
+                                          ctypes.byref(h)))
+        self._h = h
+        self._dims = {}
+
+    def submit(self, method: int, datasets, recon_dims, params: ReconParams | None = None) -> int:
+        """Queue MBIR{method} on the datasets (inputs are copied); returns the request id."""
+        params = params or ReconParams()
+        n, projs, dims, angs, gam, keep = _datasets_c(datasets)
+        rid = ctypes.c_int64()
+        pc = params._c()
+        _check(lib().lamino_server_submit(self._h, method, n, projs, dims, angs, gam,
+                                          *[int(d) for d in recon_dims], ctypes.byref(pc), ctypes.byref(rid)))
+        self._dims[rid.value] = tuple(int(d) for d in recon_dims)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float | None = None):
+        """Block until request `rid` finished; returns (volume (3, r1, r2, r3) numpy,
+        {"queue_s", "run_s", "latency_s"}).  Raises LaminoError on failure or timeout."""
+        if rid not in self._dims:
+            raise LaminoError(1, "unknown request id")
+        shape = (3,) + self._dims[rid]
+        out = np.empty(shape, dtype=np.float32)
+        q, r, l = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rc = lib().lamino_server_wait(self._h, int(rid), -1.0 if timeout is None else float(timeout),
+                                      ctypes.c_void_p(out.ctypes.data), ctypes.byref(q), ctypes.byref(r),
+                                      ctypes.byref(l))
+        if rc != 5:  # LAMINO_ERR_TIMEOUT: the request stays queryable
+            self._dims.pop(rid, None)
+        _check(rc)
+        return out, {"queue_s": q.value, "run_s": r.value, "latency_s": l.value}
+
+    def stats(self) -> dict:
+        st = (ctypes.c_int64 * 10)()
+        _check(lib().lamino_server_stats(self._h, st))
+        return dict(zip(self.STAT_KEYS, list(st)))
+
+    def close(self):
+        if self._h:
+            _check(lib().lamino_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def MBIR1(datasets, recon_dims, params: ReconParams | None = None):

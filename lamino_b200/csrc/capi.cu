@@ -1,13 +1,14 @@
 // C ABI of lamino_b200 (declared in include/lamino.h).  Every entry point
 // converts C++ exceptions into status codes plus a thread-local message, and
 // stages host buffers through device memory when it is given host pointers.
+#include <cstring>
 #include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/lamino.h"
-#include "mbir.cuh"
+#include "server.cuh"
 
 using namespace lamino;
 
@@ -24,6 +25,9 @@ struct lamino_normal_s {
 struct lamino_op_s {
     OpFn fn;
     Dims3 d;
+};
+struct lamino_server_s {
+    std::unique_ptr<Server> s;
 };
 
 namespace {
@@ -497,14 +501,10 @@ void lamino_recon_params_default(lamino_recon_params *p) {
     p->op_kind = d.op_kind;
     p->eps = d.eps;
     p->refinements = d.refinements;
+    p->use_graphs = d.use_graphs;
 }
 
-int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *pdims, const float *const *angles,
-                const float *gammas, int64_t r1, int64_t r2, int64_t r3, const lamino_recon_params *params,
-                float *out3, void *stream) {
-    API_BEGIN
-    if (nds <= 0 || !projs || !pdims || !angles || !gammas || !params) throw Error(ERR_ARG, "null argument");
-    Dims3 rd = dims_of(r1, r2, r3);
+static ReconParams params_of(const lamino_recon_params *params) {
     ReconParams prm;
     prm.max_iters = params->max_iters;
     prm.inner_iters = params->inner_iters;
@@ -518,17 +518,144 @@ int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *p
     prm.op_kind = params->op_kind;
     prm.eps = params->eps;
     prm.refinements = params->refinements;
+    prm.use_graphs = params->use_graphs;
+    if (prm.max_iters < 0 || prm.inner_iters < 0) throw Error(ERR_ARG, "iteration counts must be >= 0");
+    if (prm.op_kind < 0 || prm.op_kind > 3) throw Error(ERR_ARG, "op_kind must be 0..3");
+    return prm;
+}
+
+// A caller on the legacy default stream gets a private non-blocking stream for
+// the whole reconstruction (ordered after the caller's earlier default-stream
+// work), so the solver iterations can be graph-captured; the call still returns
+// only when the result is complete.
+struct CallStream {
+    cudaStream_t s = nullptr;
+    bool owned = false;
+    explicit CallStream(void *user) {
+        s = S(user);
+        if (s) return;
+        LAMINO_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        owned = true;
+        cudaEvent_t e;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(e, nullptr);
+            cudaStreamWaitEvent(s, e, 0);
+            cudaEventDestroy(e);
+        }
+    }
+    ~CallStream() {
+        if (owned) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+};
+
+int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *pdims, const float *const *angles,
+                const float *gammas, int64_t r1, int64_t r2, int64_t r3, const lamino_recon_params *params,
+                float *out3, void *stream) {
+    API_BEGIN
+    if (nds <= 0 || !projs || !pdims || !angles || !gammas || !params) throw Error(ERR_ARG, "null argument");
+    Dims3 rd = dims_of(r1, r2, r3);
+    ReconParams prm = params_of(params);
+    CallStream cs(stream);
     std::vector<std::unique_ptr<In<float>>> ins;
     std::vector<Dataset> data;
     for (int i = 0; i < nds; ++i) {
         int64_t np = pdims[3 * i], nr = pdims[3 * i + 1], nc = pdims[3 * i + 2];
         if (np <= 0 || nr <= 0 || nc <= 0) throw Error(ERR_ARG, "projection dims must be positive");
-        ins.emplace_back(new In<float>(projs[i], (size_t)(np * nr * nc), S(stream)));
+        ins.emplace_back(new In<float>(projs[i], (size_t)(np * nr * nc), cs.s));
         data.push_back(Dataset{ins.back()->d, np, nr, nc, angles[i], gammas[i]});
     }
-    Out<float> o(out3, 3 * rd.size(), S(stream));
-    mbir(method, data, rd, prm, o.d, S(stream));
-    o.finish(S(stream));
+    Out<float> o(out3, 3 * rd.size(), cs.s);
+    mbir(method, data, rd, prm, o.d, cs.s);
+    o.finish(cs.s);
+    API_END
+}
+
+int lamino_mbir_footprint(int method, int nds, const int64_t *pdims, int64_t r1, int64_t r2, int64_t r3,
+                          const lamino_recon_params *params, int64_t *bytes) {
+    API_BEGIN
+    if (nds <= 0 || !pdims || !params || !bytes) throw Error(ERR_ARG, "null argument");
+    if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1, 2 or 3");
+    std::vector<std::array<int64_t, 3>> pd;
+    for (int i = 0; i < nds; ++i) pd.push_back({pdims[3 * i], pdims[3 * i + 1], pdims[3 * i + 2]});
+    *bytes = mbir_footprint(method, pd, dims_of(r1, r2, r3), params_of(params));
+    API_END
+}
+
+int lamino_server_create(int64_t budget, int slots, int flags, double dry_run_ms, lamino_server_t *out) {
+    API_BEGIN
+    if (!out) throw Error(ERR_ARG, "null argument");
+    auto h = std::make_unique<lamino_server_s>();
+    h->s.reset(new Server(budget, slots, (flags & 1) != 0, dry_run_ms));
+    *out = h.release();
+    API_END
+}
+
+int lamino_server_submit(lamino_server_t srv, int method, int nds, const float *const *projs, const int64_t *pdims,
+                         const float *const *angles, const float *gammas, int64_t r1, int64_t r2, int64_t r3,
+                         const lamino_recon_params *params, int64_t *id) {
+    API_BEGIN
+    if (!srv || nds <= 0 || !projs || !pdims || !angles || !gammas || !params || !id)
+        throw Error(ERR_ARG, "null argument");
+    if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1, 2 or 3");
+    auto r = std::make_unique<ServeRequest>();
+    r->method = method;
+    r->recon = dims_of(r1, r2, r3);
+    r->prm = params_of(params);
+    for (int i = 0; i < nds; ++i) {
+        int64_t np = pdims[3 * i], nr = pdims[3 * i + 1], nc = pdims[3 * i + 2];
+        if (np <= 0 || nr <= 0 || nc <= 0) throw Error(ERR_ARG, "projection dims must be positive");
+        if (!projs[i] || !angles[i]) throw Error(ERR_ARG, "null dataset pointer");
+        size_t m = (size_t)(np * nr * nc);
+        r->projs.emplace_back(m);
+        if (is_device_ptr(projs[i]))
+            LAMINO_CUDA(cudaMemcpy(r->projs.back().data(), projs[i], m * 4, cudaMemcpyDeviceToHost));
+        else
+            std::memcpy(r->projs.back().data(), projs[i], m * 4);
+        r->pdims.push_back({np, nr, nc});
+        r->angles.emplace_back(angles[i], angles[i] + np);
+        r->gammas.push_back(gammas[i]);
+    }
+    r->footprint = mbir_footprint(method, r->pdims, r->recon, r->prm);
+    *id = srv->s->submit(std::move(r));
+    API_END
+}
+
+int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float *out3, double *queue_s,
+                       double *run_s, double *latency_s) {
+    API_BEGIN
+    if (!srv) throw Error(ERR_ARG, "null server");
+    ServeRequest *r = nullptr;
+    if (!srv->s->wait(id, timeout_s, &r)) throw Error(ERR_TIMEOUT, "request not finished within the timeout");
+    if (r->status != OK) {
+        int code = r->status;
+        std::string msg = r->err;
+        srv->s->release(id);
+        throw Error(code, msg);
+    }
+    if (out3) std::memcpy(out3, r->result.data(), r->result.size() * 4);
+    if (queue_s) *queue_s = r->t_start - r->t_submit;
+    if (run_s) *run_s = r->t_done - r->t_start;
+    if (latency_s) *latency_s = r->t_done - r->t_submit;
+    srv->s->release(id);
+    API_END
+}
+
+int lamino_server_stats(lamino_server_t srv, int64_t *st) {
+    API_BEGIN
+    if (!srv || !st) throw Error(ERR_ARG, "null argument");
+    ServerStats x = srv->s->stats();
+    int64_t v[10] = {x.submitted, x.completed, x.failed, x.in_use, x.peak_in_use,
+                     x.budget, x.active, x.peak_active, x.queued, x.slots};
+    std::memcpy(st, v, sizeof(v));
+    API_END
+}
+
+int lamino_server_destroy(lamino_server_t srv) {
+    API_BEGIN
+    delete srv;
     API_END
 }
 

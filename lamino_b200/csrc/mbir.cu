@@ -9,6 +9,7 @@
 #include <memory>
 #include <vector>
 
+#include "graph.cuh"
 #include "mbir.cuh"
 
 namespace lamino {
@@ -72,18 +73,62 @@ __global__ void k_axpy_scalar(float *__restrict__ y, float a, const float *__res
         y[i] += a * x[i];
 }
 
+static Dims3 padded_dims(int method, Dims3 recon, const ReconParams &prm) {
+    // volume padding: MBIR1 uses T(PAD-1.0); MBIR2/3 use (T(PAD) - 1) in float
+    float vfac = method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor - 1.0f;
+    return Dims3{pad_dim(recon.n1, vfac), pad_dim(recon.n2, vfac), pad_dim(recon.n3, vfac)};
+}
+
+static float proj_pad_factor(int method, const ReconParams &prm) {
+    // projection padding: MBIR1 pads by PAD-1, MBIR2/3 by PAD itself
+    return method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor;
+}
+
+static int64_t pad2d_len(int64_t n, float factor) {
+    return factor < 1.e-06f ? n : n + 2 * ((int64_t)((float)n * factor) / 2);
+}
+
+int64_t mbir_footprint(int method, const std::vector<std::array<int64_t, 3>> &proj_dims, Dims3 recon,
+                       const ReconParams &prm) {
+    const Dims3 od = padded_dims(method, recon, prm);
+    const float pf = proj_pad_factor(method, prm);
+    const int64_t V = od.size();
+    int64_t raw = 0, maxpts = 0;
+    for (auto &d : proj_dims) {
+        raw += d[0] * d[1] * d[2] * 4;
+        maxpts = std::max<int64_t>(maxpts, d[0] * pad2d_len(d[1], pf) * pad2d_len(d[2], pf));
+    }
+    const int w = es_width(prm.eps);
+    const int64_t nf = next_smooth_even(std::max<int64_t>(2 * od.n1, 2 * w)) *
+                       next_smooth_even(std::max<int64_t>(2 * od.n2, 2 * w)) *
+                       next_smooth_even(std::max<int64_t>(2 * od.n3, 2 * w));
+    // setup: raw + padded projections, projection spectra + 2-D FFT work, fine grids + 3-D FFT work
+    const int64_t setup = raw + maxpts * 4 + 2 * maxpts * 8 + (6 + 1) * nf * 8 + 3 * V * 4;
+    const int64_t L1 = next_smooth_even(2 * od.n1), L2 = next_smooth_even(2 * od.n2), L3 = next_smooth_even(2 * od.n3);
+    const int64_t S = L1 * L2 * (L3 / 2 + 1), L = L1 * L2 * L3;
+    const int64_t n1p = (od.n1 + 7) / 8 * 8;
+    const int64_t kb = prm.op_kind == OP_TOEPLITZ_FP32 ? 4 : (prm.op_kind == OP_TOEPLITZ_FP16 ? 2 : 6);
+    const int64_t inter = 3 * od.n1 * od.n2 * (L3 / 2 + 1) * 8 + 3 * L2 * (L3 / 2 + 1) * n1p * 8;
+    int64_t op = 6 * S * kb + inter;
+    const int64_t build = 6 * L * 4 + 2 * S * 8;  // transient kernel grids + R2C output and work
+    if (method == 3) op += (int64_t)proj_dims.size() * (6 * S * 4 + inter);  // per-gamma operators for the loss
+    if (prm.op_kind == OP_NUFFT) op = (6 + 1) * nf * 8 + 2 * maxpts * 8;
+    const int64_t state = (method == 2 ? 40 : 12) * V * 4 + 3 * V * 4;
+    const int64_t solve = op + state + (prm.op_kind == OP_NUFFT ? 0 : build);
+    const int64_t peak = std::max(setup, solve + 3 * V * 4 + raw);
+    return peak + peak / 4 + (64LL << 20);  // cuFFT work areas and allocator slack
+}
+
 void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
           cudaStream_t s) {
     if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1 (CG), 2 (split Bregman) or 3 (NAG)");
     if (data.empty()) throw Error(ERR_ARG, "no datasets");
-    // volume padding: MBIR1 uses T(PAD-1.0); MBIR2/3 use (T(PAD) - 1) in float
-    float vfac = method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor - 1.0f;
-    Dims3 od{pad_dim(recon.n1, vfac), pad_dim(recon.n2, vfac), pad_dim(recon.n3, vfac)};
-    // projection padding: MBIR1 pads by PAD-1, MBIR2/3 by PAD itself
-    float pfac = method == 1 ? (float)((double)prm.pad_factor - 1.0) : prm.pad_factor;
+    const Dims3 od = padded_dims(method, recon, prm);
+    const float pfac = proj_pad_factor(method, prm);
     const int64_t V = od.size(), n = 3 * V;
+    const bool graphs = prm.use_graphs != 0;
 
-    NufftPlan plan(od, prm.eps);
+    std::unique_ptr<NufftPlan> plan(new NufftPlan(od, prm.eps));
     std::vector<std::unique_ptr<Geom>> geoms;
     DevBuf<float> yT(n);
     LAMINO_CUDA(cudaMemsetAsync(yT.p, 0, yT.bytes(), s));
@@ -97,7 +142,7 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         int64_t nr, nc;
         normalize_pad2d(ds.proj, ds.nproj, ds.nrows, ds.ncols, mx, pfac, y, nr, nc, s);
         geoms.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));
-        plan.adjoint(*geoms.back(), y.p, yT.p, true, s);
+        plan->adjoint(*geoms.back(), y.p, yT.p, true, s);
         LAMINO_CUDA(cudaStreamSynchronize(s));
     }
     std::vector<const Geom *> gptr;
@@ -105,16 +150,22 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
 
     // normal operator sum_gamma sysmat
     std::unique_ptr<Toeplitz> T;
-    OpFn A, A_lo;
+    OpFn A_raw, A_lo_raw;
     const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
     if (prm.op_kind == OP_NUFFT) {
-        A = [&](const float *x, float *y, cudaStream_t st) { plan.normal(gptr, x, y, st); };
+        NufftPlan *pl = plan.get();
+        A_raw = [pl, &gptr](const float *x, float *y, cudaStream_t st) { pl->normal(gptr, x, y, st); };
     } else {
+        plan.reset();  // the fine grids are only needed for the setup adjoints
         int prec = prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : (mixed ? PREC_MIXED : PREC_FP32);
         T.reset(new Toeplitz(gptr, od, prec, s));
-        A = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st, false); };
-        if (mixed) A_lo = [&](const float *x, float *y, cudaStream_t st) { T->apply(x, y, st, true); };
+        Toeplitz *tp = T.get();
+        A_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, false); };
+        if (mixed) A_lo_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, true); };
     }
+    GraphedOp gA(A_raw, graphs), gA_lo(A_lo_raw ? A_lo_raw : A_raw, graphs);
+    OpFn A = gA.as_fn();
+    OpFn A_lo = mixed ? gA_lo.as_fn() : OpFn();
 
     DevBuf<float> x(n);
     LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));
@@ -134,7 +185,8 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         std::vector<OpFn> Ag;
         for (const Geom *g : gptr) {
             if (prm.op_kind == OP_NUFFT) {
-                Ag.push_back([&plan, g](const float *xx, float *yy, cudaStream_t st) { plan.normal({g}, xx, yy, st); });
+                NufftPlan *pl = plan.get();
+                Ag.push_back([pl, g](const float *xx, float *yy, cudaStream_t st) { pl->normal({g}, xx, yy, st); });
             } else {
                 Tg.emplace_back(new Toeplitz({g}, od, prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : PREC_FP32, s));
                 Toeplitz *tp = Tg.back().get();
@@ -146,26 +198,38 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         red.fetch(1, s);
         const double yTy = red.h[0];
         const float ng = (float)gptr.size();
-        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) {
-            A(xx, g, st);
-            k_axpy_scalar<<<grid_for(n, 256), 256, 0, st>>>(g, -ng, yT.p, n);
-            LAMINO_LAUNCH("k_axpy_scalar");
-            for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od, prm.sigma, prm.p, st);
-        };
+        // gradient: sum_gamma (sysmat x - yT) + qGGMRF (src/mbir3.cpp:91-103), one graph per input
+        GraphedOp gGrad(
+            [&](const float *xx, float *g, cudaStream_t st) {
+                A_raw(xx, g, st);
+                k_axpy_scalar<<<grid_for(n, 256), 256, 0, st>>>(g, -ng, yT.p, n);
+                LAMINO_LAUNCH("k_axpy_scalar");
+                for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od, prm.sigma, prm.p, st);
+            },
+            graphs);
+        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) { gGrad(xx, g, st); };
+        // loss: per-gamma quadratic forms into device slots (graphed), then one fetch
         DevBuf<float> Sx(n);
-        Reducer lr(8);
-        LossFn loss = [&](const float *xx, cudaStream_t st) {
-            double e = 0.0;
-            for (auto &Aq : Ag) {
-                Aq(xx, Sx.p, st);
-                lr.zero(6, st);
-                for (int i = 0; i < 3; ++i) {
-                    vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + i, st);
-                    vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 3 + i, st);
+        const int ngi = (int)Ag.size();
+        Reducer lr(6 * ngi);
+        GraphedOp gLoss(
+            [&](const float *xx, float *, cudaStream_t st) {
+                lr.zero(6 * ngi, st);
+                for (int q = 0; q < ngi; ++q) {
+                    Ag[q](xx, Sx.p, st);
+                    for (int i = 0; i < 3; ++i) {
+                        vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + 6 * q + i, st);
+                        vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 6 * q + 3 + i, st);
+                    }
                 }
-                lr.fetch(6, st);
-                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[i] - 2.0 * lr.h[3 + i] + yTy);
-            }
+            },
+            graphs);
+        LossFn loss = [&](const float *xx, cudaStream_t st) {
+            gLoss(xx, nullptr, st);
+            lr.fetch(6 * ngi, st);
+            double e = 0.0;
+            for (int q = 0; q < ngi; ++q)
+                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[6 * q + i] - 2.0 * lr.h[6 * q + 3 + i] + yTy);
             return e;
         };
         nagopt(grad, loss, x.p, od, prm.max_iters, prm.mu, prm.tol, prm.xtol, prm.inner_iters, s);

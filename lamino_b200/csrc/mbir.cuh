@@ -1,6 +1,7 @@
 // MBIR drivers (src/mbir_cg.cpp, src/mbir_sb.cpp, src/mbir3.cpp) on the GPU path.
 #pragma once
 
+#include <array>
 #include <memory>
 #include <vector>
 
@@ -24,6 +25,7 @@ struct ReconParams {  // include/config.h:146-158 defaults
     int op_kind = OP_TOEPLITZ_FP32;
     double eps = 1.2e-6;
     int refinements = 3;  // refinement cycles per linear solve with OP_TOEPLITZ_MIXED
+    int use_graphs = 1;   // replay each solver iteration's operator work as a CUDA graph
 };
 
 struct Dataset {
@@ -41,6 +43,10 @@ void normalize_pad2d(const float *proj, int64_t np, int64_t nr, int64_t nc, floa
                      DevBuf<float> &out, int64_t &onr, int64_t &onc, cudaStream_t s);
 // crop3d (include/padding.h:207-232, symmetric), 3 components
 void crop3d3(const float *in, Dims3 from, Dims3 to, float *out, cudaStream_t s);
+
+// Estimated peak device bytes of one mbir() call (admission control).
+int64_t mbir_footprint(int method, const std::vector<std::array<int64_t, 3>> &proj_dims, Dims3 recon,
+                       const ReconParams &prm);
 
 // method 1 = CG, 2 = split Bregman, 3 = NAG + qGGMRF.  out3: recon dims, device.
 void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,

@@ -18,6 +18,8 @@
 // order (fft_engine.cuh), so no pass reorders data.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "nufft.cuh"
@@ -466,6 +468,22 @@ std::vector<int> fft_positions(int n, const std::vector<int> &radix) {
     return pos;
 }
 
+// The dynamic shared-memory limit is a per-function attribute shared by every
+// operator (and host thread) of the process on a device: it is only ever raised,
+// under a lock, so an operator built concurrently for a smaller volume cannot
+// lower it beneath one that is launching with more.
+void raise_smem_limit(const void *f, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> limit;
+    int dev = 0;
+    LAMINO_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    int &cur = limit[{dev, f}];
+    if (bytes <= cur) return;
+    LAMINO_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    cur = bytes;
+}
+
 static FftLen make_len(int n, bool lead2, DevBuf<float2> &tw, std::vector<int> *radix_out) {
     std::vector<int> r = fft_schedule(n, lead2);
     FftLen F{};
@@ -615,9 +633,7 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
     const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
-    auto attr = [](const void *f, int bytes) {
-        LAMINO_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    };
+    auto attr = [](const void *f, int bytes) { raise_smem_limit(f, bytes); };
     attr((const void *)k_r2c_rows<0>, smem_rows);
     attr((const void *)k_r2c_rows<729>, smem_rows);
     attr((const void *)k_c2r_rows<0>, smem_rows);
