@@ -210,11 +210,12 @@ def synthetic_magnetization_gpu(torch, dims, seed=1234, sigma=5.0, lateral_frac=
     g = torch.Generator(device="cuda").manual_seed(seed)
     m = torch.randn((3,) + tuple(dims), device="cuda", generator=g)
     m = m / (torch.linalg.vector_norm(m, dim=0, keepdim=True) + 1e-12)
-    r = int(3 * sigma)
-    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device="cuda", dtype=torch.float32) / sigma) ** 2)
-    k = k / k.sum()
     v = m.unsqueeze(1)  # (3, 1, n1, n2, n3)
     for ax in range(3):
+        # Gaussian truncated at 3 sigma, or at the axis length for thin axes (reflect padding)
+        r = min(int(3 * sigma), dims[ax] - 1)
+        k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device="cuda", dtype=torch.float32) / sigma) ** 2)
+        k = k / k.sum()
         shape = [1, 1, 1, 1, 1]
         shape[2 + ax] = 2 * r + 1
         pad = [0, 0, 0, 0, 0, 0]
@@ -365,6 +366,182 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# served and batched forms: many uneven reconstructions
+# ---------------------------------------------------------------------------
+
+SERVE_BUDGET = 150 * 10**9   # HBM bytes the served form may admit at once
+SERVE_ITERS = 40             # NAG + qGGMRF iterations of a mix request
+
+
+def serve_mix(n: int, seed: int = 7, big_frac: float = 0.0):
+    """Seeded request specs.  Mix requests: thickness from {8,16,24,32}, square
+    lateral size from {64,128,192,256}, 2 datasets of 60-240 angles each; the
+    first at gamma 0, the second at gamma = a tilt drawn from [20, 50] deg (the
+    reference geometry has no separate tilt angle); NAG + qGGMRF (sigma 1000,
+    p 1.2) for 40 iterations.  With probability big_frac a request is instead
+    the README-size split-Bregman reconstruction (51x511x511, 4 gammas x 361
+    angles, 50 outer iterations)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(n):
+        if big_frac > 0 and rng.random() < big_frac:
+            out.append(dict(kind="readme", method=2, recon=(511, 51, 511), det=(511, 511), nproj=[NPROJ] * 4,
+                            gammas=list(GAMMAS_DEG), seed=1234 + r, sigma=5.0))
+        else:
+            t = int(rng.choice([8, 16, 24, 32]))
+            h = int(rng.choice([64, 128, 192, 256]))
+            out.append(dict(kind="mix", method=3, recon=(h, t, h), det=(h, h),
+                            nproj=[int(rng.integers(60, 241)) for _ in range(2)],
+                            gammas=[0.0, float(rng.uniform(20.0, 50.0))], seed=1234 + r, sigma=3.0))
+    return out
+
+
+def serve_data(torch, L, spec):
+    """Host projections of one request: forward model of a seeded smoothed
+    unit-vector magnetization plus Gaussian noise at 1% of the signal RMS."""
+    import numpy as np
+    m = synthetic_magnetization_gpu(torch, spec["recon"], seed=spec["seed"], sigma=spec["sigma"])
+    rng = np.random.default_rng(spec["seed"])
+    g = torch.Generator(device="cuda").manual_seed(spec["seed"] + 1)
+    plan = L.NufftPlan(spec["recon"])
+    data = []
+    for n, gd in zip(spec["nproj"], spec["gammas"]):
+        th = rng.uniform(0, 2 * np.pi, n).astype(np.float32)
+        gam = np.float32(np.deg2rad(gd))
+        y = L.forward(m, L.PolarGrid(th, spec["det"][0], spec["det"][1], gam), plan=plan)
+        y = y + 0.01 * y.pow(2).mean().sqrt() * torch.randn(y.shape, device="cuda", generator=g)
+        data.append((y.cpu().numpy(), th, gam))
+    del plan
+    return data
+
+
+def serve_params(L, spec, form: str):
+    kw = dict(op_kind="toeplitz", use_graphs=False) if form == "plain" else \
+        dict(op_kind="toeplitz", use_graphs=True)
+    if spec["method"] == 3:
+        return L.ReconParams(maxIters=SERVE_ITERS, sigma=1000.0, p=1.2, **kw)
+    return L.ReconParams(maxIters=50, innerIters=3, lam=0.1, mu=10.0, **kw)
+
+
+def _pct(v, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_plain_loop(L, specs, data, arrivals):
+    """One reconstruction at a time in arrival order (FP32 Toeplitz, eager
+    launches): returns results, latencies (arrival -> done), service times and
+    applies."""
+    fns = {1: L.MBIR1, 2: L.MBIR2, 3: L.MBIR3}
+    res, lat, svc, app = [], [], [], []
+    t0 = time.perf_counter()
+    for i, (sp, d) in enumerate(zip(specs, data)):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        a = time.perf_counter()
+        res.append(fns[sp["method"]](d, sp["recon"], serve_params(L, sp, "plain")))
+        b = time.perf_counter()
+        svc.append(b - a)
+        lat.append(b - t0 - arrivals[i])
+        app.append(L.mbir_phases()["applies"])
+    return res, lat, svc, app, time.perf_counter() - t0
+
+
+def run_served(L, specs, data, arrivals, slots: int):
+    """Requests submitted to the continuous-batching server at their arrival
+    times (a submitting thread); latency = server-measured submit -> done."""
+    import threading
+    srv = L.ReconServer(SERVE_BUDGET, slots)
+    ids = [None] * len(specs)
+    ready = [threading.Event() for _ in specs]
+    t0 = time.perf_counter()
+
+    def feeder():
+        for i, (sp, d) in enumerate(zip(specs, data)):
+            now = time.perf_counter() - t0
+            if arrivals[i] > now:
+                time.sleep(arrivals[i] - now)
+            ids[i] = srv.submit(sp["method"], d, sp["recon"], serve_params(L, sp, "served"))
+            ready[i].set()
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    res, lat, app, info = [], [], [], []
+    for i in range(len(specs)):
+        ready[i].wait()
+        vol, t = srv.wait(ids[i])
+        res.append(vol)
+        lat.append(t["latency_s"])
+        app.append(t["applies"])
+        info.append(t)
+    span = time.perf_counter() - t0
+    th.join()
+    st = srv.stats()
+    srv.close()
+    return res, lat, app, span, st, info
+
+
+def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, seed: int = 7):
+    """Plain one-at-a-time loop against the served form on the same request
+    stream: saturating throughput (all requests at t = 0), then Poisson
+    arrivals at each multiple of the plain loop's saturating throughput."""
+    import numpy as np
+    specs = serve_mix(n, seed, big_frac)
+    data = [serve_data(torch, L, sp) for sp in specs]
+    torch.cuda.synchronize()
+    # warm-up: one request through each form (module load, kernel attributes, pools)
+    run_plain_loop(L, specs[:1], data[:1], [0.0])
+    run_served(L, specs[:1], data[:1], [0.0], slots)
+    zeros = [0.0] * n
+    p_res, p_lat, p_svc, p_app, p_span = run_plain_loop(L, specs, data, zeros)
+    s_res, s_lat, s_app, s_span, s_st, _ = run_served(L, specs, data, zeros, slots)
+    err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(s_res, p_res))
+    mu_plain = n / p_span
+    out = {
+        "requests": n, "slots": slots, "budget_bytes": SERVE_BUDGET,
+        "mix": {"readme_size": sum(sp["kind"] == "readme" for sp in specs),
+                "voxels_total": int(sum(3 * np.prod(sp["recon"]) for sp in specs))},
+        "saturated": {
+            "plain": {"recon_per_s": mu_plain, "applies_per_s": sum(p_app) / p_span, "makespan_s": p_span},
+            "served": {"recon_per_s": n / s_span, "applies_per_s": sum(s_app) / s_span, "makespan_s": s_span,
+                       "peak_active": s_st["peak_active"], "peak_bytes": s_st["peak_in_use"]},
+        },
+        "max_rel_err_served_vs_plain": err,
+        "sweep": [],
+    }
+    rng = np.random.default_rng(seed + 1)
+    for f in rates:
+        lam = f * mu_plain
+        arr = list(np.cumsum(rng.exponential(1.0 / lam, n)) - 0.0)
+        arr = [a - arr[0] for a in arr]
+        _, pl, _, _, pspan = run_plain_loop(L, specs, data, arr)
+        sres, sl, _, sspan, _, _ = run_served(L, specs, data, arr, slots)
+        out["sweep"].append({
+            "rate_x_plain_capacity": f, "arrivals_per_s": lam,
+            "plain": {"p50_s": _pct(pl, 50), "p99_s": _pct(pl, 99), "recon_per_s": n / pspan},
+            "served": {"p50_s": _pct(sl, 50), "p99_s": _pct(sl, 99), "recon_per_s": n / sspan},
+        })
+    return out
+
+
+def run_serve_form(args):
+    import torch
+    import lamino_b200 as L
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L.lib()
+    rates = [float(r) for r in args.rates.split(",")]
+    t0 = time.perf_counter()
+    res = serve_compare(torch, L, args.requests, rates, args.slots, args.big_frac)
+    res["wall_s"] = time.perf_counter() - t0
+    line = {"form": args.form, "metric": "reconstruction latency p50/p99 and recon/s, served vs plain",
+            "unit": "s", "higher_is_better": False, "dtype": "f32", "data": "synthetic", **res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,7 +552,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", choices=sorted(SCALES), default="full",
                     help="smaller cases of the same geometry for profiler captures")
+    ap.add_argument("--form", choices=["apply", "served"], default="apply",
+                    help="apply: the operator metric; served: plain loop vs continuous-batching server")
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--slots", type=int, default=6)
+    ap.add_argument("--rates", default="0.5,1.0,1.5", help="arrival rates, x the plain loop's capacity")
+    ap.add_argument("--big-frac", type=float, default=0.0, help="share of README-size requests")
     args = ap.parse_args()
+    if args.form == "served":
+        return run_serve_form(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -62,6 +62,12 @@ int lamino_geom_destroy(lamino_geom_t g);
  */
 int lamino_plan_create(int64_t n1, int64_t n2, int64_t n3, double eps, lamino_plan_t *out);
 int lamino_plan_destroy(lamino_plan_t p);
+/* Fine-grid bins of b1 x b2 x b3 cells for the plan's spreading and
+ * interpolation (each bin's tile of (b + w - 1)^3 cells per component is staged
+ * in shared memory); default 8 x 8 x 8.  Drops the plan's cached point orders.
+ * No reference counterpart (FINUFFT's opts.gpu_binsize* play this role in
+ * cuFINUFFT). */
+int lamino_plan_set_bins(lamino_plan_t p, int b1, int b2, int b3);
 /* Type 2, iflag -1: c[j] = sum_k modes[k] e^{-i k.x_j} (include/nufft.h:52-64).
  * modes: complex64 interleaved [n1][n2][n3]; c: complex64 [nproj][nrows][ncols]. */
 int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream);
@@ -186,6 +192,11 @@ int lamino_mbir(int method, int ndatasets, const float *const *projs, const int6
                 const float *const *angles, const float *gammas, int64_t r1, int64_t r2, int64_t r3,
                 const lamino_recon_params *params, float *out3, void *stream);
 
+/* Host wall-clock seconds of the calling thread's last lamino_mbir: setup
+ * (normalisation, padding, grids, adjoints), operator build and solve, and the
+ * number of normal-operator applications in the solve (any pointer may be NULL). */
+int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies);
+
 /* Estimated peak device bytes of one lamino_mbir call (used for admission control). */
 int lamino_mbir_footprint(int method, int ndatasets, const int64_t *proj_dims, int64_t r1, int64_t r2, int64_t r3,
                           const lamino_recon_params *params, int64_t *bytes);
@@ -205,9 +216,11 @@ int lamino_server_submit(lamino_server_t srv, int method, int ndatasets, const f
                          int64_t r2, int64_t r3, const lamino_recon_params *params, int64_t *id);
 /* Waits for request `id` (timeout_s < 0: no limit; returns LAMINO_ERR_TIMEOUT on
  * expiry), copies the reconstruction to out3 (host, may be NULL), reports the time
- * queued and running and the total latency in seconds, then forgets the request. */
+ * queued and running and the total latency in seconds and, in phases[4], the
+ * request's lamino_mbir_phases figures (setup, build, solve seconds, applies),
+ * then forgets the request.  Every output pointer may be NULL. */
 int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float *out3, double *queue_s,
-                       double *run_s, double *latency_s);
+                       double *run_s, double *latency_s, double *phases);
 /* stats[10] = submitted, completed, failed, bytes in use, peak bytes in use, budget,
  * active, peak active, queued, slots. */
 int lamino_server_stats(lamino_server_t srv, int64_t *stats);

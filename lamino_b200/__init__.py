@@ -20,6 +20,7 @@ __all__ = [
     "LaminoError", "lib", "PolarGrid", "NufftPlan", "ToeplitzNormal", "beam_dir_vector",
     "forward", "adjoint", "sysmat", "gradient", "residual", "nufft3d1", "nufft3d2",
     "MBIR1", "MBIR2", "MBIR3", "ReconParams", "opt", "padded_volume_dims", "mbir_footprint",
+    "mbir_phases",
     "ReconServer",
 ]
 
@@ -54,6 +55,7 @@ def lib():
         "lamino_geom_destroy": ([vp], i32),
         "lamino_plan_create": ([i64, i64, i64, f64, P(vp)], i32),
         "lamino_plan_destroy": ([vp], i32),
+        "lamino_plan_set_bins": ([vp, i32, i32, i32], i32),
         "lamino_nufft3d2": ([vp, vp, vp, vp, vp], i32),
         "lamino_nufft3d1": ([vp, vp, vp, vp, vp], i32),
         "lamino_forward": ([vp, vp, vp, vp, vp], i32),
@@ -84,7 +86,8 @@ def lib():
         "lamino_mbir_footprint": ([i32, i32, P(i64), i64, i64, i64, vp, P(i64)], i32),
         "lamino_server_create": ([i64, i32, i32, f64, P(vp)], i32),
         "lamino_server_submit": ([vp, i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, P(i64)], i32),
-        "lamino_server_wait": ([vp, i64, f64, vp, P(f64), P(f64), P(f64)], i32),
+        "lamino_server_wait": ([vp, i64, f64, vp, P(f64), P(f64), P(f64), P(f64)], i32),
+        "lamino_mbir_phases": ([P(f64), P(f64), P(f64), P(i64)], i32),
         "lamino_server_stats": ([vp, P(i64)], i32),
         "lamino_server_destroy": ([vp], i32),
     }
@@ -199,6 +202,11 @@ class NufftPlan:
         h = ctypes.c_void_p()
         _check(lib().lamino_plan_create(*self.dims, float(eps), ctypes.byref(h)))
         self._h = h
+
+    def set_bins(self, b1: int, b2: int, b3: int):
+        """Fine-grid bin size of the shared-memory spreading / interpolation."""
+        _check(lib().lamino_plan_set_bins(self._h, int(b1), int(b2), int(b3)))
+        return self
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -517,6 +525,15 @@ def _mbir(method, datasets, recon_dims, params):
     return out
 
 
+def mbir_phases() -> dict:
+    """Phases of this thread's last MBIR call: setup, operator build and solve
+    seconds (host wall clock) and the solve's normal-operator applications."""
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    n = ctypes.c_int64()
+    _check(lib().lamino_mbir_phases(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(n)))
+    return {"setup_s": a.value, "build_s": b.value, "solve_s": c.value, "applies": n.value}
+
+
 def mbir_footprint(method: int, proj_shapes, recon_dims, params: ReconParams | None = None) -> int:
     """Estimated peak device bytes of one MBIR{method} call with datasets of the
     given (nproj, nrows, ncols) shapes (the server's admission figure)."""
@@ -563,19 +580,22 @@ class ReconServer:
 
     def wait(self, rid: int, timeout: float | None = None):
         """Block until request `rid` finished; returns (volume (3, r1, r2, r3) numpy,
-        {"queue_s", "run_s", "latency_s"}).  Raises LaminoError on failure or timeout."""
+        {"queue_s", "run_s", "latency_s", "setup_s", "build_s", "solve_s", "applies"}).
+        Raises LaminoError on failure or timeout."""
         if rid not in self._dims:
             raise LaminoError(1, "unknown request id")
         shape = (3,) + self._dims[rid]
         out = np.empty(shape, dtype=np.float32)
         q, r, l = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        ph = (ctypes.c_double * 4)()
         rc = lib().lamino_server_wait(self._h, int(rid), -1.0 if timeout is None else float(timeout),
                                       ctypes.c_void_p(out.ctypes.data), ctypes.byref(q), ctypes.byref(r),
-                                      ctypes.byref(l))
+                                      ctypes.byref(l), ph)
         if rc != 5:  # LAMINO_ERR_TIMEOUT: the request stays queryable
             self._dims.pop(rid, None)
         _check(rc)
-        return out, {"queue_s": q.value, "run_s": r.value, "latency_s": l.value}
+        return out, {"queue_s": q.value, "run_s": r.value, "latency_s": l.value, "setup_s": ph[0],
+                     "build_s": ph[1], "solve_s": ph[2], "applies": int(ph[3])}
 
     def stats(self) -> dict:
         st = (ctypes.c_int64 * 10)()

@@ -182,6 +182,13 @@ int lamino_plan_destroy(lamino_plan_t p) {
     API_END
 }
 
+int lamino_plan_set_bins(lamino_plan_t p, int b1, int b2, int b3) {
+    API_BEGIN
+    if (!p) throw Error(ERR_ARG, "null plan");
+    p->p->set_bins(b1, b2, b3);
+    API_END
+}
+
 int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream) {
     API_BEGIN
     if (!p || !g) throw Error(ERR_ARG, "null handle");
@@ -573,6 +580,16 @@ int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *p
     API_END
 }
 
+int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies) {
+    API_BEGIN
+    const MbirPhases &p = last_mbir_phases();
+    if (setup_s) *setup_s = p.setup_s;
+    if (build_s) *build_s = p.build_s;
+    if (solve_s) *solve_s = p.solve_s;
+    if (applies) *applies = p.applies;
+    API_END
+}
+
 int lamino_mbir_footprint(int method, int nds, const int64_t *pdims, int64_t r1, int64_t r2, int64_t r3,
                           const lamino_recon_params *params, int64_t *bytes) {
     API_BEGIN
@@ -601,6 +618,7 @@ int lamino_server_submit(lamino_server_t srv, int method, int nds, const float *
         throw Error(ERR_ARG, "null argument");
     if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1, 2 or 3");
     auto r = std::make_unique<ServeRequest>();
+    r->t_submit = Server::now();  // latency counts the input copy below
     r->method = method;
     r->recon = dims_of(r1, r2, r3);
     r->prm = params_of(params);
@@ -624,7 +642,7 @@ int lamino_server_submit(lamino_server_t srv, int method, int nds, const float *
 }
 
 int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float *out3, double *queue_s,
-                       double *run_s, double *latency_s) {
+                       double *run_s, double *latency_s, double *phases) {
     API_BEGIN
     if (!srv) throw Error(ERR_ARG, "null server");
     ServeRequest *r = nullptr;
@@ -639,6 +657,12 @@ int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float 
     if (queue_s) *queue_s = r->t_start - r->t_submit;
     if (run_s) *run_s = r->t_done - r->t_start;
     if (latency_s) *latency_s = r->t_done - r->t_submit;
+    if (phases) {
+        phases[0] = r->phases.setup_s;
+        phases[1] = r->phases.build_s;
+        phases[2] = r->phases.solve_s;
+        phases[3] = (double)r->phases.applies;
+    }
     srv->s->release(id);
     API_END
 }

@@ -12,6 +12,7 @@
 // 51x511x511 / 4-gamma size) and every setpts sort of the reference path.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -32,7 +33,14 @@ struct GeomView {  // passed by value to kernels
     float sg, cg;
 };
 
+// Process-unique id of a geometry (keys caches of per-geometry point orders).
+inline uint64_t next_geom_uid() {
+    static std::atomic<uint64_t> n{0};
+    return ++n;
+}
+
 struct Geom {
+    uint64_t uid = next_geom_uid();
     int64_t nproj = 0, nrows = 0, ncols = 0;
     float gamma = 0.f, sg = 0.f, cg = 0.f;
     std::vector<float> theta;
@@ -60,11 +68,11 @@ struct Geom {
         sg = std::sin(g);
         cg = std::cos(g);
         qX.alloc(nc); qY.alloc(nr); st.alloc(np); ct.alloc(np); coeff.alloc(3 * np);
-        LAMINO_CUDA(cudaMemcpy(qX.p, hx.data(), nc * 4, cudaMemcpyHostToDevice));
-        LAMINO_CUDA(cudaMemcpy(qY.p, hy.data(), nr * 4, cudaMemcpyHostToDevice));
-        LAMINO_CUDA(cudaMemcpy(st.p, hs.data(), np * 4, cudaMemcpyHostToDevice));
-        LAMINO_CUDA(cudaMemcpy(ct.p, hc.data(), np * 4, cudaMemcpyHostToDevice));
-        LAMINO_CUDA(cudaMemcpy(coeff.p, h_coeff.data(), 3 * np * 4, cudaMemcpyHostToDevice));
+        upload(qX.p, hx.data(), (size_t)nc);
+        upload(qY.p, hy.data(), (size_t)nr);
+        upload(st.p, hs.data(), (size_t)np);
+        upload(ct.p, hc.data(), (size_t)np);
+        upload(coeff.p, h_coeff.data(), (size_t)(3 * np));
     }
     GeomView view() const {
         return GeomView{qX.p, qY.p, st.p, ct.p, coeff.p, (int)nproj, (int)nrows, (int)ncols, sg, cg};

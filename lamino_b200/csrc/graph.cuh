@@ -31,6 +31,7 @@ class GraphedOp {
     GraphedOp &operator=(const GraphedOp &) = delete;
 
     void operator()(const float *x, float *y, cudaStream_t s) {
+        ++calls_;
         if (!enabled_ || s == nullptr) {  // the legacy default stream cannot be captured
             f_(x, y, s);
             return;
@@ -64,6 +65,7 @@ class GraphedOp {
     }
     int graphs() const { return (int)graphs_.size(); }
     long launches() const { return launches_; }
+    long calls() const { return calls_; }
 
   private:
     struct Entry {
@@ -74,7 +76,7 @@ class GraphedOp {
     bool enabled_;
     std::map<std::pair<const float *, const float *>, Entry> graphs_;
     std::set<std::pair<const float *, const float *>> seen_;
-    long launches_ = 0;
+    long launches_ = 0, calls_ = 0;
 };
 
 }  // namespace lamino

@@ -10,6 +10,8 @@
 #include <vector>
 
 #include "graph.cuh"
+#include <chrono>
+
 #include "mbir.cuh"
 
 namespace lamino {
@@ -119,6 +121,15 @@ int64_t mbir_footprint(int method, const std::vector<std::array<int64_t, 3>> &pr
     return peak + peak / 4 + (64LL << 20);  // cuFFT work areas and allocator slack
 }
 
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+MbirPhases &last_mbir_phases() {
+    static thread_local MbirPhases p;
+    return p;
+}
+
 void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
           cudaStream_t s) {
     if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1 (CG), 2 (split Bregman) or 3 (NAG)");
@@ -127,6 +138,7 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     const float pfac = proj_pad_factor(method, prm);
     const int64_t V = od.size(), n = 3 * V;
     const bool graphs = prm.use_graphs != 0;
+    const double t0 = now_s();
 
     std::unique_ptr<NufftPlan> plan(new NufftPlan(od, prm.eps));
     std::vector<std::unique_ptr<Geom>> geoms;
@@ -148,17 +160,36 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     std::vector<const Geom *> gptr;
     for (auto &g : geoms) gptr.push_back(g.get());
 
-    // normal operator sum_gamma sysmat
+    const double t_setup = now_s();
+
+    // normal operator sum_gamma sysmat; MBIR3 also needs one operator per gamma
+    // for its loss, and then the sum is formed from their spectra
     std::unique_ptr<Toeplitz> T;
+    std::vector<std::unique_ptr<Toeplitz>> Tg;
     OpFn A_raw, A_lo_raw;
+    std::vector<OpFn> Ag;
     const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
     if (prm.op_kind == OP_NUFFT) {
         NufftPlan *pl = plan.get();
         A_raw = [pl, &gptr](const float *x, float *y, cudaStream_t st) { pl->normal(gptr, x, y, st); };
+        if (method == 3)
+            for (const Geom *g : gptr)
+                Ag.push_back([pl, g](const float *xx, float *yy, cudaStream_t st) { pl->normal({g}, xx, yy, st); });
     } else {
         plan.reset();  // the fine grids are only needed for the setup adjoints
         int prec = prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : (mixed ? PREC_MIXED : PREC_FP32);
-        T.reset(new Toeplitz(gptr, od, prec, s));
+        if (method == 3) {
+            std::vector<const Toeplitz *> parts;
+            for (const Geom *g : gptr) {
+                Tg.emplace_back(new Toeplitz({g}, od, PREC_FP32, s));
+                parts.push_back(Tg.back().get());
+                Toeplitz *tp = Tg.back().get();
+                Ag.push_back([tp](const float *xx, float *yy, cudaStream_t st) { tp->apply(xx, yy, st); });
+            }
+            T.reset(new Toeplitz(parts, prec, s));
+        } else {
+            T.reset(new Toeplitz(gptr, od, prec, s));
+        }
         Toeplitz *tp = T.get();
         A_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, false); };
         if (mixed) A_lo_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, true); };
@@ -169,6 +200,9 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
 
     DevBuf<float> x(n);
     LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    const double t_build = now_s();
+    int64_t extra_applies = 0;
     if (method == 1) {
         if (mixed) {
             int R = std::max(1, prm.refinements);
@@ -180,19 +214,6 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         split_bregman_refined(A, A_lo, mixed ? std::max(1, prm.refinements) : 0, yT.p, x.p, od, prm.lambda, prm.mu,
                               prm.max_iters, prm.inner_iters, prm.tol, prm.xtol, s);
     } else {
-        // per-gamma operators for the loss (sum over gamma of per-component sqrt terms)
-        std::vector<std::unique_ptr<Toeplitz>> Tg;
-        std::vector<OpFn> Ag;
-        for (const Geom *g : gptr) {
-            if (prm.op_kind == OP_NUFFT) {
-                NufftPlan *pl = plan.get();
-                Ag.push_back([pl, g](const float *xx, float *yy, cudaStream_t st) { pl->normal({g}, xx, yy, st); });
-            } else {
-                Tg.emplace_back(new Toeplitz({g}, od, prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : PREC_FP32, s));
-                Toeplitz *tp = Tg.back().get();
-                Ag.push_back([tp](const float *xx, float *yy, cudaStream_t st) { tp->apply(xx, yy, st); });
-            }
-        }
         red.zero(1, s);
         vec_dot(yT.p, yT.p, n, red.d, s);
         red.fetch(1, s);
@@ -207,7 +228,10 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
                 for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od, prm.sigma, prm.p, st);
             },
             graphs);
-        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) { gGrad(xx, g, st); };
+        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) {
+            gGrad(xx, g, st);
+            ++extra_applies;
+        };
         // loss: per-gamma quadratic forms into device slots (graphed), then one fetch
         DevBuf<float> Sx(n);
         const int ngi = (int)Ag.size();
@@ -226,6 +250,7 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
             graphs);
         LossFn loss = [&](const float *xx, cudaStream_t st) {
             gLoss(xx, nullptr, st);
+            extra_applies += ngi;
             lr.fetch(6 * ngi, st);
             double e = 0.0;
             for (int q = 0; q < ngi; ++q)
@@ -236,6 +261,11 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     }
     crop3d3(x.p, od, recon, out3, s);
     LAMINO_CUDA(cudaStreamSynchronize(s));
+    MbirPhases &ph = last_mbir_phases();
+    ph.setup_s = t_setup - t0;
+    ph.build_s = t_build - t_setup;
+    ph.solve_s = now_s() - t_build;
+    ph.applies = gA.calls() + gA_lo.calls() + extra_applies;
 }
 
 }  // namespace lamino

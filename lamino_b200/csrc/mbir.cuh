@@ -48,6 +48,15 @@ void crop3d3(const float *in, Dims3 from, Dims3 to, float *out, cudaStream_t s);
 int64_t mbir_footprint(int method, const std::vector<std::array<int64_t, 3>> &proj_dims, Dims3 recon,
                        const ReconParams &prm);
 
+// Host wall-clock seconds of the last mbir() call on this thread: setup
+// (normalisation, padding, grids, adjoints), operator build, solve; and the
+// number of normal-operator applications of the solve.
+struct MbirPhases {
+    double setup_s = 0, build_s = 0, solve_s = 0;
+    int64_t applies = 0;
+};
+MbirPhases &last_mbir_phases();
+
 // method 1 = CG, 2 = split Bregman, 3 = NAG + qGGMRF.  out3: recon dims, device.
 void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
           cudaStream_t s);

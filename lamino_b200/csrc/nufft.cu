@@ -14,6 +14,7 @@
 // into the kernels on either side of cuFFT, and so are the fftshift2 /
 // ifftshift2 index maps and the per-projection beam-vector weighting.
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "nufft.cuh"
@@ -83,17 +84,17 @@ NufftPlan::NufftPlan(Dims3 d, double eps_) : vol(d), eps(eps_) {
         std::vector<float> ip(N);
         for (int64_t i = 0; i < N; ++i) ip[i] = (float)(1.0 / p[i]);
         buf.alloc(N);
-        LAMINO_CUDA(cudaMemcpy(buf.p, ip.data(), N * 4, cudaMemcpyHostToDevice));
+        upload(buf.p, ip.data(), (size_t)N);
     };
     up(ip1, nf1, d.n1);
     up(ip2, nf2, d.n2);
     up(ip3, nf3, d.n3);
     gin.alloc(3 * nf());
     gwork.alloc(3 * nf());
-    LAMINO_CUDA(cudaMemset(gin.p, 0, gin.bytes()));
+    zero_bytes(gin.p, gin.bytes());
     int n[3] = {(int)nf1, (int)nf2, (int)nf3};
-    LAMINO_CUFFT(cufftPlanMany(&fft3.h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 1));
-    fft3.valid = true;
+    fft3.make(3, n, CUFFT_C2C, 1);
+    set_bins(8, 8, 8);
 }
 
 // ---------------------------------------------------------------------------
@@ -283,81 +284,364 @@ __device__ __forceinline__ void decode_pid(uint32_t pid, const GeomView &g, int 
     k = (int)(r - (uint32_t)j * (uint32_t)g.ncols);
 }
 
-// forward: P[fftshift2 position] = sum_i coeff_i(th) * N2(m_i)(point)
+// ---------------------------------------------------------------------------
+// bin sort: point ids grouped by the fine-grid bin of their footprint's first cell
+
+// first cell of the kernel footprint along one dimension, in [0, nf) (as es_taps)
 template <int W>
-__global__ void __launch_bounds__(256) k_interp_forward(GeomView g, const float2 *__restrict__ G,
-                                                        int64_t NF, Fine F, float2 *__restrict__ P) {
+__device__ __forceinline__ int es_start(float xc, int nf, double s) {
+    double u = (double)xc * s;
+    int64_t l = (int64_t)ceil(u - 0.5 * W);
+    l %= nf;
+    if (l < 0) l += nf;
+    return (int)l;
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t point_bin(const GeomView &g, const Fine &F, const BinLayout &B, uint32_t pid) {
+    int p, j, k;
+    decode_pid(pid, g, p, j, k);
+    float x, y, z;
+    point_xyz(g, p, j, k, x, y, z);
+    const int l1 = es_start<W>(z, F.nf1, F.s1), l2 = es_start<W>(y, F.nf2, F.s2), l3 = es_start<W>(x, F.nf3, F.s3);
+    return ((uint32_t)(l1 / B.b1) * (uint32_t)B.nb2 + (uint32_t)(l2 / B.b2)) * (uint32_t)B.nb3 +
+           (uint32_t)(l3 / B.b3);
+}
+
+// Consecutive point ids walk a projection row, so the lanes of a warp mostly
+// share a bin: one atomic per distinct bin in the warp.
+template <int W>
+__global__ void __launch_bounds__(256) k_bin_count(GeomView g, Fine F, BinLayout B, uint32_t *__restrict__ cnt) {
     const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
-    const int d1 = g.nrows / 2, d2 = g.ncols / 2;
+    const int lane = threadIdx.x & 31;
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
-        int p, j, k;
-        decode_pid(pid, g, p, j, k);
-        float x, y, z;
-        point_xyz(g, p, j, k, x, y, z);
-        float2 v[3];
-        interp_point<W, 3>(G, NF, F, x, y, z, v);
-        float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
-        float2 o = make_float2(c0 * v[0].x + c1 * v[1].x + c2 * v[2].x, c0 * v[0].y + c1 * v[1].y + c2 * v[2].y);
-        int js = j - d1; if (js < 0) js += g.nrows;
-        int ks = k - d2; if (ks < 0) ks += g.ncols;
-        P[((int64_t)p * g.nrows + js) * g.ncols + ks] = o;
+        const uint32_t bin = point_bin<W>(g, F, B, pid);
+        const unsigned grp = __match_any_sync(__activemask(), bin);
+        if (lane == __ffs(grp) - 1) atomicAdd(cnt + bin, (uint32_t)__popc(grp));
     }
 }
 
-// raw type 2 (one component), output in point order
 template <int W>
-__global__ void __launch_bounds__(256) k_interp_raw(GeomView g, const float2 *__restrict__ G, int64_t NF,
-                                                    Fine F, float2 *__restrict__ c) {
+__global__ void __launch_bounds__(256) k_bin_scatter(GeomView g, Fine F, BinLayout B, uint32_t *__restrict__ cursor,
+                                                     uint32_t *__restrict__ perm) {
     const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    const int lane = threadIdx.x & 31;
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
-        int p, j, k;
-        decode_pid(pid, g, p, j, k);
-        float x, y, z;
-        point_xyz(g, p, j, k, x, y, z);
-        float2 v[1];
-        interp_point<W, 1>(G, NF, F, x, y, z, v);
-        c[pid] = v[0];
+        const uint32_t bin = point_bin<W>(g, F, B, pid);
+        const unsigned grp = __match_any_sync(__activemask(), bin);
+        const int leader = __ffs(grp) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(cursor + bin, (uint32_t)__popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        perm[base + __popc(grp & ((1u << lane) - 1u))] = pid;
     }
 }
 
-// adjoint: spread coeff_i(th) * c into grid i, c read through ifftshift2
+// exclusive scan of the bin counts (one CTA of 1024 threads, 4096 bins per pass)
+__global__ void __launch_bounds__(1024) k_scan_offsets(const uint32_t *__restrict__ cnt, int n,
+                                                       uint32_t *__restrict__ start, uint32_t *__restrict__ cursor) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry_s;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 4096) {
+        const int i0 = base + threadIdx.x * 4;
+        uint32_t v[4], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            v[q] = i0 + q < n ? cnt[i0 + q] : 0u;
+            sum += v[q];
+        }
+        uint32_t x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        uint32_t e = carry_s + (wid ? wsum[wid - 1] : 0u) + x - sum;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (i0 + q < n) {
+                start[i0 + q] = e;
+                cursor[i0 + q] = e;
+            }
+            e += v[q];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s += wsum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[n] = carry_s;
+}
+
+// ---------------------------------------------------------------------------
+// binned spread / interpolation: one CTA per bin, the bin's tile of
+// (b + w - 1)^3 cells per component staged in shared memory
+
+struct BinOrigin {
+    int o1, o2, o3;
+};
+__device__ __forceinline__ BinOrigin bin_origin(const BinLayout &B, int bin) {
+    const int c3 = bin % B.nb3, r = bin / B.nb3;
+    const int c2 = r % B.nb2, c1 = r / B.nb2;
+    return BinOrigin{c1 * B.b1, c2 * B.b2, c3 * B.b3};
+}
+// fine-grid index of tile cell `cell` (wrapped)
+__device__ __forceinline__ int64_t tile_cell_index(const BinLayout &B, const BinOrigin &o, const Fine &F, int cell) {
+    const int i3 = cell % B.t3, r = cell / B.t3;
+    const int i2 = r % B.t2, i1 = r / B.t2;
+    const int g1 = (o.o1 + i1) % F.nf1, g2 = (o.o2 + i2) % F.nf2, g3 = (o.o3 + i3) % F.nf3;
+    return ((int64_t)g1 * F.nf2 + g2) * F.nf3 + g3;
+}
+
+// spread NC strengths at a point into NC tiles (shared float atomics); taps precomputed
+template <int W, int NC>
+__device__ __forceinline__ void spread_tile(float2 *tile, int tsz, const BinLayout &B, int a1, int a2, int a3,
+                                            const float *w1, const float *w2, const float *w3, const float2 *str) {
+#pragma unroll 1
+    for (int t1 = 0; t1 < W; ++t1) {
+#pragma unroll
+        for (int t2 = 0; t2 < W; ++t2) {
+            float *row = reinterpret_cast<float *>(tile + ((a1 + t1) * B.t2 + a2 + t2) * B.t3 + a3);
+            const float k12 = w1[t1] * w2[t2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const float sr = k12 * str[c].x, si = k12 * str[c].y;
+                float *rc = row + 2 * c * tsz;
+#pragma unroll
+                for (int t3 = 0; t3 < W; ++t3) {
+                    atomicAdd(rc + 2 * t3, w3[t3] * sr);
+                    atomicAdd(rc + 2 * t3 + 1, w3[t3] * si);
+                }
+            }
+        }
+    }
+}
+
+template <int W, int NC>
+__device__ __forceinline__ void gather_tile(const float2 *tile, int tsz, const BinLayout &B, int a1, int a2, int a3,
+                                            const float *w1, const float *w2, const float *w3, float2 *out) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int t1 = 0; t1 < W; ++t1) {
+#pragma unroll
+        for (int t2 = 0; t2 < W; ++t2) {
+            const float2 *row = tile + ((a1 + t1) * B.t2 + a2 + t2) * B.t3 + a3;
+            const float k12 = w1[t1] * w2[t2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                float rr = 0.f, ri = 0.f;
+#pragma unroll
+                for (int t3 = 0; t3 < W; ++t3) {
+                    const float2 v = row[c * tsz + t3];
+                    rr = fmaf(w3[t3], v.x, rr);
+                    ri = fmaf(w3[t3], v.y, ri);
+                }
+                out[c].x = fmaf(k12, rr, out[c].x);
+                out[c].y = fmaf(k12, ri, out[c].y);
+            }
+        }
+    }
+}
+
+// global-memory paths for a point outside its bin's tile (never taken when the
+// sort and the kernels agree on the taps); out of line to spare registers
+template <int W, int NC>
+__device__ __noinline__ void spread_point_global(float2 *H, int64_t NF, Fine F, float x, float y, float z,
+                                                 const float2 *str) {
+    spread_point<W, NC>(H, NF, F, x, y, z, str);
+}
+template <int W, int NC>
+__device__ __noinline__ void interp_point_global(const float2 *G, int64_t NF, Fine F, float x, float y, float z,
+                                                 float2 *out) {
+    interp_point<W, NC>(G, NF, F, x, y, z, out);
+}
+
+// taps of a point and its offset inside the bin's tile; false if the point lies
+// outside the bin (only possible if the sort and this kernel disagreed)
 template <int W>
-__global__ void __launch_bounds__(256) k_spread_adjoint(GeomView g, const float2 *__restrict__ Pf,
-                                                        float2 *__restrict__ H, int64_t NF, Fine F) {
-    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
-    const int e1 = (g.nrows + 1) / 2, e2 = (g.ncols + 1) / 2;
-    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
-        int p, j, k;
-        decode_pid(pid, g, p, j, k);
-        int js = j + e1; if (js >= g.nrows) js -= g.nrows;
-        int ks = k + e2; if (ks >= g.ncols) ks -= g.ncols;
-        float2 c = Pf[((int64_t)p * g.nrows + js) * g.ncols + ks];
-        float x, y, z;
-        point_xyz(g, p, j, k, x, y, z);
-        float2 s[3];
+__device__ __forceinline__ bool point_taps(const GeomView &g, const Fine &F, const BinLayout &B, const BinOrigin &o,
+                                           int p, int j, int k, float *w1, float *w2, float *w3, int &a1, int &a2,
+                                           int &a3, float &x, float &y, float &z) {
+    point_xyz(g, p, j, k, x, y, z);
+    const int l3 = es_taps<W>(x, F.nf3, F.s3, F.beta, w3);
+    const int l2 = es_taps<W>(y, F.nf2, F.s2, F.beta, w2);
+    const int l1 = es_taps<W>(z, F.nf1, F.s1, F.beta, w1);
+    a1 = l1 - o.o1;
+    a2 = l2 - o.o2;
+    a3 = l3 - o.o3;
+    return (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
+}
+
+// strength of a point for the adjoint: coeff_i(th) * P[ifftshift2 position]
+struct AdjointStrength {
+    const float2 *Pf;
+    __device__ __forceinline__ void operator()(const GeomView &g, int p, int j, int k, uint32_t, float2 *s) const {
+        int js = j + (g.nrows + 1) / 2; if (js >= g.nrows) js -= g.nrows;
+        int ks = k + (g.ncols + 1) / 2; if (ks >= g.ncols) ks -= g.ncols;
+        const float2 c = Pf[((int64_t)p * g.nrows + js) * g.ncols + ks];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-            float cq = __ldg(g.coeff + q * g.nproj + p);
+            const float cq = __ldg(g.coeff + q * g.nproj + p);
             s[q] = make_float2(cq * c.x, cq * c.y);
         }
-        spread_point<W, 3>(H, NF, F, x, y, z, s);
     }
-}
+};
+struct RawStrength {
+    const float2 *c;
+    __device__ __forceinline__ void operator()(const GeomView &, int, int, int, uint32_t pid, float2 *s) const {
+        s[0] = c[pid];
+    }
+};
+// forward: P[fftshift2 position] = sum_i coeff_i(th) * v_i
+struct ForwardSink {
+    float2 *P;
+    __device__ __forceinline__ void operator()(const GeomView &g, int p, int j, int k, uint32_t,
+                                               const float2 *v) const {
+        const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
+        const float2 o = make_float2(c0 * v[0].x + c1 * v[1].x + c2 * v[2].x, c0 * v[0].y + c1 * v[1].y + c2 * v[2].y);
+        int js = j - g.nrows / 2; if (js < 0) js += g.nrows;
+        int ks = k - g.ncols / 2; if (ks < 0) ks += g.ncols;
+        P[((int64_t)p * g.nrows + js) * g.ncols + ks] = o;
+    }
+};
+struct RawSink {
+    float2 *c;
+    __device__ __forceinline__ void operator()(const GeomView &, int, int, int, uint32_t pid, const float2 *v) const {
+        c[pid] = v[0];
+    }
+};
 
-template <int W>
-__global__ void __launch_bounds__(256) k_spread_raw(GeomView g, const float2 *__restrict__ c,
-                                                    float2 *__restrict__ H, int64_t NF, Fine F) {
-    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
-    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
+template <int W, int NC, class Str>
+__global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_t *__restrict__ perm,
+                                                       const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                       float2 *__restrict__ H, int64_t NF, Str str) {
+    extern __shared__ float2 tile[];
+    const int bin = blockIdx.x;
+    const uint32_t p0 = start[bin], p1 = start[bin + 1];
+    if (p0 == p1) return;
+    const BinOrigin o = bin_origin(B, bin);
+    const int tsz = (int)B.tile_cells();
+    for (int i = threadIdx.x; i < NC * tsz; i += blockDim.x) tile[i] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        const uint32_t pid = __ldg(perm + i);
         int p, j, k;
         decode_pid(pid, g, p, j, k);
-        float x, y, z;
-        point_xyz(g, p, j, k, x, y, z);
-        float2 s[1] = {c[pid]};
-        spread_point<W, 1>(H, NF, F, x, y, z, s);
+        float2 s[NC];
+        str(g, p, j, k, pid, s);
+        float w1[W], w2[W], w3[W], x, y, z;
+        int a1, a2, a3;
+        if (point_taps<W>(g, F, B, o, p, j, k, w1, w2, w3, a1, a2, a3, x, y, z))
+            spread_tile<W, NC>(tile, tsz, B, a1, a2, a3, w1, w2, w3, s);
+        else
+            spread_point_global<W, NC>(H, NF, F, x, y, z, s);
+    }
+    __syncthreads();
+    for (int cell = threadIdx.x; cell < tsz; cell += blockDim.x) {
+        const int64_t gi = tile_cell_index(B, o, F, cell);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const float2 v = tile[c * tsz + cell];
+            if (v.x != 0.f || v.y != 0.f) atomicAdd(H + c * NF + gi, v);
+        }
     }
 }
 
+template <int W, int NC, class Sink>
+__global__ void __launch_bounds__(256) k_interp_binned(GeomView g, const uint32_t *__restrict__ perm,
+                                                       const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                       const float2 *__restrict__ G, int64_t NF, Sink sink) {
+    extern __shared__ float2 tile[];
+    const int bin = blockIdx.x;
+    const uint32_t p0 = start[bin], p1 = start[bin + 1];
+    if (p0 == p1) return;
+    const BinOrigin o = bin_origin(B, bin);
+    const int tsz = (int)B.tile_cells();
+    for (int i = threadIdx.x; i < NC * tsz; i += blockDim.x) {
+        const int c = i / tsz, cell = i - c * tsz;
+        tile[i] = __ldg(G + c * NF + tile_cell_index(B, o, F, cell));
+    }
+    __syncthreads();
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        const uint32_t pid = __ldg(perm + i);
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float w1[W], w2[W], w3[W], x, y, z;
+        int a1, a2, a3;
+        float2 v[NC];
+        if (point_taps<W>(g, F, B, o, p, j, k, w1, w2, w3, a1, a2, a3, x, y, z))
+            gather_tile<W, NC>(tile, tsz, B, a1, a2, a3, w1, w2, w3, v);
+        else
+            interp_point_global<W, NC>(G, NF, F, x, y, z, v);
+        sink(g, p, j, k, pid, v);
+    }
+}
+
+// sysmat per point, binned: gather 3 components from the input tile, combine
+// with the beam vector, spread back into the output tile (src/gradient.cpp:34-89)
+template <int W>
+__global__ void __launch_bounds__(512) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
+                                                       const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                       const float2 *__restrict__ G, float2 *__restrict__ H,
+                                                       int64_t NF, float inv_scale) {
+    extern __shared__ float2 sm[];
+    const int bin = blockIdx.x;
+    const uint32_t p0 = start[bin], p1 = start[bin + 1];
+    if (p0 == p1) return;
+    const BinOrigin o = bin_origin(B, bin);
+    const int tsz = (int)B.tile_cells();
+    float2 *gt = sm, *ht = sm + 3 * tsz;
+    for (int i = threadIdx.x; i < 3 * tsz; i += blockDim.x) {
+        const int c = i / tsz, cell = i - c * tsz;
+        gt[i] = __ldg(G + c * NF + tile_cell_index(B, o, F, cell));
+        ht[i] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        const uint32_t pid = __ldg(perm + i);
+        int p, j, k;
+        decode_pid(pid, g, p, j, k);
+        float w1[W], w2[W], w3[W], x, y, z;
+        int a1, a2, a3;
+        const bool in = point_taps<W>(g, F, B, o, p, j, k, w1, w2, w3, a1, a2, a3, x, y, z);
+        float2 v[3];
+        if (in) gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, w1, w2, w3, v);
+        else interp_point_global<W, 3>(G, NF, F, x, y, z, v);
+        const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
+        const float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
+        const float si = (c0 * v[0].y + c1 * v[1].y + c2 * v[2].y) * inv_scale;
+        const float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
+                             make_float2(c2 * sr, c2 * si)};
+        if (in) spread_tile<W, 3>(ht, tsz, B, a1, a2, a3, w1, w2, w3, s);
+        else spread_point_global<W, 3>(H, NF, F, x, y, z, s);
+    }
+    __syncthreads();
+    for (int cell = threadIdx.x; cell < tsz; cell += blockDim.x) {
+        const int64_t gi = tile_cell_index(B, o, F, cell);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float2 v = ht[c * tsz + cell];
+            if (v.x != 0.f || v.y != 0.f) atomicAdd(H + c * NF + gi, v);
+        }
+    }
+}
+
+// direct (unsorted) sysmat per point, for calls that may not allocate a sorted order:
 // sysmat points: v_k = N2(x_k)(pt), s = sum_k c_k v_k, spread c_i s / (nrows ncols) into H_i
 template <int W>
 __global__ void __launch_bounds__(256) k_sysmat_points(GeomView g, const float2 *__restrict__ G,
@@ -474,23 +758,98 @@ void NufftPlan::ensure_proj(const Geom &g, cudaStream_t s) {
     if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
     if ((int64_t)pbuf.n < g.npts()) pbuf.alloc(g.npts());
     if (f2_np != g.nproj || f2_nr != g.nrows || f2_nc != g.ncols) {
-        if (fft2.valid) { cufftDestroy(fft2.h); fft2.valid = false; }
         int n[2] = {(int)g.nrows, (int)g.ncols};
-        LAMINO_CUFFT(cufftPlanMany(&fft2.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)g.nproj));
-        fft2.valid = true;
+        fft2.make(2, n, CUFFT_C2C, (int)g.nproj);
         f2_np = g.nproj; f2_nr = g.nrows; f2_nc = g.ncols;
     }
 }
 
+// width as a compile-time constant for a generic lambda
+template <class Fn>
+static void with_width(int w, Fn &&fn) {
+    switch (w) {
+        case 4: fn(std::integral_constant<int, 4>{}); break;
+        case 5: fn(std::integral_constant<int, 5>{}); break;
+        case 6: fn(std::integral_constant<int, 6>{}); break;
+        case 7: fn(std::integral_constant<int, 7>{}); break;
+        case 8: fn(std::integral_constant<int, 8>{}); break;
+        default: throw Error(ERR_ARG, "unsupported kernel width");
+    }
+}
+
+void NufftPlan::set_bins(int b1, int b2, int b3) {
+    if (b1 <= 0 || b2 <= 0 || b3 <= 0) throw Error(ERR_ARG, "bin sizes must be positive");
+    BinLayout B;
+    B.b1 = b1; B.b2 = b2; B.b3 = b3;
+    B.nb1 = (int)((nf1 + b1 - 1) / b1);
+    B.nb2 = (int)((nf2 + b2 - 1) / b2);
+    B.nb3 = (int)((nf3 + b3 - 1) / b3);
+    B.t1 = b1 + w - 1; B.t2 = b2 + w - 1; B.t3 = b3 + w - 1;
+    if (B.nbins() > (int64_t)INT32_MAX - 1) throw Error(ERR_ARG, "too many bins");
+    if (6 * B.tile_cells() * (int64_t)sizeof(float2) > 227 * 1024) throw Error(ERR_ARG, "bin tile too large");
+    bins = B;
+    drop_sorted();
+}
+
+const SortedPoints *NufftPlan::find_sorted(const Geom &g) const {
+    for (const auto &sp : sorted)
+        if (sp->uid == g.uid) return sp.get();
+    return nullptr;
+}
+
+const SortedPoints &NufftPlan::sort_points(const Geom &g, cudaStream_t s) {
+    for (auto &sp : sorted)
+        if (sp->uid == g.uid) {
+            sp->last_use = ++use_clock;
+            return *sp;
+        }
+    if ((int)sorted.size() >= kMaxSorted) {
+        size_t lru = 0;
+        for (size_t i = 1; i < sorted.size(); ++i)
+            if (sorted[i]->last_use < sorted[lru]->last_use) lru = i;
+        sorted.erase(sorted.begin() + (long)lru);
+    }
+    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    auto sp = std::make_unique<SortedPoints>();
+    sp->uid = g.uid;
+    const int64_t nb = bins.nbins();
+    DevBuf<uint32_t> cnt(nb), cursor(nb);
+    sp->start.alloc(nb + 1);
+    sp->perm.alloc(g.npts());
+    LAMINO_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), s));
+    const Fine F = fine_of(*this);
+    const GeomView gv = g.view();
+    const unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    with_width(w, [&](auto WC) {
+        constexpr int W = decltype(WC)::value;
+        k_bin_count<W><<<grid, 256, 0, s>>>(gv, F, bins, cnt.p);
+        LAMINO_LAUNCH("k_bin_count");
+        k_scan_offsets<<<1, 1024, 0, s>>>(cnt.p, (int)nb, sp->start.p, cursor.p);
+        LAMINO_LAUNCH("k_scan_offsets");
+        k_bin_scatter<W><<<grid, 256, 0, s>>>(gv, F, bins, cursor.p, sp->perm.p);
+        LAMINO_LAUNCH("k_bin_scatter");
+    });
+    sp->last_use = ++use_clock;
+    sorted.push_back(std::move(sp));
+    return *sorted.back();
+}
+
 void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_t s) {
     ensure_proj(g, s);
+    const SortedPoints &sp = sort_points(g, s);
     pad_real(m3, 3, s);
     fft_fine(-1, 3, s);
-    Fine F = fine_of(*this);
-    GeomView gv = g.view();
-    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
-    LAMINO_W_DISPATCH(w, k_interp_forward, grid, 256, s, gv, gwork.p, nf(), F, pbuf.p);
-    LAMINO_LAUNCH("k_interp_forward");
+    const Fine F = fine_of(*this);
+    const GeomView gv = g.view();
+    const int smem = (int)(3 * bins.tile_cells() * sizeof(float2));
+    with_width(w, [&](auto WC) {
+        constexpr int W = decltype(WC)::value;
+        auto kern = k_interp_binned<W, 3, ForwardSink>;
+        raise_smem_limit((const void *)kern, smem);
+        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
+                                                        ForwardSink{pbuf.p});
+        LAMINO_LAUNCH("k_interp_binned<forward>");
+    });
     LAMINO_CUFFT(cufftSetStream(fft2.h, s));
     LAMINO_CUFFT(cufftExecC2C(fft2.h, (cufftComplex *)pbuf.p, (cufftComplex *)pbuf.p, CUFFT_INVERSE));
     float scale = 1.0f / (float)(g.nrows * g.ncols);
@@ -500,61 +859,75 @@ void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_
 
 void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumulate, cudaStream_t s) {
     ensure_proj(g, s);
+    const SortedPoints &sp = sort_points(g, s);
     k_proj_pre<<<grid_for(g.npts(), 256), 256, 0, s>>>(proj, (int)g.nproj, (int)g.nrows, (int)g.ncols, pbuf.p);
     LAMINO_LAUNCH("k_proj_pre");
     LAMINO_CUFFT(cufftSetStream(fft2.h, s));
     LAMINO_CUFFT(cufftExecC2C(fft2.h, (cufftComplex *)pbuf.p, (cufftComplex *)pbuf.p, CUFFT_FORWARD));
     LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, gwork.bytes(), s));
-    Fine F = fine_of(*this);
-    GeomView gv = g.view();
-    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
-    LAMINO_W_DISPATCH(w, k_spread_adjoint, grid, 256, s, gv, pbuf.p, gwork.p, nf(), F);
-    LAMINO_LAUNCH("k_spread_adjoint");
+    const Fine F = fine_of(*this);
+    const GeomView gv = g.view();
+    const int smem = (int)(3 * bins.tile_cells() * sizeof(float2));
+    with_width(w, [&](auto WC) {
+        constexpr int W = decltype(WC)::value;
+        auto kern = k_spread_binned<W, 3, AdjointStrength>;
+        raise_smem_limit((const void *)kern, smem);
+        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
+                                                        AdjointStrength{pbuf.p});
+        LAMINO_LAUNCH("k_spread_binned<adjoint>");
+    });
     fft_fine(+1, 3, s);
     extract_real(m3, 3, 1.0f / (float)(g.nrows * g.ncols), accumulate, s);
 }
 
+// sysmat of every geometry, accumulated into gin after the forward FFT of x;
+// `may_sort`: build missing point orders (allocates) or fall back to the direct kernel
+void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cudaStream_t s) {
+    const Fine F = fine_of(*this);
+    const int smem = (int)(6 * bins.tile_cells() * sizeof(float2));
+    for (int i = 0; i < ng; ++i) {
+        const Geom &g = *gs[i];
+        if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+        const GeomView gv = g.view();
+        const float inv_scale = 1.0f / (float)(g.nrows * g.ncols);
+        const SortedPoints *sp = may_sort ? &sort_points(g, s) : find_sorted(g);
+        with_width(w, [&](auto WC) {
+            constexpr int W = decltype(WC)::value;
+            if (sp) {
+                auto kern = k_sysmat_binned<W>;
+                raise_smem_limit((const void *)kern, smem);
+                kern<<<(unsigned)bins.nbins(), 512, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p, gin.p,
+                                                                nf(), inv_scale);
+                LAMINO_LAUNCH("k_sysmat_binned");
+            } else {
+                unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+                k_sysmat_points<W><<<grid, 256, 0, s>>>(gv, gwork.p, gin.p, nf(), F, inv_scale);
+                LAMINO_LAUNCH("k_sysmat_points");
+            }
+        });
+    }
+}
+
 void NufftPlan::normal(const std::vector<const Geom *> &gs, const float *x3, float *y3, cudaStream_t s) {
     if (gs.empty()) throw Error(ERR_ARG, "normal operator needs at least one geometry");
-    pad_real(x3, 3, s);
-    // forward fine-grid spectra go to gwork; accumulate the spread into gin's
-    // companion: reuse gin after its FFT (re-zeroed below for the next pad).
-    fft_fine(-1, 3, s);
-    // spread target: gin (zeroed) -- gin must be re-zeroed before the next pad_real
-    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
-    Fine F = fine_of(*this);
-    for (const Geom *g : gs) {
-        if (g->npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
-        GeomView gv = g->view();
-        unsigned grid = grid_for(g->npts(), 256, 148LL * 16 * 8);
-        float inv_scale = 1.0f / (float)(g->nrows * g->ncols);
-        LAMINO_W_DISPATCH(w, k_sysmat_points, grid, 256, s, gv, gwork.p, gin.p, nf(), F, inv_scale);
-        LAMINO_LAUNCH("k_sysmat_points");
-    }
-    // inverse FFT of the accumulated spread (in gin), then extract
-    LAMINO_CUFFT(cufftSetStream(fft3.h, s));
-    for (int c = 0; c < 3; ++c)
-        LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gin.p + c * nf()),
-                                  (cufftComplex *)(gwork.p + c * nf()), CUFFT_INVERSE));
-    extract_real(y3, 3, 1.0f, false, s);
-    LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
+    for (const Geom *g : gs) sort_points(*g, s);  // before any work on the grids
+    normal_impl(gs.data(), (int)gs.size(), true, x3, y3, s);
 }
 
 void NufftPlan::normal_ptrs(const Geom *const *gs, int ng, const float *x3, float *y3, cudaStream_t s) {
     if (!gs || ng <= 0) throw Error(ERR_ARG, "normal operator needs at least one geometry");
+    normal_impl(gs, ng, false, x3, y3, s);
+}
+
+void NufftPlan::normal_impl(const Geom *const *gs, int ng, bool may_sort, const float *x3, float *y3,
+                            cudaStream_t s) {
     for (int i = 0; i < ng; ++i)
-        if (gs[i]->npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+        if (!gs[i] || gs[i]->npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "bad geometry");
     pad_real(x3, 3, s);
+    // forward fine-grid spectra go to gwork; the spread accumulates in gin (zeroed after its FFT)
     fft_fine(-1, 3, s);
     LAMINO_CUDA(cudaMemsetAsync(gin.p, 0, gin.bytes(), s));
-    Fine F = fine_of(*this);
-    for (int i = 0; i < ng; ++i) {
-        GeomView gv = gs[i]->view();
-        unsigned grid = grid_for(gs[i]->npts(), 256, 148LL * 16 * 8);
-        float inv_scale = 1.0f / (float)(gs[i]->nrows * gs[i]->ncols);
-        LAMINO_W_DISPATCH(w, k_sysmat_points, grid, 256, s, gv, gwork.p, gin.p, nf(), F, inv_scale);
-        LAMINO_LAUNCH("k_sysmat_points");
-    }
+    normal_points(gs, ng, may_sort, s);
     LAMINO_CUFFT(cufftSetStream(fft3.h, s));
     for (int c = 0; c < 3; ++c)
         LAMINO_CUFFT(cufftExecC2C(fft3.h, (cufftComplex *)(gin.p + c * nf()),
@@ -564,24 +937,35 @@ void NufftPlan::normal_ptrs(const Geom *const *gs, int ng, const float *x3, floa
 }
 
 void NufftPlan::type2(const Geom &g, const float2 *modes, float2 *c, cudaStream_t s) {
-    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    const SortedPoints &sp = sort_points(g, s);
     pad_complex(modes, s);
     fft_fine(-1, 1, s);
-    Fine F = fine_of(*this);
-    GeomView gv = g.view();
-    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
-    LAMINO_W_DISPATCH(w, k_interp_raw, grid, 256, s, gv, gwork.p, nf(), F, c);
-    LAMINO_LAUNCH("k_interp_raw");
+    const Fine F = fine_of(*this);
+    const GeomView gv = g.view();
+    const int smem = (int)(bins.tile_cells() * sizeof(float2));
+    with_width(w, [&](auto WC) {
+        constexpr int W = decltype(WC)::value;
+        auto kern = k_interp_binned<W, 1, RawSink>;
+        raise_smem_limit((const void *)kern, smem);
+        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(), RawSink{c});
+        LAMINO_LAUNCH("k_interp_binned<raw>");
+    });
 }
 
 void NufftPlan::type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_t s) {
-    if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
+    const SortedPoints &sp = sort_points(g, s);
     LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, nf() * sizeof(float2), s));
-    Fine F = fine_of(*this);
-    GeomView gv = g.view();
-    unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
-    LAMINO_W_DISPATCH(w, k_spread_raw, grid, 256, s, gv, c, gwork.p, nf(), F);
-    LAMINO_LAUNCH("k_spread_raw");
+    const Fine F = fine_of(*this);
+    const GeomView gv = g.view();
+    const int smem = (int)(bins.tile_cells() * sizeof(float2));
+    with_width(w, [&](auto WC) {
+        constexpr int W = decltype(WC)::value;
+        auto kern = k_spread_binned<W, 1, RawStrength>;
+        raise_smem_limit((const void *)kern, smem);
+        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
+                                                        RawStrength{c});
+        LAMINO_LAUNCH("k_spread_binned<raw>");
+    });
     fft_fine(+1, 1, s);
     k_extract_complex<<<grid_for(vol.size(), 256), 256, 0, s>>>(gwork.p, (int)vol.n1, (int)vol.n2, (int)vol.n3,
                                                                   modes, F, ip1.p, ip2.p, ip3.p);

@@ -2,6 +2,7 @@
 // projection-space stages of the forward and adjoint operators.
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -17,6 +18,26 @@ inline int es_width(double eps) {
 }
 int64_t next_smooth_even(int64_t n);
 
+// Partition of the fine grid into bins of b1 x b2 x b3 cells.  A point belongs
+// to the bin holding the first cell of its kernel footprint, so its w^3 taps
+// stay inside the bin's tile of (b + w - 1) cells per dimension, which one CTA
+// stages in shared memory.
+struct BinLayout {
+    int b1 = 8, b2 = 8, b3 = 8;
+    int nb1 = 0, nb2 = 0, nb3 = 0;
+    int t1 = 0, t2 = 0, t3 = 0;
+    __host__ __device__ int64_t nbins() const { return (int64_t)nb1 * nb2 * nb3; }
+    __host__ __device__ int64_t tile_cells() const { return (int64_t)t1 * t2 * t3; }
+};
+
+// Point ids of one geometry grouped by bin (counting sort), with bin offsets.
+struct SortedPoints {
+    uint64_t uid = 0;
+    uint64_t last_use = 0;
+    DevBuf<uint32_t> perm;   // npts
+    DevBuf<uint32_t> start;  // nbins + 1
+};
+
 struct NufftPlan {
     Dims3 vol;                // recon volume (n1, n2, n3), n3 fastest
     int64_t nf1, nf2, nf3;    // fine grid paired with n1 (z), n2 (y), n3 (x)
@@ -31,10 +52,21 @@ struct NufftPlan {
     DevBuf<float2> pbuf;
     FftPlan fft2;
     int64_t f2_np = -1, f2_nr = -1, f2_nc = -1;
+    // bin-sorted point orders of the geometries used with this plan (bounded LRU)
+    BinLayout bins;
+    std::vector<std::unique_ptr<SortedPoints>> sorted;
+    uint64_t use_clock = 0;
+    static constexpr int kMaxSorted = 16;
 
     NufftPlan(Dims3 d, double eps);
     int64_t nf() const { return nf1 * nf2 * nf3; }
     void ensure_proj(const Geom &g, cudaStream_t s);
+    // bin layout for b1 x b2 x b3 bins (drops cached point orders)
+    void set_bins(int b1, int b2, int b3);
+    // the geometry's bin-sorted order (built on first use, then cached)
+    const SortedPoints &sort_points(const Geom &g, cudaStream_t s);
+    const SortedPoints *find_sorted(const Geom &g) const;
+    void drop_sorted() { sorted.clear(); }
 
     // --- operators (device pointers; volumes are 3 contiguous components) ---
     // forward projection (src/projection.cpp:42-77)
@@ -50,6 +82,8 @@ struct NufftPlan {
     void type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_t s);
 
     // internals
+    void normal_impl(const Geom *const *gs, int ng, bool may_sort, const float *x3, float *y3, cudaStream_t s);
+    void normal_points(const Geom *const *gs, int ng, bool may_sort, cudaStream_t s);
     void pad_real(const float *x3, int ncomp, cudaStream_t s);
     void pad_complex(const float2 *f, cudaStream_t s);
     void fft_fine(int sign, int ncomp, cudaStream_t s);

@@ -15,7 +15,14 @@ Server::Server(int64_t budget, int slots, bool dry_run, double dry_run_ms)
     if (budget <= 0) throw Error(ERR_ARG, "server budget must be positive");
     if (slots <= 0 || slots > 256) throw Error(ERR_ARG, "server slots must be 1..256");
     int dev = 0;
-    if (!dry_) LAMINO_CUDA(cudaGetDevice(&dev));
+    if (!dry_) {
+        LAMINO_CUDA(cudaGetDevice(&dev));
+        // keep up to the budget cached in the stream-ordered pool between requests
+        cudaMemPool_t pool;
+        LAMINO_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        uint64_t keep = (uint64_t)budget;
+        LAMINO_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     for (int i = 0; i < slots; ++i)
         workers_.emplace_back([this, dev, i]() {
             if (!dry_) cudaSetDevice(dev);
@@ -39,7 +46,7 @@ int64_t Server::submit(std::unique_ptr<ServeRequest> r) {
     std::lock_guard<std::mutex> lk(mu_);
     if (stop_) throw Error(ERR_STATE, "server is shutting down");
     r->id = next_id_++;
-    r->t_submit = now();
+    if (r->t_submit == 0) r->t_submit = now();
     const int64_t id = r->id;
     reqs_[id] = std::move(r);
     queue_.push_back(id);
@@ -81,6 +88,7 @@ void Server::worker(int wid) {
                 r->result.assign((size_t)nv, 0.f);
             } else {
                 if (!s) throw Error(ERR_CUDA, "worker stream creation failed");
+                AllocStreamScope scope(s);
                 std::vector<DevBuf<float>> dp(r->projs.size());
                 std::vector<Dataset> data;
                 for (size_t i = 0; i < r->projs.size(); ++i) {
@@ -92,6 +100,7 @@ void Server::worker(int wid) {
                 }
                 DevBuf<float> out(nv);
                 mbir(r->method, data, r->recon, r->prm, out.p, s);
+                r->phases = last_mbir_phases();
                 r->result.resize((size_t)nv);
                 LAMINO_CUDA(cudaMemcpyAsync(r->result.data(), out.p, nv * 4, cudaMemcpyDeviceToHost, s));
                 LAMINO_CUDA(cudaStreamSynchronize(s));

@@ -35,6 +35,7 @@ struct ServeRequest {
     int64_t footprint = 0;
     std::vector<float> result;  // 3 * recon voxels, host
     double t_submit = 0, t_start = 0, t_done = 0;
+    MbirPhases phases;
     int status = 0;
     std::string err;
     bool done = false;
@@ -56,15 +57,17 @@ class Server {
     Server(const Server &) = delete;
     Server &operator=(const Server &) = delete;
 
+    // r->t_submit, when already set, is kept (the caller's arrival time)
     int64_t submit(std::unique_ptr<ServeRequest> r);
     // blocks until the request finished (or timeout_s elapsed: returns false)
     bool wait(int64_t id, double timeout_s, ServeRequest **out);
     void release(int64_t id);  // forget a finished request
     ServerStats stats();
 
+    static double now();  // steady-clock seconds
+
   private:
     void worker(int wid);
-    static double now();
 
     int64_t budget_;
     int slots_;

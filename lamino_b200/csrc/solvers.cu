@@ -3,7 +3,9 @@
 // Arithmetic follows the reference's float expressions element by element
 // (including where it promotes to double); reductions use FP64 accumulation
 // with warp-shuffle trees instead of the reference's serial float sums.
+#include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "solvers.cuh"
@@ -14,13 +16,39 @@ namespace lamino {
 // reductions
 // ---------------------------------------------------------------------------
 
+namespace {
+// Pinned host blocks of the calling thread, kept for reuse until it exits.
+struct PinnedCache {
+    std::vector<std::pair<double *, int>> free_;
+    double *take(int n) {
+        for (size_t i = 0; i < free_.size(); ++i)
+            if (free_[i].second >= n) {
+                double *p = free_[i].first;
+                free_.erase(free_.begin() + (long)i);
+                return p;
+            }
+        double *p = nullptr;
+        LAMINO_CUDA(cudaMallocHost((void **)&p, sizeof(double) * std::max(n, 64)));
+        return p;
+    }
+    void give(double *p, int n) { free_.emplace_back(p, std::max(n, 64)); }
+    ~PinnedCache() {
+        for (auto &b : free_) cudaFreeHost(b.first);
+    }
+};
+PinnedCache &pinned_cache() {
+    static thread_local PinnedCache c;
+    return c;
+}
+}  // namespace
+
 Reducer::Reducer(int n) : cap(n) {
-    LAMINO_CUDA(cudaMalloc((void **)&d, sizeof(double) * n));
-    LAMINO_CUDA(cudaMallocHost((void **)&h, sizeof(double) * n));
+    dbuf.alloc((size_t)n);
+    d = dbuf.p;
+    h = pinned_cache().take(n);
 }
 Reducer::~Reducer() {
-    if (d) cudaFree(d);
-    if (h) cudaFreeHost(h);
+    if (h) pinned_cache().give(h, cap);
 }
 void Reducer::zero(int n, cudaStream_t s) { LAMINO_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, s)); }
 void Reducer::fetch(int n, cudaStream_t s) {
@@ -332,13 +360,11 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
     for (int64_t j = 0; j < n2; ++j)
         for (int64_t i = 0; i < h3; ++i) f[j * h3 + i] = std::sqrt(xf[i] * xf[i] + yf[j] * yf[j]) * scale;
     filt.alloc(n2 * h3);
-    LAMINO_CUDA(cudaMemcpy(filt.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    upload(filt.p, f.data(), f.size());
     spec.alloc(3 * d.n1 * n2 * h3);
     int n[2] = {(int)n2, (int)n3};
-    LAMINO_CUFFT(cufftPlanMany(&r2c.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, (int)(3 * d.n1)));
-    r2c.valid = true;
-    LAMINO_CUFFT(cufftPlanMany(&c2r.h, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, (int)(3 * d.n1)));
-    c2r.valid = true;
+    r2c.make(2, n, CUFFT_R2C, (int)(3 * d.n1));
+    c2r.make(2, n, CUFFT_C2R, (int)(3 * d.n1));
 }
 
 void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {

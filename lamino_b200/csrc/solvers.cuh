@@ -13,8 +13,9 @@ using OpFn = std::function<void(const float *x3, float *y3, cudaStream_t)>;
 // Device scalar scratch for FP64 reductions (pinned host mirror).
 struct Reducer {
     double *d = nullptr;   // device accumulators
-    double *h = nullptr;   // pinned host copy
+    double *h = nullptr;   // pinned host copy (from a per-thread cache: cudaFreeHost waits for the device)
     int cap = 0;
+    DevBuf<double> dbuf;
     explicit Reducer(int n = 16);
     ~Reducer();
     Reducer(const Reducer &) = delete;

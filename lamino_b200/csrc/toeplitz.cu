@@ -468,6 +468,11 @@ std::vector<int> fft_positions(int n, const std::vector<int> &radix) {
     return pos;
 }
 
+__global__ void k_add_into(float *a, const float *b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] += b[i];
+}
+
 // The dynamic shared-memory limit is a per-function attribute shared by every
 // operator (and host thread) of the process on a device: it is only ever raised,
 // under a lock, so an operator built concurrently for a smaller volume cannot
@@ -501,7 +506,7 @@ static FftLen make_len(int n, bool lead2, DevBuf<float2> &tw, std::vector<int> *
         h[e] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     tw.alloc(n);
-    LAMINO_CUDA(cudaMemcpy(tw.p, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    upload(tw.p, h.data(), (size_t)n);
     F.tw = tw.p;
     if (radix_out) *radix_out = r;
     return F;
@@ -512,8 +517,7 @@ static int64_t embed_len(int64_t n) {
     return next_smooth_even(2 * n);
 }
 
-Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaStream_t s) : vol(d), precision(prec) {
-    if (gs.empty()) throw Error(ERR_ARG, "Toeplitz operator needs at least one geometry");
+void Toeplitz::init_tables(Dims3 d, int prec) {
     if (d.n1 <= 0 || d.n2 <= 0 || d.n3 <= 0) throw Error(ERR_ARG, "volume dims must be positive");
     if (prec != PREC_FP32 && prec != PREC_FP16 && prec != PREC_MIXED)
         throw Error(ERR_ARG, "precision must be 0 (fp32), 1 (fp16) or 2 (mixed)");
@@ -537,20 +541,27 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
             h[k] = make_float2((float)std::cos(a), (float)std::sin(a));
         }
         twh3.alloc(M3 + 1);
-        LAMINO_CUDA(cudaMemcpy(twh3.p, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        upload(twh3.p, h.data(), h.size());
         std::vector<int> p3 = fft_positions((int)M3, r3);
         pos3.alloc(M3);
-        LAMINO_CUDA(cudaMemcpy(pos3.p, p3.data(), M3 * sizeof(int), cudaMemcpyHostToDevice));
+        upload(pos3.p, p3.data(), (size_t)M3);
     }
+    r1_ = r1;
+    r2_ = r2;
+}
+
+Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaStream_t s) : vol(d), precision(prec) {
+    if (gs.empty()) throw Error(ERR_ARG, "Toeplitz operator needs at least one geometry");
+    init_tables(d, prec);
     std::vector<int> nat1(L1), nat2(L2);
     {
-        std::vector<int> p1 = fft_positions((int)L1, r1), p2 = fft_positions((int)L2, r2);
+        std::vector<int> p1 = fft_positions((int)L1, r1_), p2 = fft_positions((int)L2, r2_);
         for (int k = 0; k < (int)L1; ++k) nat1[p1[k]] = k;
         for (int k = 0; k < (int)L2; ++k) nat2[p2[k]] = k;
     }
     DevBuf<int> dnat1(L1), dnat2(L2);
-    LAMINO_CUDA(cudaMemcpy(dnat1.p, nat1.data(), L1 * sizeof(int), cudaMemcpyHostToDevice));
-    LAMINO_CUDA(cudaMemcpy(dnat2.p, nat2.data(), L2 * sizeof(int), cudaMemcpyHostToDevice));
+    upload(dnat1.p, nat1.data(), (size_t)L1);
+    upload(dnat2.p, nat2.data(), (size_t)L2);
 
     // geometry tables in double
     std::vector<TGam> hg;
@@ -593,8 +604,7 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     // one-off uniform R2C per pair (cuFFT), real part stored in apply order
     FftPlan r2c;
     int n[3] = {(int)L1, (int)L2, (int)L3};
-    LAMINO_CUFFT(cufftPlanMany(&r2c.h, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, 1));
-    r2c.valid = true;
+    r2c.make(3, n, CUFFT_R2C, 1);
     LAMINO_CUFFT(cufftSetStream(r2c.h, s));
     DevBuf<float2> spec(Ssize());
     K.alloc(6 * Ssize());
@@ -605,6 +615,33 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
                                                                  dnat2.p, q, norm, K.p);
         LAMINO_LAUNCH("k_take_real_perm");
     }
+    T.release();
+    spec.release();
+    finish(s);
+}
+
+// Sum of operators over disjoint geometry sets: the kernel is linear in the
+// geometry, so its spectra add.
+Toeplitz::Toeplitz(const std::vector<const Toeplitz *> &parts, int prec, cudaStream_t s)
+    : vol(parts.empty() ? Dims3{0, 0, 0} : parts[0]->vol), precision(prec) {
+    if (parts.empty()) throw Error(ERR_ARG, "Toeplitz sum needs at least one operator");
+    for (const Toeplitz *t : parts) {
+        if (!t || !t->has_fp32()) throw Error(ERR_ARG, "Toeplitz sum needs operators with FP32 spectra");
+        if (t->vol.n1 != vol.n1 || t->vol.n2 != vol.n2 || t->vol.n3 != vol.n3)
+            throw Error(ERR_ARG, "Toeplitz sum needs operators of one volume size");
+    }
+    init_tables(vol, prec);
+    K.alloc(6 * Ssize());
+    LAMINO_CUDA(cudaMemcpyAsync(K.p, parts[0]->K.p, K.bytes(), cudaMemcpyDeviceToDevice, s));
+    for (size_t i = 1; i < parts.size(); ++i) {
+        k_add_into<<<grid_for(6 * Ssize(), 256), 256, 0, s>>>(K.p, parts[i]->K.p, 6 * Ssize());
+        LAMINO_LAUNCH("k_add_into");
+    }
+    finish(s);
+}
+
+void Toeplitz::finish(cudaStream_t s) {
+    const Dims3 d = vol;
     if (precision != PREC_FP32) {
         Kh.alloc(6 * Ssize());
         Kscale.alloc(L2 * L3h);
@@ -615,8 +652,6 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
     }
     LAMINO_CUDA(cudaStreamSynchronize(s));
     if (precision == PREC_FP16) K.release();
-    T.release();
-    spec.release();
 
     // intermediates and launch shapes
     n1p = (d.n1 + D2_IB - 1) / D2_IB * D2_IB;

@@ -43,7 +43,16 @@ struct Toeplitz {
     std::vector<cudaEvent_t> ev;      // NSTAGE+1 events per profiled apply
     int nprof = 0;
 
+  private:
+    std::vector<int> r1_, r2_;  // radix schedules of L1 and L2
+    void init_tables(Dims3 d, int precision);
+    void finish(cudaStream_t s);  // FP16 spectra, intermediates, launch shapes
+
+  public:
+
     Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int precision, cudaStream_t s);
+    // the operator of the union of the parts' geometries, from their FP32 spectra
+    Toeplitz(const std::vector<const Toeplitz *> &parts, int precision, cudaStream_t s);
     ~Toeplitz();
     int64_t Lsize() const { return L1 * L2 * L3; }
     int64_t Ssize() const { return L1 * L2 * L3h; }

@@ -70,6 +70,40 @@ def test_operators_vs_oracle(L, O, dims, geoms):
     assert rel(L.sysmat(xr, pgs), O.normal(xr, opgs, [p.gamma for p in opgs], plan_o)) < TOL
 
 
+@pytest.mark.parametrize("bins", [(8, 8, 8), (4, 4, 4), (16, 2, 8), (3, 5, 7), (4, 16, 4)])
+def test_bin_layouts_vs_oracle(L, O, bins):
+    """Spreading / interpolation give the oracle's result for any bin layout,
+    including bins larger than the fine grid (tiles wrapping onto themselves)."""
+    dims, geoms = CASES[0]
+    rng = np.random.default_rng(21)
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    plan = L.NufftPlan(dims).set_bins(*bins)
+    pgs, opgs = [], []
+    for np_, nr, nc, g in geoms:
+        th = rng.uniform(0, 2 * np.pi, np_).astype(np.float32)
+        pgs.append(L.PolarGrid(th, nr, nc, np.float32(g)))
+        opgs.append(O.PolarGrid(th, nr, nc, np.float32(g)))
+    m = rng.standard_normal((3,) + dims).astype(np.float32)
+    for pg, opg in zip(pgs, opgs):
+        assert rel(L.forward(m, pg, plan=plan), O.forward(m, opg, opg.gamma, plan_o)) < TOL
+        proj = rng.standard_normal(opg.dims()).astype(np.float32)
+        assert rel(L.adjoint(proj, pg, dims, plan=plan), O.adjoint(proj, opg, dims, opg.gamma, plan_o)) < TOL
+    assert rel(L.sysmat(m, pgs, plan=plan), O.normal(m, opgs, [p.gamma for p in opgs], plan_o)) < TOL
+    f = (rng.standard_normal(dims) + 1j * rng.standard_normal(dims)).astype(np.complex64)
+    c = L.nufft3d2(f, pgs[1], plan=plan)
+    assert rel(c, O.nufft3d2(f.astype(np.complex128), opgs[1], plan_o)) < TOL
+    assert rel(L.nufft3d1(c, pgs[1], dims, plan=plan),
+               O.nufft3d1(c.astype(np.complex128), opgs[1], plan_o)) < TOL
+
+
+def test_bin_layout_rejects_bad_sizes(L):
+    plan = L.NufftPlan((8, 6, 8))
+    with pytest.raises(L.LaminoError):
+        plan.set_bins(0, 8, 8)
+    with pytest.raises(L.LaminoError):
+        plan.set_bins(40, 40, 40)  # tile beyond shared memory
+
+
 @pytest.mark.parametrize("dims,geoms", CASES)
 def test_toeplitz_vs_oracle(L, O, dims, geoms):
     rng = np.random.default_rng(12)
