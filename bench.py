@@ -420,8 +420,8 @@ def serve_data(torch, L, spec):
 def serve_params(L, spec, form: str):
     kw = dict(op_kind="toeplitz", use_graphs=False) if form == "plain" else \
         dict(op_kind="toeplitz", use_graphs=True)
-    if spec["method"] == 3:
-        return L.ReconParams(maxIters=SERVE_ITERS, sigma=1000.0, p=1.2, **kw)
+    if spec["method"] == 3:  # mu = 0: Lipschitz constant from 30 power iterations
+        return L.ReconParams(maxIters=SERVE_ITERS, sigma=1000.0, p=1.2, mu=0.0, **kw)
     return L.ReconParams(maxIters=50, innerIters=3, lam=0.1, mu=10.0, **kw)
 
 
@@ -435,7 +435,7 @@ def run_plain_loop(L, specs, data, arrivals):
     launches): returns results, latencies (arrival -> done), service times and
     applies."""
     fns = {1: L.MBIR1, 2: L.MBIR2, 3: L.MBIR3}
-    res, lat, svc, app = [], [], [], []
+    res, lat, svc, app, ph = [], [], [], [], []
     t0 = time.perf_counter()
     for i, (sp, d) in enumerate(zip(specs, data)):
         now = time.perf_counter() - t0
@@ -446,8 +446,9 @@ def run_plain_loop(L, specs, data, arrivals):
         b = time.perf_counter()
         svc.append(b - a)
         lat.append(b - t0 - arrivals[i])
-        app.append(L.mbir_phases()["applies"])
-    return res, lat, svc, app, time.perf_counter() - t0
+        ph.append(L.mbir_phases())
+        app.append(ph[-1]["applies"])
+    return res, lat, svc, app, time.perf_counter() - t0, ph
 
 
 def run_served(L, specs, data, arrivals, slots: int):
@@ -496,10 +497,15 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
     run_plain_loop(L, specs[:1], data[:1], [0.0])
     run_served(L, specs[:1], data[:1], [0.0], slots)
     zeros = [0.0] * n
-    p_res, p_lat, p_svc, p_app, p_span = run_plain_loop(L, specs, data, zeros)
-    s_res, s_lat, s_app, s_span, s_st, _ = run_served(L, specs, data, zeros, slots)
-    err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(s_res, p_res))
+    p_res, p_lat, p_svc, p_app, p_span, p_ph = run_plain_loop(L, specs, data, zeros)
+    s_res, s_lat, s_app, s_span, s_st, s_info = run_served(L, specs, data, zeros, slots)
+    errs = [float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(s_res, p_res)]
+    nonfinite = sum(int(not np.all(np.isfinite(a))) + int(not np.all(np.isfinite(b))) for a, b in zip(s_res, p_res))
+    err = max(errs)
     mu_plain = n / p_span
+
+    def phase_means(rows):
+        return {k: float(np.mean([r[k] for r in rows])) for k in ("setup_s", "build_s", "solve_s", "applies")}
     out = {
         "requests": n, "slots": slots, "budget_bytes": SERVE_BUDGET,
         "mix": {"readme_size": sum(sp["kind"] == "readme" for sp in specs),
@@ -510,6 +516,8 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
                        "peak_active": s_st["peak_active"], "peak_bytes": s_st["peak_in_use"]},
         },
         "max_rel_err_served_vs_plain": err,
+        "nonfinite_results": nonfinite,
+        "mean_phases": {"plain": phase_means(p_ph), "served": phase_means(s_info)},
         "sweep": [],
     }
     rng = np.random.default_rng(seed + 1)
@@ -517,7 +525,7 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
         lam = f * mu_plain
         arr = list(np.cumsum(rng.exponential(1.0 / lam, n)) - 0.0)
         arr = [a - arr[0] for a in arr]
-        _, pl, _, _, pspan = run_plain_loop(L, specs, data, arr)
+        _, pl, _, _, pspan, _ = run_plain_loop(L, specs, data, arr)
         sres, sl, _, sspan, _, _ = run_served(L, specs, data, arr, slots)
         out["sweep"].append({
             "rate_x_plain_capacity": f, "arrivals_per_s": lam,

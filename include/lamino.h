@@ -124,6 +124,13 @@ int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *st
 /* Embedding-grid sizes L[3] = (L1, L2, L3) and device bytes held by the operator. */
 int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes);
 int lamino_normal_destroy(lamino_normal_t op);
+/* Quadratic forms out[3 g + i] = x_i . (S_g x)_i (double, host) for the
+ * operators parts[g] (FP32 or mixed spectra, op's volume size), computed from
+ * one forward half-spectrum of x with op's buffers (Parseval) instead of one
+ * apply per part; the x_i . sysmat_g(x)_i terms of residual()
+ * (src/gradient.cpp:117-127) and of the MBIR3 loss (src/mbir3.cpp:108-116). */
+int lamino_normal_quadforms(lamino_normal_t op, const lamino_normal_t *parts, int nparts, const float *x3,
+                            double *out, void *stream);
 /* Per-stage CUDA-event timing of lamino_normal_apply on the launching stream
  * (measurement hook; no reference counterpart).  enable != 0 records events for
  * up to max_applies subsequent applies. */
@@ -175,7 +182,9 @@ int lamino_lipschitz(lamino_op_t A, int64_t n1, int64_t n2, int64_t n3, int max_
  * tomocam::ReconParams (include/config.h:146-158); lamino_recon_params_default fills them.
  * op_kind: 0 Toeplitz FP32, 1 Toeplitz FP16 spectra, 2 NUFFT form, 3 mixed (FP16
  * correction solves inside `refinements` FP32-residual refinement cycles per
- * linear solve; MBIR1 and MBIR2).
+ * linear solve; MBIR1 and MBIR2).  MBIR3 uses mu as the Lipschitz constant of
+ * its gradient (src/mbir3.cpp:124); mu <= 0 estimates it instead with 30 power
+ * iterations of the normal operator (FP64 norms), as lamino_lipschitz.
  */
 typedef struct {
     int max_iters, inner_iters;

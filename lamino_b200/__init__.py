@@ -67,6 +67,7 @@ def lib():
         "lamino_normal_apply": ([vp, vp, vp, vp], i32),
         "lamino_normal_info": ([vp, P(i64), P(i64)], i32),
         "lamino_normal_destroy": ([vp], i32),
+        "lamino_normal_quadforms": ([vp, P(vp), i32, vp, P(f64), vp], i32),
         "lamino_normal_profile": ([vp, i32, i32], i32),
         "lamino_normal_stage_times": ([vp, P(i32), P(f64), P(i64), P(i32), P(i32)], i32),
         "lamino_qggmrf": ([vp, vp, i64, i64, i64, f32, f32, vp], i32),
@@ -349,6 +350,15 @@ class ToeplitzNormal:
         b = ctypes.c_int64()
         _check(lib().lamino_normal_info(self._h, L, ctypes.byref(b)))
         return tuple(L), b.value
+
+    def quadforms(self, x, parts) -> np.ndarray:
+        """(len(parts), 3) array of x_i . (S_g x)_i for the operators `parts`
+        (same volume size), from one forward half-spectrum of x."""
+        x = _as_f32(x)
+        arr = (ctypes.c_void_p * len(parts))(*[p._h.value for p in parts])
+        out = (ctypes.c_double * (3 * len(parts)))()
+        _check(lib().lamino_normal_quadforms(self._h, arr, len(parts), _ptr(x), out, _stream(x)))
+        return np.array(out[:], dtype=np.float64).reshape(len(parts), 3)
 
 
 def _pad_n(n: int, f) -> int:

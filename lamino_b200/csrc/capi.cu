@@ -351,6 +351,25 @@ int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes) {
     API_END
 }
 
+int lamino_normal_quadforms(lamino_normal_t op, const lamino_normal_t *parts, int nparts, const float *x3,
+                            double *out, void *stream) {
+    API_BEGIN
+    if (!op || !parts || nparts <= 0 || !out) throw Error(ERR_ARG, "null argument");
+    std::vector<const Toeplitz *> ps;
+    for (int i = 0; i < nparts; ++i) {
+        if (!parts[i]) throw Error(ERR_ARG, "null operator");
+        ps.push_back(parts[i]->t.get());
+    }
+    cudaStream_t s = S(stream);
+    In<float> in(x3, (size_t)(3 * op->t->vol.size()), s);
+    DevBuf<double> acc((size_t)(3 * nparts));
+    LAMINO_CUDA(cudaMemsetAsync(acc.p, 0, acc.bytes(), s));
+    op->t->quadforms(in.d, ps, acc.p, s);
+    LAMINO_CUDA(cudaMemcpyAsync(out, acc.p, acc.bytes(), cudaMemcpyDeviceToHost, s));
+    LAMINO_CUDA(cudaStreamSynchronize(s));
+    API_END
+}
+
 int lamino_normal_destroy(lamino_normal_t op) {
     API_BEGIN
     delete op;

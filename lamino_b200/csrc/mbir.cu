@@ -182,9 +182,8 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
             std::vector<const Toeplitz *> parts;
             for (const Geom *g : gptr) {
                 Tg.emplace_back(new Toeplitz({g}, od, PREC_FP32, s));
+                Tg.back()->drop_work();  // kept for its spectra (loss quadratic forms, the sum)
                 parts.push_back(Tg.back().get());
-                Toeplitz *tp = Tg.back().get();
-                Ag.push_back([tp](const float *xx, float *yy, cudaStream_t st) { tp->apply(xx, yy, st); });
             }
             T.reset(new Toeplitz(parts, prec, s));
         } else {
@@ -232,32 +231,44 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
             gGrad(xx, g, st);
             ++extra_applies;
         };
-        // loss: per-gamma quadratic forms into device slots (graphed), then one fetch
-        DevBuf<float> Sx(n);
-        const int ngi = (int)Ag.size();
-        Reducer lr(6 * ngi);
+        // loss (src/mbir3.cpp:108-116): sum over gamma and component of
+        // sqrt(x_i . S_g x_i - 2 x_i . yT_i + yTy).  Toeplitz forms get every
+        // x_i . S_g x_i from one forward half-spectrum of x (Parseval); the NUFFT
+        // form applies each S_g.  Device slots, one graph per input, one fetch.
+        const int ngi = (int)gptr.size();
+        std::vector<const Toeplitz *> parts;
+        for (auto &t : Tg) parts.push_back(t.get());
+        DevBuf<float> Sx(T ? 0 : n);
+        Reducer lr(3 * ngi + 3);
         GraphedOp gLoss(
             [&](const float *xx, float *, cudaStream_t st) {
-                lr.zero(6 * ngi, st);
-                for (int q = 0; q < ngi; ++q) {
-                    Ag[q](xx, Sx.p, st);
-                    for (int i = 0; i < 3; ++i) {
-                        vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + 6 * q + i, st);
-                        vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 6 * q + 3 + i, st);
+                lr.zero(3 * ngi + 3, st);
+                if (T) {
+                    T->quadforms(xx, parts, lr.d, st);
+                } else {
+                    for (int q = 0; q < ngi; ++q) {
+                        Ag[q](xx, Sx.p, st);
+                        for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + 3 * q + i, st);
                     }
                 }
+                for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 3 * ngi + i, st);
             },
             graphs);
         LossFn loss = [&](const float *xx, cudaStream_t st) {
             gLoss(xx, nullptr, st);
-            extra_applies += ngi;
-            lr.fetch(6 * ngi, st);
+            extra_applies += T ? 0 : ngi;
+            lr.fetch(3 * ngi + 3, st);
             double e = 0.0;
             for (int q = 0; q < ngi; ++q)
-                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[6 * q + i] - 2.0 * lr.h[6 * q + 3 + i] + yTy);
+                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[3 * q + i] - 2.0 * lr.h[3 * ngi + i] + yTy);
             return e;
         };
-        nagopt(grad, loss, x.p, od, prm.max_iters, prm.mu, prm.tol, prm.xtol, prm.inner_iters, s);
+        float lip = prm.mu;
+        if (!(lip > 0.f)) {  // estimate: 30 power iterations of sum_gamma sysmat (qGGMRF curvature neglected)
+            lip = (float)lipschitz(A, od, 30, 0.0, 12345ULL, s);
+            if (!(lip > 0.f)) lip = 1.f;
+        }
+        nagopt(grad, loss, x.p, od, prm.max_iters, lip, prm.tol, prm.xtol, prm.inner_iters, s);
     }
     crop3d3(x.p, od, recon, out3, s);
     LAMINO_CUDA(cudaStreamSynchronize(s));

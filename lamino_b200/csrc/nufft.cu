@@ -407,30 +407,6 @@ __device__ __forceinline__ int64_t tile_cell_index(const BinLayout &B, const Bin
     return ((int64_t)g1 * F.nf2 + g2) * F.nf3 + g3;
 }
 
-// spread NC strengths at a point into NC tiles (shared float atomics); taps precomputed
-template <int W, int NC>
-__device__ __forceinline__ void spread_tile(float2 *tile, int tsz, const BinLayout &B, int a1, int a2, int a3,
-                                            const float *w1, const float *w2, const float *w3, const float2 *str) {
-#pragma unroll 1
-    for (int t1 = 0; t1 < W; ++t1) {
-#pragma unroll
-        for (int t2 = 0; t2 < W; ++t2) {
-            float *row = reinterpret_cast<float *>(tile + ((a1 + t1) * B.t2 + a2 + t2) * B.t3 + a3);
-            const float k12 = w1[t1] * w2[t2];
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const float sr = k12 * str[c].x, si = k12 * str[c].y;
-                float *rc = row + 2 * c * tsz;
-#pragma unroll
-                for (int t3 = 0; t3 < W; ++t3) {
-                    atomicAdd(rc + 2 * t3, w3[t3] * sr);
-                    atomicAdd(rc + 2 * t3 + 1, w3[t3] * si);
-                }
-            }
-        }
-    }
-}
-
 template <int W, int NC>
 __device__ __forceinline__ void gather_tile(const float2 *tile, int tsz, const BinLayout &B, int a1, int a2, int a3,
                                             const float *w1, const float *w2, const float *w3, float2 *out) {
@@ -526,6 +502,73 @@ struct RawSink {
     }
 };
 
+// A staged point: its offset in the bin's tile, its separable kernel weights and
+// its NC strengths.
+template <int W, int NC>
+struct PointRec {
+    int a1, a2, a3;
+    float w1[W], w2[W], w3[W];
+    float2 s[NC];
+};
+constexpr int kStageChunk = 256;  // points staged per pass
+constexpr size_t point_rec_bytes(int w, int nc) { return (size_t)((12 + 12 * w + 7) / 8 * 8 + 8 * nc); }
+static_assert(sizeof(PointRec<7, 3>) == point_rec_bytes(7, 3), "record layout");
+static_assert(sizeof(PointRec<8, 1>) == point_rec_bytes(8, 1), "record layout");
+
+// Spread the staged points into the tile without atomics: warp v owns the tile
+// slabs i1 = v, v + nwarps, ... and applies every staged point's taps that fall
+// in its slabs, its lanes covering the point's w x w (t2, t3) taps, so each
+// cell has one writer and the order of the sums is fixed.
+template <int W, int NC>
+__device__ __forceinline__ void spread_staged(float2 *tile, int tsz, const BinLayout &B,
+                                              const PointRec<W, NC> *recs, int n) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    constexpr int NT = W * W;
+    constexpr int NR = (NT + 31) / 32;
+    int t2s[NR], t3s[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int q = lane + 32 * r;
+        t2s[r] = q < NT ? q / W : -1;
+        t3s[r] = q < NT ? q - (q / W) * W : 0;
+    }
+    for (int q = 0; q < n; ++q) {
+        const PointRec<W, NC> &pr = recs[q];
+        const int a1 = pr.a1;
+        for (int slab = warp; slab < B.t1; slab += nwarps) {
+            const int t1 = slab - a1;
+            if ((unsigned)t1 >= (unsigned)W) continue;
+            const float w1v = pr.w1[t1];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                if (t2s[r] < 0) continue;
+                const float wt = w1v * pr.w2[t2s[r]] * pr.w3[t3s[r]];
+                const int cell = (slab * B.t2 + pr.a2 + t2s[r]) * B.t3 + pr.a3 + t3s[r];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    float2 v = tile[c * tsz + cell];
+                    v.x = fmaf(wt, pr.s[c].x, v.x);
+                    v.y = fmaf(wt, pr.s[c].y, v.y);
+                    tile[c * tsz + cell] = v;
+                }
+            }
+        }
+    }
+}
+
+template <int NC>
+__device__ __forceinline__ void flush_tile(const float2 *tile, int tsz, const BinLayout &B, const BinOrigin &o,
+                                           const Fine &F, float2 *H, int64_t NF) {
+    for (int cell = threadIdx.x; cell < tsz; cell += blockDim.x) {
+        const int64_t gi = tile_cell_index(B, o, F, cell);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const float2 v = tile[c * tsz + cell];
+            if (v.x != 0.f || v.y != 0.f) atomicAdd(H + c * NF + gi, v);
+        }
+    }
+}
+
 template <int W, int NC, class Str>
 __global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_t *__restrict__ perm,
                                                        const uint32_t *__restrict__ start, BinLayout B, Fine F,
@@ -536,30 +579,35 @@ __global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_
     if (p0 == p1) return;
     const BinOrigin o = bin_origin(B, bin);
     const int tsz = (int)B.tile_cells();
+    PointRec<W, NC> *recs = reinterpret_cast<PointRec<W, NC> *>(tile + NC * tsz);
     for (int i = threadIdx.x; i < NC * tsz; i += blockDim.x) tile[i] = make_float2(0.f, 0.f);
-    __syncthreads();
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
-        const uint32_t pid = __ldg(perm + i);
-        int p, j, k;
-        decode_pid(pid, g, p, j, k);
-        float2 s[NC];
-        str(g, p, j, k, pid, s);
-        float w1[W], w2[W], w3[W], x, y, z;
-        int a1, a2, a3;
-        if (point_taps<W>(g, F, B, o, p, j, k, w1, w2, w3, a1, a2, a3, x, y, z))
-            spread_tile<W, NC>(tile, tsz, B, a1, a2, a3, w1, w2, w3, s);
-        else
-            spread_point_global<W, NC>(H, NF, F, x, y, z, s);
-    }
-    __syncthreads();
-    for (int cell = threadIdx.x; cell < tsz; cell += blockDim.x) {
-        const int64_t gi = tile_cell_index(B, o, F, cell);
+    for (uint32_t base = p0; base < p1; base += kStageChunk) {
+        const int n = (int)min((uint32_t)kStageChunk, p1 - base);
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const uint32_t pid = __ldg(perm + base + t);
+            int p, j, k;
+            decode_pid(pid, g, p, j, k);
+            PointRec<W, NC> &pr = recs[t];
+            float2 s[NC];
+            str(g, p, j, k, pid, s);
+            float x, y, z;
+            int a1, a2, a3;
+            if (point_taps<W>(g, F, B, o, p, j, k, pr.w1, pr.w2, pr.w3, a1, a2, a3, x, y, z)) {
+                pr.a1 = a1;
+                pr.a2 = a2;
+                pr.a3 = a3;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const float2 v = tile[c * tsz + cell];
-            if (v.x != 0.f || v.y != 0.f) atomicAdd(H + c * NF + gi, v);
+                for (int c = 0; c < NC; ++c) pr.s[c] = s[c];
+            } else {
+                pr.a1 = -(1 << 20);  // matches no slab
+                spread_point_global<W, NC>(H, NF, F, x, y, z, s);
+            }
         }
+        __syncthreads();
+        spread_staged<W, NC>(tile, tsz, B, recs, n);
+        __syncthreads();
     }
+    flush_tile<NC>(tile, tsz, B, o, F, H, NF);
 }
 
 template <int W, int NC, class Sink>
@@ -592,10 +640,11 @@ __global__ void __launch_bounds__(256) k_interp_binned(GeomView g, const uint32_
     }
 }
 
-// sysmat per point, binned: gather 3 components from the input tile, combine
-// with the beam vector, spread back into the output tile (src/gradient.cpp:34-89)
+// sysmat per point, binned: gather 3 components from the input tile (a thread
+// per point), combine with the beam vector, stage, then spread into the output
+// tile as k_spread_binned (src/gradient.cpp:34-89)
 template <int W>
-__global__ void __launch_bounds__(512) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
+__global__ void __launch_bounds__(256) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
                                                        const uint32_t *__restrict__ start, BinLayout B, Fine F,
                                                        const float2 *__restrict__ G, float2 *__restrict__ H,
                                                        int64_t NF, float inv_scale) {
@@ -606,39 +655,48 @@ __global__ void __launch_bounds__(512) k_sysmat_binned(GeomView g, const uint32_
     const BinOrigin o = bin_origin(B, bin);
     const int tsz = (int)B.tile_cells();
     float2 *gt = sm, *ht = sm + 3 * tsz;
+    PointRec<W, 3> *recs = reinterpret_cast<PointRec<W, 3> *>(sm + 6 * tsz);
     for (int i = threadIdx.x; i < 3 * tsz; i += blockDim.x) {
         const int c = i / tsz, cell = i - c * tsz;
         gt[i] = __ldg(G + c * NF + tile_cell_index(B, o, F, cell));
         ht[i] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
-        const uint32_t pid = __ldg(perm + i);
-        int p, j, k;
-        decode_pid(pid, g, p, j, k);
-        float w1[W], w2[W], w3[W], x, y, z;
-        int a1, a2, a3;
-        const bool in = point_taps<W>(g, F, B, o, p, j, k, w1, w2, w3, a1, a2, a3, x, y, z);
-        float2 v[3];
-        if (in) gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, w1, w2, w3, v);
-        else interp_point_global<W, 3>(G, NF, F, x, y, z, v);
-        const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
-        const float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
-        const float si = (c0 * v[0].y + c1 * v[1].y + c2 * v[2].y) * inv_scale;
-        const float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
-                             make_float2(c2 * sr, c2 * si)};
-        if (in) spread_tile<W, 3>(ht, tsz, B, a1, a2, a3, w1, w2, w3, s);
-        else spread_point_global<W, 3>(H, NF, F, x, y, z, s);
-    }
-    __syncthreads();
-    for (int cell = threadIdx.x; cell < tsz; cell += blockDim.x) {
-        const int64_t gi = tile_cell_index(B, o, F, cell);
+    for (uint32_t base = p0; base < p1; base += kStageChunk) {
+        const int n = (int)min((uint32_t)kStageChunk, p1 - base);
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const uint32_t pid = __ldg(perm + base + t);
+            int p, j, k;
+            decode_pid(pid, g, p, j, k);
+            PointRec<W, 3> &pr = recs[t];
+            float x, y, z;
+            int a1, a2, a3;
+            const bool in = point_taps<W>(g, F, B, o, p, j, k, pr.w1, pr.w2, pr.w3, a1, a2, a3, x, y, z);
+            float2 v[3];
+            if (in) gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, pr.w1, pr.w2, pr.w3, v);
+            else interp_point_global<W, 3>(G, NF, F, x, y, z, v);
+            const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p),
+                        c2 = __ldg(g.coeff + 2 * g.nproj + p);
+            const float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
+            const float si = (c0 * v[0].y + c1 * v[1].y + c2 * v[2].y) * inv_scale;
+            const float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
+                                 make_float2(c2 * sr, c2 * si)};
+            if (in) {
+                pr.a1 = a1;
+                pr.a2 = a2;
+                pr.a3 = a3;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float2 v = ht[c * tsz + cell];
-            if (v.x != 0.f || v.y != 0.f) atomicAdd(H + c * NF + gi, v);
+                for (int c = 0; c < 3; ++c) pr.s[c] = s[c];
+            } else {
+                pr.a1 = -(1 << 20);
+                spread_point_global<W, 3>(H, NF, F, x, y, z, s);
+            }
         }
+        __syncthreads();
+        spread_staged<W, 3>(ht, tsz, B, recs, n);
+        __syncthreads();
     }
+    flush_tile<3>(ht, tsz, B, o, F, H, NF);
 }
 
 // direct (unsorted) sysmat per point, for calls that may not allocate a sorted order:
@@ -786,7 +844,8 @@ void NufftPlan::set_bins(int b1, int b2, int b3) {
     B.nb3 = (int)((nf3 + b3 - 1) / b3);
     B.t1 = b1 + w - 1; B.t2 = b2 + w - 1; B.t3 = b3 + w - 1;
     if (B.nbins() > (int64_t)INT32_MAX - 1) throw Error(ERR_ARG, "too many bins");
-    if (6 * B.tile_cells() * (int64_t)sizeof(float2) > 227 * 1024) throw Error(ERR_ARG, "bin tile too large");
+    if (6 * B.tile_cells() * (int64_t)sizeof(float2) + kStageChunk * (int64_t)point_rec_bytes(w, 3) > 227 * 1024)
+        throw Error(ERR_ARG, "bin tile too large for shared memory");
     bins = B;
     drop_sorted();
 }
@@ -867,7 +926,7 @@ void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumu
     LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, gwork.bytes(), s));
     const Fine F = fine_of(*this);
     const GeomView gv = g.view();
-    const int smem = (int)(3 * bins.tile_cells() * sizeof(float2));
+    const int smem = (int)(3 * bins.tile_cells() * sizeof(float2) + kStageChunk * point_rec_bytes(w, 3));
     with_width(w, [&](auto WC) {
         constexpr int W = decltype(WC)::value;
         auto kern = k_spread_binned<W, 3, AdjointStrength>;
@@ -884,7 +943,7 @@ void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumu
 // `may_sort`: build missing point orders (allocates) or fall back to the direct kernel
 void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cudaStream_t s) {
     const Fine F = fine_of(*this);
-    const int smem = (int)(6 * bins.tile_cells() * sizeof(float2));
+    const int smem = (int)(6 * bins.tile_cells() * sizeof(float2) + kStageChunk * point_rec_bytes(w, 3));
     for (int i = 0; i < ng; ++i) {
         const Geom &g = *gs[i];
         if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
@@ -896,7 +955,7 @@ void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cuda
             if (sp) {
                 auto kern = k_sysmat_binned<W>;
                 raise_smem_limit((const void *)kern, smem);
-                kern<<<(unsigned)bins.nbins(), 512, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p, gin.p,
+                kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p, gin.p,
                                                                 nf(), inv_scale);
                 LAMINO_LAUNCH("k_sysmat_binned");
             } else {
@@ -957,7 +1016,7 @@ void NufftPlan::type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_
     LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, nf() * sizeof(float2), s));
     const Fine F = fine_of(*this);
     const GeomView gv = g.view();
-    const int smem = (int)(bins.tile_cells() * sizeof(float2));
+    const int smem = (int)(bins.tile_cells() * sizeof(float2) + kStageChunk * point_rec_bytes(w, 1));
     with_width(w, [&](auto WC) {
         constexpr int W = decltype(WC)::value;
         auto kern = k_spread_binned<W, 1, RawStrength>;

@@ -330,6 +330,77 @@ __global__ void __launch_bounds__(256) k_pencil(float2 *__restrict__ xa, int n1,
     }
 }
 
+// Quadratic forms x_i . (S_g x)_i of up to kMaxQuadSets operators S_g sharing
+// this pencil layout, by Parseval on the half spectrum: after the forward
+// pencil FFT, sum_p1 w(k3) Re(conj(X_i) (K_g X)_i), w = 1 on the k3 = 0 and
+// Nyquist planes and 2 elsewhere (K is real and even, X Hermitian).
+constexpr int kMaxQuadSets = 8;
+struct QuadSets {
+    const float *K[kMaxQuadSets];
+};
+
+template <int N1>
+__global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h,
+                                                     FftLen F1, const float2 *__restrict__ tw1, QuadSets ks, int ng,
+                                                     double *__restrict__ acc) {
+    extern __shared__ float2 sm[];
+    __shared__ float red[8][3 * kMaxQuadSets];
+    const int64_t pen = blockIdx.x;
+    const int L1 = N1 ? N1 : F1.n;
+    const int half = L1 / 2;
+    const int64_t cs = (int64_t)L2 * L3h * n1p;
+    const float2 *pv = xa + pen * n1p;
+    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
+        int c = t / half, i1 = t - c * half;
+        float2 v = i1 < n1 ? pv[c * cs + i1] : make_float2(0.f, 0.f);
+        sm[c * L1 + i1] = v;
+        sm[c * L1 + i1 + half] = c_mul(v, __ldg(tw1 + i1));
+    }
+    __syncthreads();
+    fft_fwd_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
+    float part[kMaxQuadSets][3];
+#pragma unroll
+    for (int g = 0; g < kMaxQuadSets; ++g) part[g][0] = part[g][1] = part[g][2] = 0.f;
+    for (int p1 = threadIdx.x; p1 < L1; p1 += blockDim.x) {
+        const float2 a = sm[p1], b = sm[L1 + p1], c = sm[2 * L1 + p1];
+#pragma unroll
+        for (int g = 0; g < kMaxQuadSets; ++g) {
+            if (g < ng) {
+                const float *Kp = ks.K[g] + pen * 6 * L1 + p1;
+                const float k00 = Kp[0], k11 = Kp[L1], k22 = Kp[2 * L1], k01 = Kp[3 * L1], k02 = Kp[4 * L1],
+                            k12 = Kp[5 * L1];
+                const float2 y0 = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
+                const float2 y1 = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
+                const float2 y2 = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+                part[g][0] += a.x * y0.x + a.y * y0.y;
+                part[g][1] += b.x * y1.x + b.y * y1.y;
+                part[g][2] += c.x * y2.x + c.y * y2.y;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int g = 0; g < kMaxQuadSets; ++g) {
+        if (g < ng) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                float v = part[g][i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) red[warp][g * 3 + i] = v;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 * ng) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += (double)red[w][threadIdx.x];
+        const int k3 = (int)(pen % L3h);
+        const double wk = (k3 == 0 || k3 == L3h - 1) ? 1.0 : 2.0;
+        atomicAdd(acc + threadIdx.x, wk * t);
+    }
+}
+
 // C2: undo along k2 (positions -> natural), first n2 rows kept, back into z1 rows
 template <int N2>
 __global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, int n1p,
@@ -681,6 +752,8 @@ void Toeplitz::finish(cudaStream_t s) {
     attr((const void *)k_pencil<true, 0>, smem_pen);
     attr((const void *)k_pencil<false, 1458>, smem_pen);
     attr((const void *)k_pencil<true, 1458>, smem_pen);
+    attr((const void *)k_pencil_quad<0>, smem_pen);
+    attr((const void *)k_pencil_quad<1458>, smem_pen);
 }
 
 Toeplitz::~Toeplitz() {
@@ -734,6 +807,7 @@ void Toeplitz::stage_bytes(int64_t *b) const {
 }
 
 void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
+    if (!z1.p || !xa.p) throw Error(ERR_STATE, "Toeplitz operator has no work buffers");
     const bool prof = profiling && (size_t)(nprof + 1) * (NSTAGE + 1) <= ev.size();
     cudaEvent_t *E = prof ? &ev[(size_t)nprof * (NSTAGE + 1)] : nullptr;
     const int64_t nrows = 3 * vol.n1 * vol.n2;
@@ -775,6 +849,46 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
         LAMINO_CUDA(cudaEventRecord(E[5], s));
         ++nprof;
     }
+}
+
+void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &parts, double *acc,
+                         cudaStream_t s) {
+    if (!z1.p || !xa.p) throw Error(ERR_STATE, "Toeplitz operator has no work buffers");
+    if (parts.empty()) return;
+    for (const Toeplitz *t : parts) {
+        if (!t || !t->has_fp32()) throw Error(ERR_ARG, "quadratic forms need operators with FP32 spectra");
+        if (t->vol.n1 != vol.n1 || t->vol.n2 != vol.n2 || t->vol.n3 != vol.n3)
+            throw Error(ERR_ARG, "quadratic forms need operators of this volume size");
+    }
+    const int64_t nrows = 3 * vol.n1 * vol.n2;
+    const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
+    const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
+    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
+    const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
+    const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
+    const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
+    const unsigned gpen = (unsigned)(L2 * L3h);
+    if (ct3) k_r2c_rows<729><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    LAMINO_LAUNCH("k_r2c_rows");
+    if (ct2) k_dim2_fwd<144><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    LAMINO_LAUNCH("k_dim2_fwd");
+    for (size_t g0 = 0; g0 < parts.size(); g0 += kMaxQuadSets) {
+        QuadSets qs{};
+        const int ng = (int)std::min<size_t>(kMaxQuadSets, parts.size() - g0);
+        for (int g = 0; g < ng; ++g) qs.K[g] = parts[g0 + g]->K.p;
+        if (ct1)
+            k_pencil_quad<1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
+        else
+            k_pencil_quad<0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
+        LAMINO_LAUNCH("k_pencil_quad");
+    }
+}
+
+void Toeplitz::drop_work() {
+    z1.release();
+    xa.release();
 }
 
 }  // namespace lamino

@@ -58,6 +58,12 @@ struct Toeplitz {
     int64_t Ssize() const { return L1 * L2 * L3h; }
     // low = true applies with the FP16 spectra (PREC_FP16 always does; PREC_MIXED on request)
     void apply(const float *x3, float *y3, cudaStream_t s, bool low = false);
+    // acc[3 g + i] += x_i . (S_g x)_i for the operators S_g of `parts` (FP32
+    // spectra, this volume size): one forward half-spectrum of x with this
+    // operator's buffers, no inverse transform.  acc: device doubles.
+    void quadforms(const float *x3, const std::vector<const Toeplitz *> &parts, double *acc, cudaStream_t s);
+    // free the work buffers of an operator kept only for its spectra
+    void drop_work();
     bool has_fp32() const { return K.p != nullptr; }
     bool has_fp16() const { return Kh.p != nullptr; }
     void set_profiling(bool on, int max_applies);

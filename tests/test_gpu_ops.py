@@ -137,6 +137,25 @@ def test_toeplitz_matches_analytic_oracle(L, O):
     assert rel(T(x), O.toeplitz_apply(x.astype(np.float64), Tk)) < TOL
 
 
+@pytest.mark.parametrize("dims,geoms", CASES)
+def test_toeplitz_quadforms_match_applies(L, O, dims, geoms):
+    """Parseval quadratic forms x_i . S_g x_i equal the dot products with applies
+    of each per-gamma operator, and the summed operator's form is their sum."""
+    rng = np.random.default_rng(31)
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, n).astype(np.float32), nr, nc, np.float32(g))
+           for n, nr, nc, g in geoms]
+    parts = [L.ToeplitzNormal([pg], dims) for pg in pgs]
+    total = L.ToeplitzNormal(pgs, dims)
+    x = rng.standard_normal((3,) + dims).astype(np.float32)
+    q = total.quadforms(x, parts)
+    for gi, T in enumerate(parts):
+        y = T(x)
+        want = [float(np.dot(x[i].ravel().astype(np.float64), y[i].ravel())) for i in range(3)]
+        assert np.allclose(q[gi], want, rtol=1e-5, atol=1e-6 * max(abs(w) for w in want)), (gi, q[gi], want)
+    qs = total.quadforms(x, [total])[0]
+    assert np.allclose(qs, q.sum(axis=0), rtol=1e-5)
+
+
 def test_edge_sizes(L, O):
     """Degenerate shapes: single projection, single row, thin volume."""
     rng = np.random.default_rng(14)
