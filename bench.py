@@ -335,8 +335,17 @@ def run_ours(args):
     dom_ms = stages[dom][0] / max(napplies, 1)
     dom_bytes = stages[dom][1]
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    # whole-apply algorithmic bytes: x and y (3V floats each), 6 real FP32 half-spectra
+    # and 3 forward + 3 product complex spectra written and read, S = 2n1 2n2 (n3+1)
+    n1, n2, n3 = dims
+    S_alg = (2 * n1) * (2 * n2) * (n3 + 1)
+    V = n1 * n2 * n3
+    b_apply = 2 * 3 * V * 4 + 6 * S_alg * (2 if args.precision == "fp16" else 4) + 12 * S_alg * 8
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src, "traffic": read_traffic(dom),
+                "apply_algorithmic_bytes": b_apply,
+                "apply_achieved": b_apply / (ms / args.steps / 1e3) / 1e9,
+                "apply_frac": b_apply / (ms / args.steps / 1e3) / 1e9 / peak,
                 "stages_ms_per_apply": {k: v[0] / max(napplies, 1) for k, v in stages.items()},
                 "stages_algorithmic_bytes": {k: v[1] for k, v in stages.items()}}
 
@@ -525,14 +534,73 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
         lam = f * mu_plain
         arr = list(np.cumsum(rng.exponential(1.0 / lam, n)) - 0.0)
         arr = [a - arr[0] for a in arr]
-        _, pl, _, _, pspan, _ = run_plain_loop(L, specs, data, arr)
-        sres, sl, _, sspan, _, _ = run_served(L, specs, data, arr, slots)
+        _, pl, psvc, _, pspan, _ = run_plain_loop(L, specs, data, arr)
+        sres, sl, _, sspan, _, sinfo = run_served(L, specs, data, arr, slots)
         out["sweep"].append({
-            "rate_x_plain_capacity": f, "arrivals_per_s": lam,
-            "plain": {"p50_s": _pct(pl, 50), "p99_s": _pct(pl, 99), "recon_per_s": n / pspan},
-            "served": {"p50_s": _pct(sl, 50), "p99_s": _pct(sl, 99), "recon_per_s": n / sspan},
+            "rate_x_plain_capacity": f, "arrivals_per_s": lam, "arrival_span_s": float(arr[-1]),
+            "plain": {"p50_s": _pct(pl, 50), "p99_s": _pct(pl, 99), "mean_s": float(np.mean(pl)),
+                      "recon_per_s": n / pspan, "service_mean_s": float(np.mean(psvc))},
+            "served": {"p50_s": _pct(sl, 50), "p99_s": _pct(sl, 99), "mean_s": float(np.mean(sl)),
+                       "recon_per_s": n / sspan, "run_mean_s": float(np.mean([t["run_s"] for t in sinfo]))},
         })
     return out
+
+
+def run_nufft_form(args):
+    """The plain NUFFT form of the operator at a bench scale: forward and adjoint
+    projection of one gamma dataset and the sum-over-gamma sysmat (interp ->
+    weight -> spread per point), CUDA-event timed with inputs in HBM.  The
+    first call of each geometry includes its bin sort (cached afterwards)."""
+    import numpy as np
+    import torch
+    import lamino_b200 as L
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L.lib()
+    dims, nproj, det = SCALES[args.scale]
+    rng = np.random.default_rng(2026)
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, nproj).astype(np.float32), det, det,
+                       np.float32(np.deg2rad(g))) for g in GAMMAS_DEG]
+    plan = L.NufftPlan(dims)
+    if args.bins:
+        plan.set_bins(*[int(b) for b in args.bins.split(",")])
+    x = synthetic_magnetization_gpu(torch, dims)
+    proj = torch.rand((nproj, det, det), device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    t_sort = time.perf_counter()
+    L.adjoint(proj, pgs[0], dims, plan=plan)  # includes the bin sort of pgs[0]
+    torch.cuda.synchronize()
+    t_sort = time.perf_counter() - t_sort
+    k = max(1, args.steps)
+    ms_adj = timed(lambda: L.adjoint(proj, pgs[0], dims, plan=plan), k)
+    ms_fwd = timed(lambda: L.forward(x, pgs[0], plan=plan), k)
+    ms_sys = timed(lambda: L.sysmat(x, pgs, plan=plan), k)
+    M = nproj * det * det
+    w = 7
+    # interp + spread taps: 3 components x M points x w^3 taps x 2 (interp, spread) x 2 FMA (complex x real)
+    fma_sys = 2 * 3 * (len(pgs) * M) * w ** 3 * 2
+    line = {"form": "nufft", "metric": "NUFFT-form operator times", "unit": "ms", "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"padded volume {dims}, {len(pgs)} gammas x {nproj} angles, {det}^2 projections",
+                       "bins": [int(b) for b in (args.bins or "8,8,8").split(",")]},
+            "points_per_gamma": M, "first_adjoint_incl_sort_s": t_sort,
+            "adjoint_ms": ms_adj, "forward_ms": ms_fwd, "sysmat_sum_gamma_ms": ms_sys,
+            "sysmat_applies_per_s": 1e3 / ms_sys,
+            "sysmat_tflops_fp32": 2 * fma_sys / (ms_sys / 1e3) / 1e12}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_serve_form(args):
@@ -560,8 +628,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", choices=sorted(SCALES), default="full",
                     help="smaller cases of the same geometry for profiler captures")
-    ap.add_argument("--form", choices=["apply", "served"], default="apply",
-                    help="apply: the operator metric; served: plain loop vs continuous-batching server")
+    ap.add_argument("--form", choices=["apply", "served", "nufft"], default="apply",
+                    help="apply: the operator metric; served: plain loop vs continuous-batching server; "
+                         "nufft: the NUFFT-form forward / adjoint / sysmat")
+    ap.add_argument("--bins", default="", help="nufft form: fine-grid bin size b1,b2,b3")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--slots", type=int, default=6)
     ap.add_argument("--rates", default="0.5,1.0,1.5", help="arrival rates, x the plain loop's capacity")
@@ -569,6 +639,8 @@ def main():
     args = ap.parse_args()
     if args.form == "served":
         return run_serve_form(args)
+    if args.form == "nufft":
+        return run_nufft_form(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
