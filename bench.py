@@ -267,6 +267,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     op = L.ToeplitzNormal(pgs, dims, args.precision)
     build_s = time.perf_counter() - t0
+    shape = op.autotune()  # launch shapes by timing (untimed setup)
     x = synthetic_magnetization_gpu(torch, dims)
     y = torch.empty_like(x)
     stream = torch.cuda.current_stream()
@@ -362,6 +363,7 @@ def run_ours(args):
         "roofline": roofline,
         "clocks": clocks,
         "operator_build_s": build_s,
+        "launch_shape": {"rows_per_cta": shape[0], "k3_per_cta": shape[1], "tuned_apply_ms": shape[2]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, threads, sample = cpu_sample_seconds(128, DET_PADDED)
@@ -427,8 +429,9 @@ def serve_data(torch, L, spec):
 
 
 def serve_params(L, spec, form: str):
-    kw = dict(op_kind="toeplitz", use_graphs=False) if form == "plain" else \
-        dict(op_kind="toeplitz", use_graphs=True)
+    # plain: eager launches, default launch shapes; served: graphs, tuned shapes
+    kw = dict(op_kind="toeplitz", use_graphs=False, autotune=False) if form == "plain" else \
+        dict(op_kind="toeplitz", use_graphs=True, autotune=True)
     if spec["method"] == 3:  # mu = 0: Lipschitz constant from 30 power iterations
         return L.ReconParams(maxIters=SERVE_ITERS, sigma=1000.0, p=1.2, mu=0.0, **kw)
     return L.ReconParams(maxIters=50, innerIters=3, lam=0.1, mu=10.0, **kw)
@@ -502,9 +505,15 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
     specs = serve_mix(n, seed, big_frac)
     data = [serve_data(torch, L, sp) for sp in specs]
     torch.cuda.synchronize()
-    # warm-up: one request through each form (module load, kernel attributes, pools)
-    run_plain_loop(L, specs[:1], data[:1], [0.0])
-    run_served(L, specs[:1], data[:1], [0.0], slots)
+    # warm-up: one request of each distinct size through each form (module load,
+    # kernel attributes, memory pools, the autotuner's per-size cache)
+    seen, warm = set(), []
+    for i, sp in enumerate(specs):
+        if (sp["method"], tuple(sp["recon"])) not in seen:
+            seen.add((sp["method"], tuple(sp["recon"])))
+            warm.append(i)
+    run_plain_loop(L, [specs[i] for i in warm[:2]], [data[i] for i in warm[:2]], [0.0] * min(2, len(warm)))
+    run_served(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), slots)
     zeros = [0.0] * n
     p_res, p_lat, p_svc, p_app, p_span, p_ph = run_plain_loop(L, specs, data, zeros)
     s_res, s_lat, s_app, s_span, s_st, s_info = run_served(L, specs, data, zeros, slots)
@@ -514,7 +523,8 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
     mu_plain = n / p_span
 
     def phase_means(rows):
-        return {k: float(np.mean([r[k] for r in rows])) for k in ("setup_s", "build_s", "solve_s", "applies")}
+        return {k: float(np.mean([r[k] for r in rows]))
+                for k in ("setup_s", "plan_s", "adjoint_s", "build_s", "tune_s", "solve_s", "applies")}
     out = {
         "requests": n, "slots": slots, "budget_bytes": SERVE_BUDGET,
         "mix": {"readme_size": sum(sp["kind"] == "readme" for sp in specs),
@@ -594,7 +604,7 @@ def run_nufft_form(args):
     line = {"form": "nufft", "metric": "NUFFT-form operator times", "unit": "ms", "higher_is_better": False,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"padded volume {dims}, {len(pgs)} gammas x {nproj} angles, {det}^2 projections",
-                       "bins": [int(b) for b in (args.bins or "8,8,8").split(",")]},
+                       "bins": [int(b) for b in (args.bins or "4,8,16").split(",")]},
             "points_per_gamma": M, "first_adjoint_incl_sort_s": t_sort,
             "adjoint_ms": ms_adj, "forward_ms": ms_fwd, "sysmat_sum_gamma_ms": ms_sys,
             "sysmat_applies_per_s": 1e3 / ms_sys,

@@ -64,10 +64,18 @@ int lamino_plan_create(int64_t n1, int64_t n2, int64_t n3, double eps, lamino_pl
 int lamino_plan_destroy(lamino_plan_t p);
 /* Fine-grid bins of b1 x b2 x b3 cells for the plan's spreading and
  * interpolation (each bin's tile of (b + w - 1)^3 cells per component is staged
- * in shared memory); default 8 x 8 x 8.  Drops the plan's cached point orders.
+ * in shared memory); default 4 x 8 x 16.  Drops the plan's cached point orders.
  * No reference counterpart (FINUFFT's opts.gpu_binsize* play this role in
  * cuFINUFFT). */
 int lamino_plan_set_bins(lamino_plan_t p, int b1, int b2, int b3);
+/* Autotuner: times candidate bin layouts on the given geometries and keeps the
+ * fastest for objective 0 (adjoint of geoms[0] including its bin sort, a setup
+ * pass) or 1 (sum over geoms of sysmat with cached sorts, a solver's operator).
+ * The choice is cached per fine grid, kernel width, objective and point count
+ * for the process.  bins[3] (may be NULL) receives the layout, *best_ms (may be
+ * NULL) its time (0 when taken from the cache). */
+int lamino_plan_autotune(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, int objective, int *bins,
+                         double *best_ms, void *stream);
 /* Type 2, iflag -1: c[j] = sum_k modes[k] e^{-i k.x_j} (include/nufft.h:52-64).
  * modes: complex64 interleaved [n1][n2][n3]; c: complex64 [nproj][nrows][ncols]. */
 int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream);
@@ -124,6 +132,10 @@ int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *st
 /* Embedding-grid sizes L[3] = (L1, L2, L3) and device bytes held by the operator. */
 int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes);
 int lamino_normal_destroy(lamino_normal_t op);
+/* Autotuner: times the valid launch shapes (rows per CTA of the n3 transforms,
+ * k3 values per CTA of the n2 transforms) and keeps the fastest; cached per
+ * embedding size and precision for the process.  Outputs may be NULL. */
+int lamino_normal_autotune(lamino_normal_t op, int *rows, int *kb, double *best_ms, void *stream);
 /* Quadratic forms out[3 g + i] = x_i . (S_g x)_i (double, host) for the
  * operators parts[g] (FP32 or mixed spectra, op's volume size), computed from
  * one forward half-spectrum of x with op's buffers (Parseval) instead of one
@@ -193,6 +205,7 @@ typedef struct {
     double eps;
     int refinements;
     int use_graphs; /* replay each solver iteration's operator work as a CUDA graph (non-default streams) */
+    int autotune;   /* pick launch shapes / bin layouts by timing (cached per size) */
 } lamino_recon_params;
 void lamino_recon_params_default(lamino_recon_params *p);
 /* method 1, 2 or 3.  projs[i]: [proj_dims[3i]][proj_dims[3i+1]][proj_dims[3i+2]];
@@ -202,9 +215,11 @@ int lamino_mbir(int method, int ndatasets, const float *const *projs, const int6
                 const lamino_recon_params *params, float *out3, void *stream);
 
 /* Host wall-clock seconds of the calling thread's last lamino_mbir: setup
- * (normalisation, padding, grids, adjoints), operator build and solve, and the
- * number of normal-operator applications in the solve (any pointer may be NULL). */
-int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies);
+ * (normalisation, padding, grids, adjoints), operator build and solve, the
+ * number of normal-operator applications in the solve, and parts[3] = seconds
+ * in the NUFFT plan creation, the setup adjoints and autotuning (any pointer may
+ * be NULL). */
+int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies, double *parts);
 
 /* Estimated peak device bytes of one lamino_mbir call (used for admission control). */
 int lamino_mbir_footprint(int method, int ndatasets, const int64_t *proj_dims, int64_t r1, int64_t r2, int64_t r3,
@@ -225,9 +240,10 @@ int lamino_server_submit(lamino_server_t srv, int method, int ndatasets, const f
                          int64_t r2, int64_t r3, const lamino_recon_params *params, int64_t *id);
 /* Waits for request `id` (timeout_s < 0: no limit; returns LAMINO_ERR_TIMEOUT on
  * expiry), copies the reconstruction to out3 (host, may be NULL), reports the time
- * queued and running and the total latency in seconds and, in phases[4], the
- * request's lamino_mbir_phases figures (setup, build, solve seconds, applies),
- * then forgets the request.  Every output pointer may be NULL. */
+ * queued and running and the total latency in seconds and, in phases[7], the
+ * request's lamino_mbir_phases figures (setup, build, solve seconds, applies,
+ * plan, adjoints, tuning seconds), then forgets the request.  Every output
+ * pointer may be NULL. */
 int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float *out3, double *queue_s,
                        double *run_s, double *latency_s, double *phases);
 /* stats[10] = submitted, completed, failed, bytes in use, peak bytes in use, budget,

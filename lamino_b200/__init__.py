@@ -56,6 +56,8 @@ def lib():
         "lamino_plan_create": ([i64, i64, i64, f64, P(vp)], i32),
         "lamino_plan_destroy": ([vp], i32),
         "lamino_plan_set_bins": ([vp, i32, i32, i32], i32),
+        "lamino_plan_autotune": ([vp, P(vp), i32, i32, P(i32), P(f64), vp], i32),
+        "lamino_normal_autotune": ([vp, P(i32), P(i32), P(f64), vp], i32),
         "lamino_nufft3d2": ([vp, vp, vp, vp, vp], i32),
         "lamino_nufft3d1": ([vp, vp, vp, vp, vp], i32),
         "lamino_forward": ([vp, vp, vp, vp, vp], i32),
@@ -88,7 +90,7 @@ def lib():
         "lamino_server_create": ([i64, i32, i32, f64, P(vp)], i32),
         "lamino_server_submit": ([vp, i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, P(i64)], i32),
         "lamino_server_wait": ([vp, i64, f64, vp, P(f64), P(f64), P(f64), P(f64)], i32),
-        "lamino_mbir_phases": ([P(f64), P(f64), P(f64), P(i64)], i32),
+        "lamino_mbir_phases": ([P(f64), P(f64), P(f64), P(i64), P(f64)], i32),
         "lamino_server_stats": ([vp, P(i64)], i32),
         "lamino_server_destroy": ([vp], i32),
     }
@@ -208,6 +210,17 @@ class NufftPlan:
         """Fine-grid bin size of the shared-memory spreading / interpolation."""
         _check(lib().lamino_plan_set_bins(self._h, int(b1), int(b2), int(b3)))
         return self
+
+    def autotune(self, grids, objective: str = "normal"):
+        """Time candidate bin layouts on `grids` and keep the fastest for
+        'adjoint' (one setup pass incl. the sort) or 'normal' (repeated sysmat);
+        returns (bins, best_ms)."""
+        arr = (ctypes.c_void_p * len(grids))(*[g._h.value for g in grids])
+        b = (ctypes.c_int * 3)()
+        ms = ctypes.c_double()
+        _check(lib().lamino_plan_autotune(self._h, arr, len(grids), {"adjoint": 0, "normal": 1}[objective], b,
+                                          ctypes.byref(ms), ctypes.c_void_p(0)))
+        return tuple(b), ms.value
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -351,6 +364,13 @@ class ToeplitzNormal:
         _check(lib().lamino_normal_info(self._h, L, ctypes.byref(b)))
         return tuple(L), b.value
 
+    def autotune(self):
+        """Time the launch shapes and keep the fastest; returns (rows, kb, best_ms)."""
+        r, k, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(lib().lamino_normal_autotune(self._h, ctypes.byref(r), ctypes.byref(k), ctypes.byref(ms),
+                                            ctypes.c_void_p(0)))
+        return r.value, k.value, ms.value
+
     def quadforms(self, x, parts) -> np.ndarray:
         """(len(parts), 3) array of x_i . (S_g x)_i for the operators `parts`
         (same volume size), from one forward half-spectrum of x."""
@@ -472,14 +492,15 @@ class _ReconParamsC(ctypes.Structure):
                 ("sigma", ctypes.c_float), ("p", ctypes.c_float), ("lam", ctypes.c_float),
                 ("mu", ctypes.c_float), ("tol", ctypes.c_float), ("xtol", ctypes.c_float),
                 ("pad_factor", ctypes.c_float), ("op_kind", ctypes.c_int), ("eps", ctypes.c_double),
-                ("refinements", ctypes.c_int), ("use_graphs", ctypes.c_int)]
+                ("refinements", ctypes.c_int), ("use_graphs", ctypes.c_int), ("autotune", ctypes.c_int)]
 
 
 class ReconParams:
     """tomocam::ReconParams defaults (include/config.h:146-158) plus the operator
     form: op_kind 'toeplitz' (FP32 spectra), 'toeplitz_fp16', 'nufft' or 'mixed'
     (FP16 correction solves in `refinements` FP32-residual cycles), and
-    use_graphs (replay each solver iteration's operator work as a CUDA graph)."""
+    use_graphs (replay each solver iteration's operator work as a CUDA graph) and
+    autotune (launch shapes / bin layouts picked by timing, cached per size)."""
 
     def __init__(self, **kw):
         c = _ReconParamsC()
@@ -489,6 +510,7 @@ class ReconParams:
         self.tol, self.xtol, self.PAD_FACTOR = c.tol, c.xtol, c.pad_factor
         self.op_kind, self.eps, self.refinements = "toeplitz", c.eps, c.refinements
         self.use_graphs = bool(c.use_graphs)
+        self.autotune = bool(c.autotune)
         for k, v in kw.items():
             setattr(self, k, v)
 
@@ -497,7 +519,7 @@ class ReconParams:
         return _ReconParamsC(int(self.maxIters), int(self.innerIters), float(self.sigma), float(self.p),
                              float(self.lam), float(self.mu), float(self.tol), float(self.xtol),
                              float(self.PAD_FACTOR), kind, float(self.eps), int(self.refinements),
-                             int(bool(self.use_graphs)))
+                             int(bool(self.use_graphs)), int(bool(self.autotune)))
 
 
 def _datasets_c(datasets):
@@ -540,8 +562,10 @@ def mbir_phases() -> dict:
     seconds (host wall clock) and the solve's normal-operator applications."""
     a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     n = ctypes.c_int64()
-    _check(lib().lamino_mbir_phases(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(n)))
-    return {"setup_s": a.value, "build_s": b.value, "solve_s": c.value, "applies": n.value}
+    parts = (ctypes.c_double * 3)()
+    _check(lib().lamino_mbir_phases(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(n), parts))
+    return {"setup_s": a.value, "build_s": b.value, "solve_s": c.value, "applies": n.value,
+            "plan_s": parts[0], "adjoint_s": parts[1], "tune_s": parts[2]}
 
 
 def mbir_footprint(method: int, proj_shapes, recon_dims, params: ReconParams | None = None) -> int:
@@ -597,7 +621,7 @@ class ReconServer:
         shape = (3,) + self._dims[rid]
         out = np.empty(shape, dtype=np.float32)
         q, r, l = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-        ph = (ctypes.c_double * 4)()
+        ph = (ctypes.c_double * 7)()
         rc = lib().lamino_server_wait(self._h, int(rid), -1.0 if timeout is None else float(timeout),
                                       ctypes.c_void_p(out.ctypes.data), ctypes.byref(q), ctypes.byref(r),
                                       ctypes.byref(l), ph)
@@ -605,7 +629,8 @@ class ReconServer:
             self._dims.pop(rid, None)
         _check(rc)
         return out, {"queue_s": q.value, "run_s": r.value, "latency_s": l.value, "setup_s": ph[0],
-                     "build_s": ph[1], "solve_s": ph[2], "applies": int(ph[3])}
+                     "build_s": ph[1], "solve_s": ph[2], "applies": int(ph[3]), "plan_s": ph[4],
+                     "adjoint_s": ph[5], "tune_s": ph[6]}
 
     def stats(self) -> dict:
         st = (ctypes.c_int64 * 10)()

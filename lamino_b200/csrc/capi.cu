@@ -189,6 +189,21 @@ int lamino_plan_set_bins(lamino_plan_t p, int b1, int b2, int b3) {
     API_END
 }
 
+int lamino_plan_autotune(lamino_plan_t p, const lamino_geom_t *geoms, int ngeom, int objective, int *bins,
+                         double *best_ms, void *stream) {
+    API_BEGIN
+    if (!p) throw Error(ERR_ARG, "null plan");
+    auto gs = geoms_of(geoms, ngeom);
+    double ms = p->p->autotune_bins(gs, objective, S(stream));
+    if (bins) {
+        bins[0] = p->p->bins.b1;
+        bins[1] = p->p->bins.b2;
+        bins[2] = p->p->bins.b3;
+    }
+    if (best_ms) *best_ms = ms;
+    API_END
+}
+
 int lamino_nufft3d2(lamino_plan_t p, lamino_geom_t g, const float *modes, float *c, void *stream) {
     API_BEGIN
     if (!p || !g) throw Error(ERR_ARG, "null handle");
@@ -370,6 +385,16 @@ int lamino_normal_quadforms(lamino_normal_t op, const lamino_normal_t *parts, in
     API_END
 }
 
+int lamino_normal_autotune(lamino_normal_t op, int *rows, int *kb, double *best_ms, void *stream) {
+    API_BEGIN
+    if (!op) throw Error(ERR_ARG, "null operator");
+    double ms = op->t->autotune(S(stream));
+    if (rows) *rows = op->t->rows1;
+    if (kb) *kb = op->t->kb2;
+    if (best_ms) *best_ms = ms;
+    API_END
+}
+
 int lamino_normal_destroy(lamino_normal_t op) {
     API_BEGIN
     delete op;
@@ -528,6 +553,7 @@ void lamino_recon_params_default(lamino_recon_params *p) {
     p->eps = d.eps;
     p->refinements = d.refinements;
     p->use_graphs = d.use_graphs;
+    p->autotune = d.autotune;
 }
 
 static ReconParams params_of(const lamino_recon_params *params) {
@@ -545,6 +571,7 @@ static ReconParams params_of(const lamino_recon_params *params) {
     prm.eps = params->eps;
     prm.refinements = params->refinements;
     prm.use_graphs = params->use_graphs;
+    prm.autotune = params->autotune;
     if (prm.max_iters < 0 || prm.inner_iters < 0) throw Error(ERR_ARG, "iteration counts must be >= 0");
     if (prm.op_kind < 0 || prm.op_kind > 3) throw Error(ERR_ARG, "op_kind must be 0..3");
     return prm;
@@ -599,13 +626,18 @@ int lamino_mbir(int method, int nds, const float *const *projs, const int64_t *p
     API_END
 }
 
-int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies) {
+int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_t *applies, double *parts) {
     API_BEGIN
     const MbirPhases &p = last_mbir_phases();
     if (setup_s) *setup_s = p.setup_s;
     if (build_s) *build_s = p.build_s;
     if (solve_s) *solve_s = p.solve_s;
     if (applies) *applies = p.applies;
+    if (parts) {
+        parts[0] = p.plan_s;
+        parts[1] = p.adjoint_s;
+        parts[2] = p.tune_s;
+    }
     API_END
 }
 
@@ -681,6 +713,9 @@ int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float 
         phases[1] = r->phases.build_s;
         phases[2] = r->phases.solve_s;
         phases[3] = (double)r->phases.applies;
+        phases[4] = r->phases.plan_s;
+        phases[5] = r->phases.adjoint_s;
+        phases[6] = r->phases.tune_s;
     }
     srv->s->release(id);
     API_END

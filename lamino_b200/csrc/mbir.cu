@@ -141,6 +141,8 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     const double t0 = now_s();
 
     std::unique_ptr<NufftPlan> plan(new NufftPlan(od, prm.eps));
+    const double t_plan = now_s();
+    double t_adj = 0.0, t_tune = 0.0;
     std::vector<std::unique_ptr<Geom>> geoms;
     DevBuf<float> yT(n);
     LAMINO_CUDA(cudaMemsetAsync(yT.p, 0, yT.bytes(), s));
@@ -154,8 +156,10 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         int64_t nr, nc;
         normalize_pad2d(ds.proj, ds.nproj, ds.nrows, ds.ncols, mx, pfac, y, nr, nc, s);
         geoms.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));
+        const double ta = now_s();
         plan->adjoint(*geoms.back(), y.p, yT.p, true, s);
         LAMINO_CUDA(cudaStreamSynchronize(s));
+        t_adj += now_s() - ta;
     }
     std::vector<const Geom *> gptr;
     for (auto &g : geoms) gptr.push_back(g.get());
@@ -171,6 +175,11 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
     if (prm.op_kind == OP_NUFFT) {
         NufftPlan *pl = plan.get();
+        if (prm.autotune) {
+            const double tt = now_s();
+            pl->autotune_bins(gptr, 1, s);
+            t_tune += now_s() - tt;
+        }
         A_raw = [pl, &gptr](const float *x, float *y, cudaStream_t st) { pl->normal(gptr, x, y, st); };
         if (method == 3)
             for (const Geom *g : gptr)
@@ -190,6 +199,11 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
             T.reset(new Toeplitz(gptr, od, prec, s));
         }
         Toeplitz *tp = T.get();
+        if (prm.autotune) {
+            const double tt = now_s();
+            tp->autotune(s);
+            t_tune += now_s() - tt;
+        }
         A_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, false); };
         if (mixed) A_lo_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, true); };
     }
@@ -277,6 +291,9 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
     ph.build_s = t_build - t_setup;
     ph.solve_s = now_s() - t_build;
     ph.applies = gA.calls() + gA_lo.calls() + extra_applies;
+    ph.plan_s = t_plan - t0;
+    ph.adjoint_s = t_adj;
+    ph.tune_s = t_tune;
 }
 
 }  // namespace lamino

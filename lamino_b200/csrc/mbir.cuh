@@ -26,6 +26,7 @@ struct ReconParams {  // include/config.h:146-158 defaults
     double eps = 1.2e-6;
     int refinements = 3;  // refinement cycles per linear solve with OP_TOEPLITZ_MIXED
     int use_graphs = 1;   // replay each solver iteration's operator work as a CUDA graph
+    int autotune = 1;     // pick launch shapes / bin layouts by timing (cached per size)
 };
 
 struct Dataset {
@@ -54,6 +55,7 @@ int64_t mbir_footprint(int method, const std::vector<std::array<int64_t, 3>> &pr
 struct MbirPhases {
     double setup_s = 0, build_s = 0, solve_s = 0;
     int64_t applies = 0;
+    double plan_s = 0, adjoint_s = 0, tune_s = 0;  // parts: NUFFT plan, setup adjoints, autotuning
 };
 MbirPhases &last_mbir_phases();
 

@@ -13,7 +13,10 @@
 // Deconvolution, the pad into the fine grid and the crop out of it are fused
 // into the kernels on either side of cuFFT, and so are the fftshift2 /
 // ifftshift2 index maps and the per-projection beam-vector weighting.
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -94,7 +97,7 @@ NufftPlan::NufftPlan(Dims3 d, double eps_) : vol(d), eps(eps_) {
     zero_bytes(gin.p, gin.bytes());
     int n[3] = {(int)nf1, (int)nf2, (int)nf3};
     fft3.make(3, n, CUFFT_C2C, 1);
-    set_bins(8, 8, 8);
+    set_bins(4, 8, 16);
 }
 
 // ---------------------------------------------------------------------------
@@ -401,7 +404,7 @@ __device__ __forceinline__ BinOrigin bin_origin(const BinLayout &B, int bin) {
 }
 // fine-grid index of tile cell `cell` (wrapped)
 __device__ __forceinline__ int64_t tile_cell_index(const BinLayout &B, const BinOrigin &o, const Fine &F, int cell) {
-    const int i3 = cell % B.t3, r = cell / B.t3;
+    const int i3 = cell % B.r3, r = cell / B.r3;
     const int i2 = r % B.t2, i1 = r / B.t2;
     const int g1 = (o.o1 + i1) % F.nf1, g2 = (o.o2 + i2) % F.nf2, g3 = (o.o3 + i3) % F.nf3;
     return ((int64_t)g1 * F.nf2 + g2) * F.nf3 + g3;
@@ -416,7 +419,7 @@ __device__ __forceinline__ void gather_tile(const float2 *tile, int tsz, const B
     for (int t1 = 0; t1 < W; ++t1) {
 #pragma unroll
         for (int t2 = 0; t2 < W; ++t2) {
-            const float2 *row = tile + ((a1 + t1) * B.t2 + a2 + t2) * B.t3 + a3;
+            const float2 *row = tile + ((a1 + t1) * B.t2 + a2 + t2) * B.r3 + a3;
             const float k12 = w1[t1] * w2[t2];
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
@@ -532,24 +535,41 @@ __device__ __forceinline__ void spread_staged(float2 *tile, int tsz, const BinLa
         t2s[r] = q < NT ? q / W : -1;
         t3s[r] = q < NT ? q - (q / W) * W : 0;
     }
+    const int slab_stride = B.t2 * B.r3;
     for (int q = 0; q < n; ++q) {
         const PointRec<W, NC> &pr = recs[q];
         const int a1 = pr.a1;
+        // this warp's slabs hit by the point (warp-uniform)
+        bool any = false;
+        for (int slab = warp; slab < B.t1; slab += nwarps) any |= (unsigned)(slab - a1) < (unsigned)W;
+        if (!any) continue;
+        float2 s[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] = pr.s[c];
+        float w23[NR];
+        int off[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const int t2 = t2s[r] < 0 ? 0 : t2s[r];
+            w23[r] = t2s[r] < 0 ? 0.f : pr.w2[t2] * pr.w3[t3s[r]];
+            off[r] = (pr.a2 + t2) * B.r3 + pr.a3 + t3s[r];
+        }
         for (int slab = warp; slab < B.t1; slab += nwarps) {
             const int t1 = slab - a1;
             if ((unsigned)t1 >= (unsigned)W) continue;
             const float w1v = pr.w1[t1];
+            float2 *srow = tile + slab * slab_stride;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
                 if (t2s[r] < 0) continue;
-                const float wt = w1v * pr.w2[t2s[r]] * pr.w3[t3s[r]];
-                const int cell = (slab * B.t2 + pr.a2 + t2s[r]) * B.t3 + pr.a3 + t3s[r];
+                const float wt = w1v * w23[r];
+                float2 *cp = srow + off[r];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    float2 v = tile[c * tsz + cell];
-                    v.x = fmaf(wt, pr.s[c].x, v.x);
-                    v.y = fmaf(wt, pr.s[c].y, v.y);
-                    tile[c * tsz + cell] = v;
+                    float2 v = cp[c * tsz];
+                    v.x = fmaf(wt, s[c].x, v.x);
+                    v.y = fmaf(wt, s[c].y, v.y);
+                    cp[c * tsz] = v;
                 }
             }
         }
@@ -610,6 +630,8 @@ __global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_
     flush_tile<NC>(tile, tsz, B, o, F, H, NF);
 }
 
+// Interpolation: the CTA loads its bin's tile, each thread gathers one point's
+// w^3 taps from shared memory and hands the NC values to the sink.
 template <int W, int NC, class Sink>
 __global__ void __launch_bounds__(256) k_interp_binned(GeomView g, const uint32_t *__restrict__ perm,
                                                        const uint32_t *__restrict__ start, BinLayout B, Fine F,
@@ -843,9 +865,13 @@ void NufftPlan::set_bins(int b1, int b2, int b3) {
     B.nb2 = (int)((nf2 + b2 - 1) / b2);
     B.nb3 = (int)((nf3 + b3 - 1) / b3);
     B.t1 = b1 + w - 1; B.t2 = b2 + w - 1; B.t3 = b3 + w - 1;
+    auto smem_need = [&](const BinLayout &L) {  // the largest kernel: sysmat, two 3-component tiles
+        return 6 * L.tile_cells() * (int64_t)sizeof(float2) + kStageChunk * (int64_t)point_rec_bytes(w, 3);
+    };
+    B.r3 = B.t3 + (((w - B.t3) % 16) + 16) % 16;  // conflict-free rows when they fit
+    if (smem_need(B) > 227 * 1024) B.r3 = B.t3;
     if (B.nbins() > (int64_t)INT32_MAX - 1) throw Error(ERR_ARG, "too many bins");
-    if (6 * B.tile_cells() * (int64_t)sizeof(float2) + kStageChunk * (int64_t)point_rec_bytes(w, 3) > 227 * 1024)
-        throw Error(ERR_ARG, "bin tile too large for shared memory");
+    if (smem_need(B) > 227 * 1024) throw Error(ERR_ARG, "bin tile too large for shared memory");
     bins = B;
     drop_sorted();
 }
@@ -891,6 +917,78 @@ const SortedPoints &NufftPlan::sort_points(const Geom &g, cudaStream_t s) {
     sp->last_use = ++use_clock;
     sorted.push_back(std::move(sp));
     return *sorted.back();
+}
+
+namespace {
+std::mutex g_bins_mu;
+std::map<std::array<int64_t, 6>, std::array<int, 3>> g_bins_cache;
+
+__global__ void k_fill(float *__restrict__ a, int64_t n, float v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+}  // namespace
+
+double NufftPlan::autotune_bins(const std::vector<const Geom *> &gs, int objective, cudaStream_t s) {
+    if (gs.empty()) throw Error(ERR_ARG, "autotune needs at least one geometry");
+    if (objective != 0 && objective != 1) throw Error(ERR_ARG, "objective must be 0 (adjoint) or 1 (normal)");
+    int64_t pts = 0;
+    for (const Geom *g : gs) pts += g->npts();
+    const std::array<int64_t, 6> key{nf1, nf2, nf3, (int64_t)w, (int64_t)objective, pts};
+    {
+        std::lock_guard<std::mutex> lk(g_bins_mu);
+        auto it = g_bins_cache.find(key);
+        if (it != g_bins_cache.end()) {
+            if (it->second[0] != bins.b1 || it->second[1] != bins.b2 || it->second[2] != bins.b3)
+                set_bins(it->second[0], it->second[1], it->second[2]);
+            return 0.0;
+        }
+    }
+    const int64_t nv = 3 * vol.size();
+    DevBuf<float> x((size_t)nv), y((size_t)nv), proj;
+    k_fill<<<grid_for(nv, 256), 256, 0, s>>>(x.p, nv, 1.0f);
+    LAMINO_LAUNCH("k_fill");
+    if (objective == 0) {
+        proj.alloc((size_t)gs[0]->npts());
+        k_fill<<<grid_for(gs[0]->npts(), 256), 256, 0, s>>>(proj.p, gs[0]->npts(), 1.0f);
+        LAMINO_LAUNCH("k_fill");
+    }
+    cudaEvent_t e0, e1;
+    LAMINO_CUDA(cudaEventCreate(&e0));
+    LAMINO_CUDA(cudaEventCreate(&e1));
+    const std::array<int, 3> cands[] = {{4, 8, 16}, {8, 4, 16}, {4, 4, 16}, {2, 8, 16}, {8, 8, 8}, {4, 4, 8}, {16, 4, 8}};
+    double best = 1e300;
+    std::array<int, 3> bb{bins.b1, bins.b2, bins.b3};
+    for (const auto &c : cands) {
+        try {
+            set_bins(c[0], c[1], c[2]);
+        } catch (const Error &) {
+            continue;
+        }
+        float ms = 0.f;
+        if (objective == 0) {
+            LAMINO_CUDA(cudaEventRecord(e0, s));
+            adjoint(*gs[0], proj.p, y.p, false, s);  // sorts, then spreads
+            LAMINO_CUDA(cudaEventRecord(e1, s));
+        } else {
+            normal(gs, x.p, y.p, s);  // sorts
+            LAMINO_CUDA(cudaEventRecord(e0, s));
+            normal(gs, x.p, y.p, s);
+            LAMINO_CUDA(cudaEventRecord(e1, s));
+        }
+        LAMINO_CUDA(cudaEventSynchronize(e1));
+        LAMINO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            bb = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_bins(bb[0], bb[1], bb[2]);
+    std::lock_guard<std::mutex> lk(g_bins_mu);
+    g_bins_cache[key] = bb;
+    return best;
 }
 
 void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_t s) {

@@ -21,13 +21,15 @@ int64_t next_smooth_even(int64_t n);
 // Partition of the fine grid into bins of b1 x b2 x b3 cells.  A point belongs
 // to the bin holding the first cell of its kernel footprint, so its w^3 taps
 // stay inside the bin's tile of (b + w - 1) cells per dimension, which one CTA
-// stages in shared memory.
+// stages in shared memory.  Tile rows are r3 >= t3 cells apart with
+// r3 = w (mod 16): the w x w (t2, t3) taps that consecutive lanes take then fall
+// in distinct shared-memory banks.
 struct BinLayout {
     int b1 = 8, b2 = 8, b3 = 8;
     int nb1 = 0, nb2 = 0, nb3 = 0;
-    int t1 = 0, t2 = 0, t3 = 0;
+    int t1 = 0, t2 = 0, t3 = 0, r3 = 0;
     __host__ __device__ int64_t nbins() const { return (int64_t)nb1 * nb2 * nb3; }
-    __host__ __device__ int64_t tile_cells() const { return (int64_t)t1 * t2 * t3; }
+    __host__ __device__ int64_t tile_cells() const { return (int64_t)t1 * t2 * r3; }
 };
 
 // Point ids of one geometry grouped by bin (counting sort), with bin offsets.
@@ -66,6 +68,12 @@ struct NufftPlan {
     // the geometry's bin-sorted order (built on first use, then cached)
     const SortedPoints &sort_points(const Geom &g, cudaStream_t s);
     const SortedPoints *find_sorted(const Geom &g) const;
+    // time candidate bin layouts and keep the fastest for objective 0 (adjoint of
+    // the first geometry, including its sort: a setup pass) or 1 (the sum over
+    // the geometries of sysmat, sorted orders reused: a solver's operator);
+    // cached per (fine grid, width, objective, points) for the process.  Returns
+    // the best time in ms (0 when taken from the cache).
+    double autotune_bins(const std::vector<const Geom *> &gs, int objective, cudaStream_t s);
     void drop_sorted() { sorted.clear(); }
 
     // --- operators (device pointers; volumes are 3 contiguous components) ---

@@ -17,6 +17,7 @@
 // inverse passes.  Spectra and intermediates stay in digit-reversed position
 // order (fft_engine.cuh), so no pass reorders data.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -884,6 +885,79 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
             k_pencil_quad<0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
         LAMINO_LAUNCH("k_pencil_quad");
     }
+}
+
+void Toeplitz::set_shape(int rows, int kb) {
+    if (rows < 1 || kb < 1) throw Error(ERR_ARG, "launch shape values must be positive");
+    const int64_t smem_rows = (int64_t)rows * L3h * (int64_t)sizeof(float2);
+    const int64_t smem_d2 = (int64_t)D2_IB * kb * d2_stride((int)L2, kb) * (int64_t)sizeof(float2);
+    if (smem_rows > 200 * 1024 || smem_d2 > 200 * 1024) throw Error(ERR_ARG, "launch shape exceeds shared memory");
+    rows1 = rows;
+    kb2 = kb;
+    raise_smem_limit((const void *)k_r2c_rows<0>, (int)smem_rows);
+    raise_smem_limit((const void *)k_r2c_rows<729>, (int)smem_rows);
+    raise_smem_limit((const void *)k_c2r_rows<0>, (int)smem_rows);
+    raise_smem_limit((const void *)k_c2r_rows<729>, (int)smem_rows);
+    raise_smem_limit((const void *)k_dim2_fwd<0>, (int)smem_d2);
+    raise_smem_limit((const void *)k_dim2_fwd<144>, (int)smem_d2);
+    raise_smem_limit((const void *)k_dim2_inv<0>, (int)smem_d2);
+    raise_smem_limit((const void *)k_dim2_inv<144>, (int)smem_d2);
+}
+
+namespace {
+std::mutex g_shape_mu;
+std::map<std::array<int64_t, 4>, std::pair<int, int>> g_shape_cache;
+}  // namespace
+
+double Toeplitz::autotune(cudaStream_t s) {
+    const std::array<int64_t, 4> key{L1, L2, L3, (int64_t)precision};
+    {
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        auto it = g_shape_cache.find(key);
+        if (it != g_shape_cache.end()) {
+            set_shape(it->second.first, it->second.second);
+            return 0.0;
+        }
+    }
+    const int64_t n = 3 * vol.size();
+    DevBuf<float> x((size_t)n), y((size_t)n);
+    LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));  // timing does not depend on the values
+    cudaEvent_t e0, e1;
+    LAMINO_CUDA(cudaEventCreate(&e0));
+    LAMINO_CUDA(cudaEventCreate(&e1));
+    const int r0 = rows1, k0 = kb2;
+    double best = 1e300;
+    int br = r0, bk = k0;
+    const bool was_prof = profiling;
+    profiling = false;
+    for (int rows : {1, 2, 4, 8, 16}) {
+        for (int kb : {1, 2, 4, 8}) {
+            try {
+                set_shape(rows, kb);
+            } catch (const Error &) {
+                continue;
+            }
+            apply(x.p, y.p, s);  // warm-up
+            LAMINO_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) apply(x.p, y.p, s);
+            LAMINO_CUDA(cudaEventRecord(e1, s));
+            LAMINO_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            LAMINO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms / 3.0 < best) {
+                best = ms / 3.0;
+                br = rows;
+                bk = kb;
+            }
+        }
+    }
+    profiling = was_prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_shape(br, bk);
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    g_shape_cache[key] = {br, bk};
+    return best;
 }
 
 void Toeplitz::drop_work() {

@@ -64,6 +64,12 @@ struct Toeplitz {
     void quadforms(const float *x3, const std::vector<const Toeplitz *> &parts, double *acc, cudaStream_t s);
     // free the work buffers of an operator kept only for its spectra
     void drop_work();
+    // launch shape: rows per CTA of the n3 kernels, k3 values per CTA of the n2 kernels
+    void set_shape(int rows, int kb);
+    // time the valid launch shapes on this operator and keep the fastest; the
+    // choice is cached per (L1, L2, L3, precision) for the process.  Returns the
+    // best apply time in ms (0 when taken from the cache).
+    double autotune(cudaStream_t s);
     bool has_fp32() const { return K.p != nullptr; }
     bool has_fp16() const { return Kh.p != nullptr; }
     void set_profiling(bool on, int max_applies);

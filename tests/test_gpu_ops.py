@@ -96,6 +96,32 @@ def test_bin_layouts_vs_oracle(L, O, bins):
                O.nufft3d1(c.astype(np.complex128), opgs[1], plan_o)) < TOL
 
 
+def test_autotuners_keep_results(L, O):
+    """The tuned launch shapes and bin layouts give the oracle's results, and a
+    second tuning of the same size comes from the cache."""
+    dims, geoms = CASES[0]
+    rng = np.random.default_rng(41)
+    pgs, opgs = [], []
+    for np_, nr, nc, g in geoms:
+        th = rng.uniform(0, 2 * np.pi, np_).astype(np.float32)
+        pgs.append(L.PolarGrid(th, nr, nc, np.float32(g)))
+        opgs.append(O.PolarGrid(th, nr, nc, np.float32(g)))
+    plan_o = O.NufftPlan(dims, eps=1e-12)
+    x = rng.standard_normal((3,) + dims).astype(np.float32)
+    want = O.normal(x, opgs, [p.gamma for p in opgs], plan_o)
+    plan = L.NufftPlan(dims)
+    bins, ms = plan.autotune(pgs, "normal")
+    assert len(bins) == 3 and ms > 0
+    assert rel(L.sysmat(x, pgs, plan=plan), want) < TOL
+    bins2, ms2 = L.NufftPlan(dims).autotune(pgs, "normal")
+    assert bins2 == bins and ms2 == 0.0
+    T = L.ToeplitzNormal(pgs, dims)
+    rows, kb, ms = T.autotune()
+    assert rows >= 1 and kb >= 1 and ms > 0
+    assert rel(T(x), want) < TOL
+    assert L.ToeplitzNormal(pgs, dims).autotune()[2] == 0.0
+
+
 def test_bin_layout_rejects_bad_sizes(L):
     plan = L.NufftPlan((8, 6, 8))
     with pytest.raises(L.LaminoError):
