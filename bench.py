@@ -12,7 +12,15 @@ the Toeplitz operator, inputs resident in HBM.  Inputs (443 MB) and spectra
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs N independent replicas (one per rank, launched by torchrun); the
-operator has no cross-GPU exchange.  Rank 0 prints one JSON line.
+operator has no cross-GPU exchange.  Rank 0 prints one JSON line.  At N = 1 the
+line also carries `served`: p50/p99 reconstruction latency and saturated
+reconstructions/s of the continuous-batching server against the plain
+one-at-a-time FP32 loop on a 16-request stream of uneven NAG + qGGMRF
+reconstructions (--no-served skips it).
+
+Other forms (their own JSON line): --form served (the full plain-vs-served
+sweep), --form nufft (NUFFT-form forward / adjoint / sysmat times), --form recon
+(README-size split-Bregman reconstruction end to end, FP32 and mixed).
 """
 from __future__ import annotations
 
@@ -365,6 +373,18 @@ def run_ours(args):
         "operator_build_s": build_s,
         "launch_shape": {"rows_per_cta": shape[0], "k3_per_cta": shape[1], "tuned_apply_ms": shape[2]},
     }
+    if rank == 0 and world == 1 and not args.no_served:
+        # the served form against the plain loop on a short request stream (one GPU)
+        sv = serve_compare(torch, L, 16, [1.0], 2)
+        sw = sv["sweep"][0]
+        line["served"] = {
+            "workload": "16 requests of the mixed-size NAG + qGGMRF stream, Poisson arrivals at the plain "
+                        "loop's capacity, 2 slots, 150 GB budget",
+            "p50_s": sw["served"]["p50_s"], "p99_s": sw["served"]["p99_s"],
+            "plain_p50_s": sw["plain"]["p50_s"], "plain_p99_s": sw["plain"]["p99_s"],
+            "saturated_recon_per_s": sv["saturated"]["served"]["recon_per_s"],
+            "plain_saturated_recon_per_s": sv["saturated"]["plain"]["recon_per_s"],
+            "max_rel_err_vs_plain": sv["max_rel_err_served_vs_plain"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, threads, sample = cpu_sample_seconds(128, DET_PADDED)
         line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "applies/s", "cores": threads, "kind": "port",
@@ -512,7 +532,7 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
         if (sp["method"], tuple(sp["recon"])) not in seen:
             seen.add((sp["method"], tuple(sp["recon"])))
             warm.append(i)
-    run_plain_loop(L, [specs[i] for i in warm[:2]], [data[i] for i in warm[:2]], [0.0] * min(2, len(warm)))
+    run_plain_loop(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm))
     run_served(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), slots)
     zeros = [0.0] * n
     p_res, p_lat, p_svc, p_app, p_span, p_ph = run_plain_loop(L, specs, data, zeros)
@@ -613,6 +633,41 @@ def run_nufft_form(args):
     return 0
 
 
+def run_recon_form(args):
+    """One README-size reconstruction end to end through the C ABI with host
+    buffers (split Bregman, lambda 0.1, mu 10, 50 outer x 3 inner iterations on
+    51x511x511 from 4 gammas x 361 angles of 511^2 projections): the FP32 form
+    and the mixed-precision form (FP16 correction solves inside 3 FP32-residual
+    refinement cycles per linear solve), with their relative difference."""
+    import numpy as np
+    import torch
+    import lamino_b200 as L
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L.lib()
+    spec = dict(kind="readme", method=2, recon=(511, 51, 511), det=(511, 511), nproj=[NPROJ] * 4,
+                gammas=list(GAMMAS_DEG), seed=1234, sigma=5.0)
+    t0 = time.perf_counter()
+    data = serve_data(torch, L, spec)
+    t_data = time.perf_counter() - t0
+    out = {"form": "recon", "metric": "README-size MBIR2 reconstruction seconds", "unit": "s",
+           "higher_is_better": False, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "MBIR2 (split Bregman, 50 x 3), recon 3x51x511x511, 4 gammas x 361 angles, "
+                                  "511^2 projections, host buffers through lamino_mbir"},
+           "data_generation_s": t_data}
+    vols = {}
+    for name, kind in (("fp32", "toeplitz"), ("mixed", "mixed")):
+        p = L.ReconParams(maxIters=50, innerIters=3, lam=0.1, mu=10.0, op_kind=kind)
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        vols[name] = L.MBIR2(data, spec["recon"], p)
+        b = time.perf_counter()
+        out[name] = {"seconds": b - a, **L.mbir_phases()}
+    d = vols["mixed"].astype(np.float64) - vols["fp32"]
+    out["mixed_vs_fp32_rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(vols["fp32"]))
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_serve_form(args):
     import torch
     import lamino_b200 as L
@@ -636,14 +691,15 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-form summary of the apply line")
     ap.add_argument("--scale", choices=sorted(SCALES), default="full",
                     help="smaller cases of the same geometry for profiler captures")
-    ap.add_argument("--form", choices=["apply", "served", "nufft"], default="apply",
+    ap.add_argument("--form", choices=["apply", "served", "nufft", "recon"], default="apply",
                     help="apply: the operator metric; served: plain loop vs continuous-batching server; "
-                         "nufft: the NUFFT-form forward / adjoint / sysmat")
+                         "nufft: the NUFFT-form forward / adjoint / sysmat; recon: README-size MBIR2 end to end")
     ap.add_argument("--bins", default="", help="nufft form: fine-grid bin size b1,b2,b3")
     ap.add_argument("--requests", type=int, default=24)
-    ap.add_argument("--slots", type=int, default=6)
+    ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--rates", default="0.5,1.0,1.5", help="arrival rates, x the plain loop's capacity")
     ap.add_argument("--big-frac", type=float, default=0.0, help="share of README-size requests")
     args = ap.parse_args()
@@ -651,6 +707,8 @@ def main():
         return run_serve_form(args)
     if args.form == "nufft":
         return run_nufft_form(args)
+    if args.form == "recon":
+        return run_recon_form(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
