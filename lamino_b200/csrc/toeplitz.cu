@@ -30,26 +30,50 @@ namespace lamino {
 
 struct TProj {
     double ct, st;
-    double w[6];  // c_i c_j for pairs 00, 11, 22, 01, 02, 12
+    float w[6];  // c_i c_j for pairs 00, 11, 22, 01, 02, 12
 };
 struct TGam {
     double cg, sg, inv_scale;
+    double inv_nrows, inv_ncols;
     int nrows, ncols, p0, np;
 };
 
+// sin(pi x) for |x| <= 1/2: the Taylor series of sin through the x^11 term
+// (truncation error below 6e-8 on the interval), Horner in x^2 in float;
+// max relative error 1.7e-7 against double sin (checked on 2e5 points).
+__device__ __forceinline__ float sinpi_half(float x) {
+    constexpr double P = 3.14159265358979323846;
+    constexpr double P2 = P * P;
+    constexpr float c1 = (float)P;
+    constexpr float c3 = (float)(-P * P2 / 6.0);
+    constexpr float c5 = (float)(P * P2 * P2 / 120.0);
+    constexpr float c7 = (float)(-P * P2 * P2 * P2 / 5040.0);
+    constexpr float c9 = (float)(P * P2 * P2 * P2 * P2 / 362880.0);
+    constexpr float c11 = (float)(-P * P2 * P2 * P2 * P2 * P2 / 39916800.0);
+    const float x2 = x * x;
+    float p = fmaf(c11, x2, c9);
+    p = fmaf(p, x2, c7);
+    p = fmaf(p, x2, c5);
+    p = fmaf(p, x2, c3);
+    p = fmaf(p, x2, c1);
+    return p * x;
+}
+
 // D_n(s) = sin(pi s) / sin(pi s / n), with the 0/0 limit n (-1)^{m (n-1)} at s = m n.
-__device__ __forceinline__ double dirichlet(double s, int n) {
+// inv_n = 1/n in double: s / n only feeds the fractional part f2 (s is an exact
+// multiple of n only at s = 0, where the product is exact too).
+__device__ __forceinline__ float dirichlet(double s, int n, double inv_n) {
     double m1 = rint(s);
     double f1 = s - m1;
-    double q = s / (double)n;
+    double q = s * inv_n;
     double m2 = rint(q);
     double f2 = q - m2;
     long long i1 = (long long)m1, i2 = (long long)m2;
-    if (f2 == 0.0) return ((i2 * (long long)(n - 1)) & 1LL) ? -(double)n : (double)n;
-    float num = sinpif((float)f1);
-    float den = sinpif((float)f2);
-    float r = num / den;
-    return ((i1 + i2) & 1LL) ? -(double)r : (double)r;
+    if (f2 == 0.0) return ((i2 * (long long)(n - 1)) & 1LL) ? -(float)n : (float)n;
+    float num = sinpi_half((float)f1);
+    float den = sinpi_half((float)f2);
+    float r = __fdividef(num, den);
+    return ((i1 + i2) & 1LL) ? -r : r;
 }
 
 // One thread per cell with d_z = m1 in [0, n1); writes T[d] and its mirror T[-d].
@@ -68,17 +92,18 @@ __global__ void __launch_bounds__(256) k_toeplitz_kernel(
         double acc[6] = {0, 0, 0, 0, 0, 0};
         for (int gi = 0; gi < ngam; ++gi) {
             const TGam G = gams[gi];
-            double Da = dirichlet((double)dx * G.cg - (double)dz * G.sg, G.ncols) * G.inv_scale;
+            double Da = (double)dirichlet((double)dx * G.cg - (double)dz * G.sg, G.ncols, G.inv_ncols) * G.inv_scale;
             double u = (double)dx * G.sg + (double)dz * G.cg;
-            double part[6] = {0, 0, 0, 0, 0, 0};
+            // per-dataset sums over the projections in float (|terms| <= nrows), then FP64
+            float part[6] = {0, 0, 0, 0, 0, 0};
             for (int p = 0; p < G.np; ++p) {
                 const TProj P = projs[G.p0 + p];
-                double Db = dirichlet(P.ct * u - (double)dy * P.st, G.nrows);
+                const float Db = dirichlet(P.ct * u - (double)dy * P.st, G.nrows, G.inv_nrows);
 #pragma unroll
-                for (int q = 0; q < 6; ++q) part[q] = fma(P.w[q], Db, part[q]);
+                for (int q = 0; q < 6; ++q) part[q] = fmaf(P.w[q], Db, part[q]);
             }
 #pragma unroll
-            for (int q = 0; q < 6; ++q) acc[q] = fma(Da, part[q], acc[q]);
+            for (int q = 0; q < 6; ++q) acc[q] = fma(Da, (double)part[q], acc[q]);
         }
         int64_t m1 = dz, m2 = dy < 0 ? dy + L2 : dy, m3 = dx < 0 ? dx + L3 : dx;
         int64_t c0 = (m1 * L2 + m2) * L3 + m3;
@@ -644,6 +669,8 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
         G.cg = std::cos(gm);
         G.sg = std::sin(gm);
         G.inv_scale = 1.0 / (double)(g->nrows * g->ncols);
+        G.inv_nrows = 1.0 / (double)g->nrows;
+        G.inv_ncols = 1.0 / (double)g->ncols;
         G.nrows = (int)g->nrows;
         G.ncols = (int)g->ncols;
         G.p0 = (int)hp.size();
@@ -655,8 +682,8 @@ Toeplitz::Toeplitz(const std::vector<const Geom *> &gs, Dims3 d, int prec, cudaS
             TProj P;
             P.ct = std::cos(th);
             P.st = std::sin(th);
-            P.w[0] = c[0] * c[0]; P.w[1] = c[1] * c[1]; P.w[2] = c[2] * c[2];
-            P.w[3] = c[0] * c[1]; P.w[4] = c[0] * c[2]; P.w[5] = c[1] * c[2];
+            P.w[0] = (float)(c[0] * c[0]); P.w[1] = (float)(c[1] * c[1]); P.w[2] = (float)(c[2] * c[2]);
+            P.w[3] = (float)(c[0] * c[1]); P.w[4] = (float)(c[0] * c[2]); P.w[5] = (float)(c[1] * c[2]);
             hp.push_back(P);
         }
     }
