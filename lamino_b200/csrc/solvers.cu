@@ -153,21 +153,27 @@ __constant__ float c_qggmrf_w[27] = {0.0302f, 0.037f, 0.0302f, 0.037f, 0.0523f, 
                                      0.0302f, 0.037f, 0.0302f, 0.037f, 0.0523f, 0.037f, 0.0302f, 0.037f, 0.0302f};
 
 // rho'(delta) with q = 2, C = 0.001, evaluated with the reference's float/double mix
-__device__ __forceinline__ float d_potential(float delta, float sigma_q, float sigma_qp, float p) {
-    const double Q = 2.0, Cd = 0.001;
-    const float C = (float)Cd;
-    float ad = fabsf(delta);
-    float t1 = (float)(pow((double)ad, Q - (double)p) / (double)sigma_qp);
-    float t3 = C + t1;
-    if (ad > 0.f) {
-        float a = delta / (t3 * sigma_q);
-        return (float)((double)a * (Q - ((Q - (double)p) * (double)t1) / (double)t3));
-    }
-    return (float)(Q / ((double)sigma_q * Cd));
+// Derivative of the qGGMRF potential (src/qggmrf.cpp:42-57), q = 2, C = 0.001,
+// in float (powf for |delta|^(q-p)); the reference evaluates parts of it in
+// double, which moves the result by ~1e-7 relative.
+struct QgConst {
+    float qmp;         // q - p
+    float inv_sqp;     // 1 / sigma^(q-p)
+    float inv_sq;      // 1 / sigma^q
+    float at_zero;     // q / (sigma^q C)
+};
+__device__ __forceinline__ float d_potential(float delta, const QgConst &k) {
+    const float C = 0.001f;
+    const float ad = fabsf(delta);
+    if (!(ad > 0.f)) return k.at_zero;
+    const float t1 = powf(ad, k.qmp) * k.inv_sqp;
+    const float t3 = C + t1;
+    const float r = 1.0f / t3;
+    const float a = delta * r * k.inv_sq;
+    return a * (2.0f - k.qmp * t1 * r);
 }
 
-__global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2, int n3, float sigma_q,
-                         float sigma_qp, float p) {
+__global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2, int n3, QgConst kq) {
     const int64_t ni = (int64_t)(n1 - 2) * (n2 - 2) * (n3 - 2);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ni; t += (int64_t)gridDim.x * blockDim.x) {
         int k = (int)(t % (n3 - 2)) + 1;
@@ -186,7 +192,7 @@ __global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int
                     if (dx == 0 && dy == 0 && dz == 0) continue;
                     float v = x[c + ((int64_t)dx * n2 + dy) * n3 + dz];
                     float w = c_qggmrf_w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
-                    sum += w * d_potential(v - u, sigma_q, sigma_qp, p);
+                    sum += w * d_potential(v - u, kq);
                 }
         g[c] += sum;
     }
@@ -197,7 +203,12 @@ void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStr
     float sigma_q = std::pow(sigma, 2.0f);
     float sigma_qp = std::pow(sigma, 2.0f - p);
     int64_t ni = (d.n1 - 2) * (d.n2 - 2) * (d.n3 - 2);
-    k_qggmrf<<<grid_for(ni, 256), 256, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, sigma_q, sigma_qp, p);
+    QgConst kq;
+    kq.qmp = 2.0f - p;
+    kq.inv_sqp = (float)(1.0 / (double)sigma_qp);
+    kq.inv_sq = (float)(1.0 / (double)sigma_q);
+    kq.at_zero = (float)(2.0 / ((double)sigma_q * 0.001));
+    k_qggmrf<<<grid_for(ni, 256), 256, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, kq);
     LAMINO_LAUNCH("k_qggmrf");
 }
 
