@@ -156,7 +156,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "applies/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config("n/a", args.gpus),
+        "config": workload_config(args.precision, args.gpus),
         "cpu_baseline": {"value": v, "unit": "applies/s", "cores": threads, "kind": "port",
                          "sample": sample + "; reference CPU path = this project's oracle port "
                                             "(FINUFFT/FFTW absent, reference NUFFT path unbuildable)"},
@@ -251,6 +251,18 @@ def read_traffic(stage: str):
     return None
 
 
+def max_over_ranks(ms: float, dist=None) -> float:
+    """The slowest rank's time (every rank takes part; NCCL reduces a CUDA
+    tensor, gloo a host one)."""
+    if dist is None:
+        return ms
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -304,10 +316,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     stages, napplies, kpa = op.stage_times()
     op.profile(False)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
+    ms = max_over_ranks(ms, dist)
     value = world * args.steps / (ms / 1e3)
 
     # e2e: the same apply through the C ABI with pinned host buffers (H2D + apply + D2H)
@@ -326,10 +335,7 @@ def run_ours(args):
     f1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = t.item()
+    ms_e2e = max_over_ranks(ms_e2e, dist)
     nbytes = x.numel() * 4
 
     # roofline of the dominant stage
