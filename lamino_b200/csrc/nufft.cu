@@ -5,11 +5,13 @@
 // upsampfac 2, tol 1.2e-6 in float), src/projection.cpp:42-126 (forward /
 // adjoint) and src/gradient.cpp:34-89 (sysmat).
 //
-// Design: points are never stored or sorted.  Each thread regenerates its
-// point from the per-column / per-row / per-projection factors (geometry.cuh)
-// and consecutive threads walk a projection row, so a warp touches a compact
-// patch of the fine grid.  The fine grid is (nf1, nf2, nf3) complex64 with nf
-// the smallest even 2,3,5-smooth size >= 2n; the uniform FFTs on it use cuFFT.
+// Design: point coordinates are never stored; each kernel regenerates a point
+// from the per-column / per-row / per-projection factors (geometry.cuh).  Point
+// ids are bin-sorted once per geometry and plan (a counting sort keyed by the
+// fine-grid bin of the first cell of the point's kernel footprint, cached), and
+// spreading / interpolation run one CTA per bin with the bin's tile of the fine
+// grid in shared memory.  The fine grid is (nf1, nf2, nf3) complex64 with nf the
+// smallest even 2,3,5-smooth size >= 2n; the uniform FFTs on it use cuFFT.
 // Deconvolution, the pad into the fine grid and the crop out of it are fused
 // into the kernels on either side of cuFFT, and so are the fftshift2 /
 // ifftshift2 index maps and the per-projection beam-vector weighting.
@@ -710,7 +712,7 @@ __global__ void __launch_bounds__(256) k_sysmat_binned(GeomView g, const uint32_
 #pragma unroll
                 for (int c = 0; c < 3; ++c) pr.s[c] = s[c];
             } else {
-                pr.a1 = -(1 << 20);
+                pr.a1 = -(1 << 20);  // matches no slab
                 spread_point_global<W, 3>(H, NF, F, x, y, z, s);
             }
         }
@@ -787,16 +789,6 @@ static Fine fine_of(const NufftPlan &pl) {
     F.beta = pl.beta;
     return F;
 }
-
-#define LAMINO_W_DISPATCH(w, KERNEL, GRID, BLOCK, STREAM, ...)                          \
-    switch (w) {                                                                         \
-        case 4: KERNEL<4><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
-        case 5: KERNEL<5><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
-        case 6: KERNEL<6><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
-        case 7: KERNEL<7><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
-        case 8: KERNEL<8><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;              \
-        default: throw Error(ERR_ARG, "unsupported kernel width");                       \
-    }
 
 void NufftPlan::pad_real(const float *x3, int ncomp, cudaStream_t s) {
     Fine F = fine_of(*this);

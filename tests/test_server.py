@@ -195,3 +195,23 @@ def test_server_results_independent_of_batch(L, O):
     assert st["completed"] == len(reqs) and st["failed"] == 0 and st["peak_active"] >= 2
     for k, (g, w) in enumerate(zip(got, direct)):
         assert rel(g, w) < 1e-5, k
+
+
+@pytest.mark.gpu
+def test_server_reports_failed_requests(L, O):
+    """A request that fails inside its worker (an invalid NUFFT tolerance) comes
+    back as an error from wait(), is counted as failed, and does not disturb the
+    requests around it."""
+    good = _problem(O, (8, 5, 9), (6,), (9, 11), (0.0,), 3)
+    with L.ReconServer(budget_bytes=4 << 30, slots=2) as srv:
+        a = srv.submit(1, good, (8, 5, 9), L.ReconParams(maxIters=3))
+        b = srv.submit(1, good, (8, 5, 9), L.ReconParams(maxIters=3, op_kind="nufft", eps=1e-12))
+        c = srv.submit(1, good, (8, 5, 9), L.ReconParams(maxIters=3))
+        va, _ = srv.wait(a, timeout=120)
+        with pytest.raises(L.LaminoError) as e:
+            srv.wait(b, timeout=120)
+        assert e.value.code == 1 and "tolerance" in str(e.value)
+        vc, _ = srv.wait(c, timeout=120)
+        st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 2 and st["in_use"] == 0
+    assert rel(vc, va) < 1e-6
