@@ -14,6 +14,7 @@
  *   grad_u / divergence / laplacian src/finitediff.cpp:8-71, include/bregman.h:34-36
  *   qggmrf                         src/qggmrf.cpp:60-95
  *   nagopt (vector form)           src/nagopt.cpp:116-209
+ *   mask_infs_nans / mask_support  include/mask.h:29-91
  * Nothing here is part of the product.
  */
 #include <array>
@@ -28,6 +29,7 @@
 #include "bregman.h"
 #include "fftutils.h"
 #include "logger.h"
+#include "mask.h"
 #include "optimize.h"
 #include "padding.h"
 #include "polar_grid.h"
@@ -185,4 +187,13 @@ void ref_nagopt_f(ref_grad_cb gcb, ref_loss_cb lcb, void *ctx, float *x3, int64_
     for (int i = 0; i < 3; ++i) to_ptr(r[i], x3 + i * V);
 }
 
+
+void ref_mask_infs_nans_f(const float *in, int64_t n1, int64_t n2, int64_t n3, float *out) {
+    to_ptr(tomocam::mask_infs_nans(from_ptr(in, n1, n2, n3)), out);
+}
+void ref_mask_support_f(const float *in, int64_t n1, int64_t n2, int64_t n3, int64_t d1, int64_t d2, int64_t d3,
+                        const float *theta, float gamma, float *out) {
+    std::vector<float> th(theta, theta + n1);
+    to_ptr(tomocam::mask_support(from_ptr(in, n1, n2, n3), dims_t(d1, d2, d3), th, gamma), out);
+}
 }  // extern "C"
