@@ -166,6 +166,11 @@ int lamino_grad_u(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out
 int lamino_divergence(const float *du3, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream);
 /* tomocam::opt::laplacian (include/bregman.h:34-36): divergence(grad_u(u)). */
 int lamino_laplacian(const float *u, int64_t n1, int64_t n2, int64_t n3, float *out, void *stream);
+/* tomocam::opt::demag (include/demag.h:13-79): the demagnetizing field
+ * h3 = F^-1[-k (k . F m) / |k|^2] / N of m3, both [3][n1][n2][n3]; k = 0 gives 0.
+ * The reference defines it for the CG solver's constraint hook
+ * (src/conjgrad.cpp:46-52), where its use is switched off; so is it here. */
+int lamino_demag(const float *m3, int64_t n1, int64_t n2, int64_t n3, float *h3, void *stream);
 /* tomocam::opt::RampPreconditioner::apply (include/precond.h:72-86), all 3 components. */
 int lamino_ramp_precond(const float *r3, int64_t n1, int64_t n2, int64_t n3, float *z3, void *stream);
 

@@ -76,6 +76,7 @@ def lib():
         "lamino_grad_u": ([vp, i64, i64, i64, vp, vp], i32),
         "lamino_divergence": ([vp, i64, i64, i64, vp, vp], i32),
         "lamino_laplacian": ([vp, i64, i64, i64, vp, vp], i32),
+        "lamino_demag": ([vp, i64, i64, i64, vp, vp], i32),
         "lamino_ramp_precond": ([vp, i64, i64, i64, vp, vp], i32),
         "lamino_op_from_normal": ([vp, P(vp)], i32),
         "lamino_op_from_plan": ([vp, P(vp), i32, P(vp)], i32),
@@ -442,6 +443,17 @@ class opt:  # namespace mirroring tomocam::opt
         u = _as_f32(u)
         out = _empty_like_kind(u, tuple(u.shape))
         _check(lib().lamino_laplacian(_ptr(u), *u.shape, _ptr(out), _stream(u)))
+        return out
+
+    @staticmethod
+    def demag(m3):
+        """tomocam::opt::demag (include/demag.h:13-79): the demagnetizing field of
+        m3 (3, n1, n2, n3)."""
+        m3 = _as_f32(m3)
+        if m3.ndim != 4 or m3.shape[0] != 3:
+            raise ValueError("expected a (3, n1, n2, n3) magnetization")
+        out = _empty_like_kind(m3, tuple(m3.shape))
+        _check(lib().lamino_demag(_ptr(m3), *m3.shape[1:], _ptr(out), _stream(m3)))
         return out
 
     @staticmethod

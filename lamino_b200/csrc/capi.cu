@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/lamino.h"
+#include "demag.cuh"
 #include "server.cuh"
 
 using namespace lamino;
@@ -428,6 +429,16 @@ int lamino_divergence(const float *du3, int64_t n1, int64_t n2, int64_t n3, floa
     In<float> di(du3, 3 * d.size(), S(stream));
     Out<float> o(out, d.size(), S(stream));
     divergence(di.d, d, o.d, S(stream));
+    o.finish(S(stream));
+    API_END
+}
+
+int lamino_demag(const float *m3, int64_t n1, int64_t n2, int64_t n3, float *h3, void *stream) {
+    API_BEGIN
+    Dims3 d = dims_of(n1, n2, n3);
+    In<float> mi(m3, (size_t)(3 * d.size()), S(stream));
+    Out<float> o(h3, (size_t)(3 * d.size()), S(stream));
+    demag(mi.d, d, o.d, S(stream));
     o.finish(S(stream));
     API_END
 }

@@ -583,6 +583,30 @@ def laplacian(u):
     return divergence(grad_u(u))
 
 
+def _fftfreq_ref(n: int) -> np.ndarray:
+    """include/fftutils.h:36-51: 0..ceil(n/2)-1, then negatives, times 2 pi / n."""
+    half = n // 2 if n % 2 == 0 else n // 2 + 1
+    return np.array([i if i < half else i - n for i in range(n)], np.float64) * (2 * np.pi / n)
+
+
+def demag(m3):
+    """include/demag.h:13-79 in FP64: H = irfftn(-k (k . rfftn(m)) / |k|^2), the k = 0
+    term set to 0 (the reference's frequency grids: fftfreq along n1, n2, rfftfreq
+    along n3, each times 2 pi / n)."""
+    m = np.asarray(m3, dtype=np.float64)
+    n1, n2, n3 = m.shape[1:]
+    kx, ky = _fftfreq_ref(n1), _fftfreq_ref(n2)
+    kz = np.arange(n3 // 2 + 1, dtype=np.float64) * (2 * np.pi / n3)
+    K = np.meshgrid(kx, ky, kz, indexing="ij")
+    M = np.fft.rfftn(m, axes=(1, 2, 3))
+    kk = K[0] ** 2 + K[1] ** 2 + K[2] ** 2
+    kk[0, 0, 0] = 1.0
+    kdm = K[0] * M[0] + K[1] * M[1] + K[2] * M[2]
+    H = np.stack([-kdm * K[c] / kk for c in range(3)])
+    H[:, 0, 0, 0] = 0
+    return np.fft.irfftn(H, s=(n1, n2, n3), axes=(1, 2, 3))
+
+
 def split_bregman(A: Callable, yT, x0, lam, mu, outer_max, inner_max, tol, xtol, log=None,
                   A_lo: Callable | None = None, refinements: int = 0):
     """src/bregman.cpp:39-134 (isotropic TV, inner PCG on A + mu*laplacian).  With
