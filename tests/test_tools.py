@@ -305,10 +305,19 @@ def _run(args, cwd):
                           timeout=600)
 
 
+_REGULARIZERS = {
+    1: "",
+    2: '[recon_params.regularizer]\nmethod = "split_bregman"\n'
+       '[recon_params.regularizer.split_bregman]\ninner_iters = 2\n',
+    3: '[recon_params.regularizer]\nmethod = "qGGMRF"\n[recon_params.regularizer.qGGMRF]\nsigma = 1000.0\n',
+}
+
+
 @pytest.mark.gpu
-def test_recon_tool_end_to_end(L, O, tmp_path):
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_recon_tool_end_to_end(L, O, tmp_path, method):
     """TIFF stacks + angle files + TOML -> `python -m lamino_b200.recon` -> TIFF and
-    VTI outputs equal to the direct MBIR2 call in the reference's axis order."""
+    VTI outputs equal to the direct MBIR1/2/3 call in the reference's axis order."""
     T, H, W = 5, 9, 11
     internal = (W, T, H)
     rng = np.random.default_rng(5)
@@ -329,11 +338,7 @@ filename = "{tmp_path}/out/rec.tiff"
 [recon_params]
 recon_dims = [{T}, {H}, {W}]
 max_iters = 4
-[recon_params.regularizer]
-method = "split_bregman"
-[recon_params.regularizer.split_bregman]
-inner_iters = 2
-""")
+""" + _REGULARIZERS[method])
     r = _run(["lamino_b200.recon", str(tmp_path / "c.toml")], tmp_path)
     assert r.returncode == 0, r.stderr
     got = np.stack([tiffio.read(str(tmp_path / "out" / f"rec{i}.tiff"), odd=False) for i in range(3)])
@@ -341,7 +346,8 @@ inner_iters = 2
     vt, _ = vti.read_vectors(str(tmp_path / "out" / "rec.vti"))
     assert np.array_equal(np.stack(vt).astype(np.float32), got)
     ds = cfg.parse_input_datasets(cfg.read_toml_file(str(tmp_path / "c.toml")))
-    want = L.MBIR2(ds, internal, L.ReconParams(maxIters=4, innerIters=2))
+    fn = {1: L.MBIR1, 2: L.MBIR2, 3: L.MBIR3}[method]
+    want = fn(ds, internal, L.ReconParams(maxIters=4, innerIters=2 if method == 2 else 3))
     want = np.stack([np.transpose(want[i], (1, 2, 0)) for i in range(3)])
     assert rel(got, want) < 1e-5
 
