@@ -254,6 +254,9 @@ int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float 
 /* stats[10] = submitted, completed, failed, bytes in use, peak bytes in use, budget,
  * active, peak active, queued, slots. */
 int lamino_server_stats(lamino_server_t srv, int64_t *stats);
+/* Shuts the server down: requests still queued fail (their waiters return
+ * LAMINO_ERR_STATE), running ones finish, and the call returns once every other
+ * call on this server has returned.  No call may start on it after this one. */
 int lamino_server_destroy(lamino_server_t srv);
 
 #ifdef __cplusplus

@@ -699,6 +699,7 @@ int lamino_server_submit(lamino_server_t srv, int method, int nds, const float *
         r->gammas.push_back(gammas[i]);
     }
     r->footprint = mbir_footprint(method, r->pdims, r->recon, r->prm);
+    Server::Use use(*srv->s);
     *id = srv->s->submit(std::move(r));
     API_END
 }
@@ -707,6 +708,7 @@ int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float 
                        double *run_s, double *latency_s, double *phases) {
     API_BEGIN
     if (!srv) throw Error(ERR_ARG, "null server");
+    Server::Use use(*srv->s);
     ServeRequest *r = nullptr;
     if (!srv->s->wait(id, timeout_s, &r)) throw Error(ERR_TIMEOUT, "request not finished within the timeout");
     if (r->status != OK) {
@@ -735,6 +737,7 @@ int lamino_server_wait(lamino_server_t srv, int64_t id, double timeout_s, float 
 int lamino_server_stats(lamino_server_t srv, int64_t *st) {
     API_BEGIN
     if (!srv || !st) throw Error(ERR_ARG, "null argument");
+    Server::Use use(*srv->s);
     ServerStats x = srv->s->stats();
     int64_t v[10] = {x.submitted, x.completed, x.failed, x.in_use, x.peak_in_use,
                      x.budget, x.active, x.peak_active, x.queued, x.slots};

@@ -34,9 +34,33 @@ Server::~Server() {
     {
         std::lock_guard<std::mutex> lk(mu_);
         stop_ = true;
+        for (int64_t id : queue_) {  // never started: fail them so their waiters return
+            ServeRequest *r = reqs_[id].get();
+            r->status = ERR_STATE;
+            r->err = "server shut down before the request started";
+            r->t_start = r->t_done = now();
+            r->done = true;
+            ++failed_;
+        }
+        queue_.clear();
     }
     cv_.notify_all();
-    for (auto &t : workers_) t.join();
+    for (auto &t : workers_) t.join();  // running requests finish first
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return users_ == 0; });
+}
+
+Server::Use::Use(Server &sv) : s(sv) {
+    std::lock_guard<std::mutex> lk(s.mu_);
+    if (s.stop_) throw Error(ERR_STATE, "server is shutting down");
+    ++s.users_;
+}
+
+Server::Use::~Use() {
+    // notify under the lock: once it is released the destructor may free `s`
+    std::lock_guard<std::mutex> lk(s.mu_);
+    --s.users_;
+    s.cv_.notify_all();
 }
 
 int64_t Server::submit(std::unique_ptr<ServeRequest> r) {

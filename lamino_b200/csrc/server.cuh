@@ -59,6 +59,17 @@ class Server {
 
     // r->t_submit, when already set, is kept (the caller's arrival time)
     int64_t submit(std::unique_ptr<ServeRequest> r);
+    // Marks an API call in progress on this server: the destructor waits for it to
+    // end (a thread blocked in wait() for a request that the shutdown drops wakes
+    // with that request failed), so destroying the server never frees state that a
+    // concurrent call still reads.  Throws ERR_STATE once shutdown has begun.
+    struct Use {
+        Server &s;
+        explicit Use(Server &sv);
+        ~Use();
+        Use(const Use &) = delete;
+        Use &operator=(const Use &) = delete;
+    };
     // blocks until the request finished (or timeout_s elapsed: returns false)
     bool wait(int64_t id, double timeout_s, ServeRequest **out);
     void release(int64_t id);  // forget a finished request
@@ -80,6 +91,7 @@ class Server {
     int64_t next_id_ = 1, in_use_ = 0, peak_ = 0, submitted_ = 0, completed_ = 0, failed_ = 0;
     int active_ = 0, peak_active_ = 0;
     bool stop_ = false;
+    int users_ = 0;
     std::vector<std::thread> workers_;
 };
 

@@ -112,6 +112,33 @@ def test_dry_run_rejects_oversize_and_times_out(LB):
             srv.wait(rid)  # forgotten once collected
 
 
+def test_dry_run_shutdown_fails_queued_requests(LB):
+    """Closing the server while a request is queued and another thread waits for it:
+    the waiter gets LAMINO_ERR_STATE, the running request completes, close returns."""
+    import threading
+    p = LB.ReconParams()
+    recon = (8, 8, 8)
+    srv = LB.ReconServer(budget_bytes=1 << 40, slots=1, dry_run_ms=300)
+    a = srv.submit(1, _req(seed=1), recon, p)
+    b = srv.submit(1, _req(seed=2), recon, p)
+    got = {}
+
+    def waiter(rid, key):
+        try:
+            got[key] = srv.wait(rid)[1]["run_s"]
+        except LB.LaminoError as e:
+            got[key] = e.code
+
+    ts = [threading.Thread(target=waiter, args=(a, "a")), threading.Thread(target=waiter, args=(b, "b"))]
+    for t in ts:
+        t.start()
+    time.sleep(0.05)
+    srv.close()
+    for t in ts:
+        t.join(10)
+    assert got["b"] == 7 and got["a"] >= 0.25
+
+
 def test_server_bad_arguments(LB):
     with pytest.raises(LB.LaminoError):
         LB.ReconServer(budget_bytes=0, slots=1, dry_run_ms=1)
