@@ -281,12 +281,19 @@ __device__ __forceinline__ void fft_stage_fixed(float2 *__restrict__ data, int P
     constexpr int m = B / R;
     constexpr int nb = N / R;
     constexpr int ts = N / B;
+    // Thread order over the (block b, offset n1) butterflies: n1 fastest reads
+    // consecutive addresses, but with fewer than 16 offsets per block a half-warp
+    // spans blocks B apart and collides in the shared-memory banks; with b fastest
+    // the lanes are B apart, all distinct banks when B is odd (and they share
+    // their twiddles).
+    constexpr bool b_fast = (m > 1) && (m < 16) && (B % 2 == 1);
+    constexpr int nblk = N / B;
     const int total = P * nb;
     for (int t = tid; t < total; t += nth) {
         const int pen = t / nb;
         const int u = t - pen * nb;
-        const int b = u / m;
-        const int n1 = u - b * m;
+        const int b = b_fast ? u % nblk : u / m;
+        const int n1 = b_fast ? u / nblk : u - b * m;
         float2 *base = data + pen * ps + b * B + n1;
         float2 v[R];
         if constexpr (!INV) {
