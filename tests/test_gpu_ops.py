@@ -270,5 +270,11 @@ def test_toeplitz_compiled_fft_lengths(L, O, dims):
     opg = O.PolarGrid(th, 13, 11, np.float32(0.7), dtype=np.float64)
     x = rng.standard_normal((3,) + dims).astype(np.float32)
     want = O.sysmat(x, opg, opg.gamma, O.NufftPlan(dims, exact=True))
-    assert rel(L.ToeplitzNormal([pg], dims)(x), want) < TOL
+    T = L.ToeplitzNormal([pg], dims)
+    y = T(x)
+    assert rel(y, want) < TOL
     assert rel(L.ToeplitzNormal([pg], dims, "fp16")(x), want) < 2e-3
+    # the quadratic forms read the spectra in the same storage order as the apply
+    q = T.quadforms(x, [T])[0]
+    dots = [float(np.dot(x[i].ravel().astype(np.float64), y[i].ravel())) for i in range(3)]
+    assert np.allclose(q, dots, rtol=1e-5, atol=1e-6 * max(abs(d) for d in dots)), (q, dots)
