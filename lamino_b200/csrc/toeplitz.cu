@@ -167,6 +167,63 @@ __global__ void k_to_half(const float *__restrict__ K, int64_t n, int L1, const 
 // independent global loads kept in flight per thread in the load phases
 constexpr int LD_BATCH = 8;
 
+// Rows of M3 = 729 (schedule 9, 9, 9): the first radix-9 stage (one block, 81
+// offsets) runs in registers on the way in (k_r2c_rows) and its inverse on the
+// way out (k_c2r_rows).  Item (r, n) holds the packed values n + 81 j of row r.
+constexpr int R729_OFS = 81;
+
+__device__ __forceinline__ void rows729_load(const float *__restrict__ xb, int nr, int n3,
+                                             const float2 *__restrict__ tw3, float2 *__restrict__ sm, int ps,
+                                             int tid, int nth) {
+    for (int t = tid; t < nr * R729_OFS; t += nth) {
+        const int r = t / R729_OFS, n = t - r * R729_OFS;
+        const float *xr = xb + (int64_t)r * n3;
+        float2 x[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            const int i = 2 * (n + R729_OFS * j);
+            x[j].x = i < n3 ? xr[i] : 0.f;
+            x[j].y = i + 1 < n3 ? xr[i + 1] : 0.f;
+        }
+        dft_small<9, false>(x);
+        if (n != 0) {
+            float2 w[9];
+            twiddle_powers<9>(tw3, n, w);
+#pragma unroll
+            for (int k = 1; k < 9; ++k) x[k] = c_mul(x[k], w[k]);
+        }
+        float2 *sp = sm + r * ps + n;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sp[R729_OFS * k] = x[k];
+    }
+}
+
+__device__ __forceinline__ void rows729_store(const float2 *__restrict__ sm, int nr, int ps, int n3,
+                                              const float2 *__restrict__ tw3, float *__restrict__ yb, int tid,
+                                              int nth) {
+    for (int t = tid; t < nr * R729_OFS; t += nth) {
+        const int r = t / R729_OFS, n = t - r * R729_OFS;
+        const float2 *sp = sm + r * ps + n;
+        float2 a[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a[k] = sp[R729_OFS * k];
+        if (n != 0) {
+            float2 w[9];
+            twiddle_powers<9>(tw3, n, w);
+#pragma unroll
+            for (int k = 1; k < 9; ++k) a[k] = c_mulc(a[k], w[k]);
+        }
+        dft_small<9, true>(a);
+        float *yr = yb + (int64_t)r * n3;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            const int i = 2 * (n + R729_OFS * j);
+            if (i < n3) yr[i] = a[j].x;
+            if (i + 1 < n3) yr[i + 1] = a[j].y;
+        }
+    }
+}
+
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
@@ -178,7 +235,11 @@ __global__ void __launch_bounds__(256, 6) k_r2c_rows(const float *__restrict__ x
     const int ps = M3 + 1;
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
-    {
+    if constexpr (N3 == 729) {
+        rows729_load(x + row0 * n3, nr, n3, F3.tw, sm, ps, threadIdx.x, blockDim.x);
+        __syncthreads();
+        ct_forward<729, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
+    } else {
         const int total = nr * M3;
         const float *xb = x + row0 * n3;
         for (int t0 = threadIdx.x; t0 < total; t0 += LD_BATCH * blockDim.x) {
@@ -199,9 +260,9 @@ __global__ void __launch_bounds__(256, 6) k_r2c_rows(const float *__restrict__ x
                 }
             }
         }
+        __syncthreads();
+        fft_fwd_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
     }
-    __syncthreads();
-    fft_fwd_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
     for (int t = threadIdx.x; t < nr * (M3 + 1); t += blockDim.x) {
         int r = t / (M3 + 1), k = t - r * (M3 + 1);
         int ka = (k == M3) ? 0 : k;
@@ -228,9 +289,95 @@ __host__ __device__ constexpr int d2_stride(int L2, int KB) {
 }
 
 
+// n2 passes of L2 = 144 (schedule 2, 8, 9): the zero-padded radix-2 stage and the
+// radix-8 stage (two blocks of 72, 9 offsets each) run in registers on the way in
+// (k_dim2_fwd) and their inverses on the way out (k_dim2_inv).  Item (ii, n, kk),
+// kk fastest, holds the values i2 = n + 9 j of tile pencil ii * KB + kk.
+constexpr int D2_144_OFS = 9;
+
+// threads of an n2-pass CTA: one per item of the fused stages for L2 = 144
+__host__ __device__ constexpr int d2_threads(int L2, int KB) {
+    return (L2 == 144 && KB <= 4) ? D2_144_OFS * D2_IB * KB : 256;
+}
+
+__device__ __forceinline__ void dim2_144_load(const float2 *__restrict__ z1, int n1, int n2, int L3h, int c, int i1b,
+                                              int k3b, int nk, int KB, int ps, const float2 *__restrict__ tw2,
+                                              float2 *__restrict__ sm, int tid, int nth) {
+    const int total = D2_IB * D2_144_OFS * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int n = r % D2_144_OFS, ii = r / D2_144_OFS;
+        const int i1 = i1b + ii;
+        const bool live = kk < nk && i1 < n1;
+        float2 x[8], u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int i2 = n + D2_144_OFS * j;
+            x[j] = (live && i2 < n2) ? z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = c_mul(x[j], __ldg(tw2 + n + D2_144_OFS * j));
+        dft_small<8, false>(x);
+        dft_small<8, false>(u);
+        if (n != 0) {
+            float2 w[8];
+            twiddle_powers<8>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < 8; ++k) {
+                x[k] = c_mul(x[k], w[k]);
+                u[k] = c_mul(u[k], w[k]);
+            }
+        }
+        float2 *sp = sm + (ii * KB + kk) * ps + n;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            sp[D2_144_OFS * k] = x[k];
+            sp[72 + D2_144_OFS * k] = u[k];
+        }
+    }
+}
+
+__device__ __forceinline__ void dim2_144_store(const float2 *__restrict__ sm, int n1, int n2, int L3h, int c,
+                                               int i1b, int k3b, int nk, int KB, int ps,
+                                               const float2 *__restrict__ tw2, float2 *__restrict__ z1, int tid,
+                                               int nth) {
+    const int total = D2_IB * D2_144_OFS * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int n = r % D2_144_OFS, ii = r / D2_144_OFS;
+        const int i1 = i1b + ii;
+        if (kk >= nk || i1 >= n1) continue;
+        const float2 *sp = sm + (ii * KB + kk) * ps + n;
+        float2 a[8], b[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a[k] = sp[D2_144_OFS * k];
+            b[k] = sp[72 + D2_144_OFS * k];
+        }
+        if (n != 0) {
+            float2 w[8];
+            twiddle_powers<8>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < 8; ++k) {
+                a[k] = c_mulc(a[k], w[k]);
+                b[k] = c_mulc(b[k], w[k]);
+            }
+        }
+        dft_small<8, true>(a);
+        dft_small<8, true>(b);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int i2 = n + D2_144_OFS * j;
+            if (i2 < n2)
+                z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] =
+                    c_add(a[j], c_mulc(b[j], __ldg(tw2 + i2)));
+        }
+    }
+}
+
 // A2: columns along n2 (zero-padded to L2) -> pencil-major xa[((c L2 + p2) L3h + k3) n1p + i1]
 template <int N2>
-__global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, int n1p,
+__global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, int n1p,
                                                   FftLen F2, const float2 *__restrict__ tw2, int KB,
                                                   float2 *__restrict__ xa) {
     extern __shared__ float2 sm[];
@@ -238,38 +385,44 @@ __global__ void __launch_bounds__(256) k_dim2_fwd(const float2 *__restrict__ z1,
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
     const int ps = d2_stride(L2, KB), half = L2 / 2;
-    // load: kk fastest (coalesced along k3); D2_BATCH independent loads in flight per thread
-    constexpr int D2_BATCH = 4;
-    const int total = D2_IB * half * KB;
-    for (int t0 = threadIdx.x; t0 < total; t0 += D2_BATCH * blockDim.x) {
-        float2 v[D2_BATCH];
+    if constexpr (N2 == 144) {
+        dim2_144_load(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm, threadIdx.x, blockDim.x);
+        __syncthreads();
+        ct_forward<144, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+    } else {
+        // load: kk fastest (coalesced along k3); D2_BATCH independent loads in flight per thread
+        constexpr int D2_BATCH = 4;
+        const int total = D2_IB * half * KB;
+        for (int t0 = threadIdx.x; t0 < total; t0 += D2_BATCH * blockDim.x) {
+            float2 v[D2_BATCH];
 #pragma unroll
-        for (int u = 0; u < D2_BATCH; ++u) {
-            int t = t0 + u * blockDim.x;
-            int kk = t % KB;
-            int r = t / KB;
-            int i2 = r % half;
-            int i1 = i1b + r / half;
-            v[u] = make_float2(0.f, 0.f);
-            if (t < total && kk < nk && i2 < n2 && i1 < n1)
-                v[u] = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
-        }
-#pragma unroll
-        for (int u = 0; u < D2_BATCH; ++u) {
-            int t = t0 + u * blockDim.x;
-            if (t < total) {
+            for (int u = 0; u < D2_BATCH; ++u) {
+                int t = t0 + u * blockDim.x;
                 int kk = t % KB;
                 int r = t / KB;
                 int i2 = r % half;
-                int ii = r / half;
-                float2 *pp = sm + (ii * KB + kk) * ps;
-                pp[i2] = v[u];
-                pp[i2 + half] = c_mul(v[u], __ldg(tw2 + i2));
+                int i1 = i1b + r / half;
+                v[u] = make_float2(0.f, 0.f);
+                if (t < total && kk < nk && i2 < n2 && i1 < n1)
+                    v[u] = z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk];
+            }
+#pragma unroll
+            for (int u = 0; u < D2_BATCH; ++u) {
+                int t = t0 + u * blockDim.x;
+                if (t < total) {
+                    int kk = t % KB;
+                    int r = t / KB;
+                    int i2 = r % half;
+                    int ii = r / half;
+                    float2 *pp = sm + (ii * KB + kk) * ps;
+                    pp[i2] = v[u];
+                    pp[i2 + half] = c_mul(v[u], __ldg(tw2 + i2));
+                }
             }
         }
+        __syncthreads();
+        fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     }
-    __syncthreads();
-    fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     // store: one thread per (p2, kk) writes its 8 i1 values (64 B)
     for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
         int kk = t % nk, p2 = t / nk;
@@ -354,10 +507,10 @@ __device__ __forceinline__ void pencil1458_store(float2 *__restrict__ pv, int64_
 
 // B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
 // symmetric multiply with the spectra (same position order), undo, first n1 kept.
-// In place on xa.  N1: compile-time L1 or 0.  Five CTAs of 256 threads per SM
-// (48 registers, 35 KB of shared memory each at L1 = 1458).
+// In place on xa.  N1: compile-time L1 or 0.  At L1 = 1458, five CTAs of 256
+// threads per SM (48 registers, 35 KB of shared memory each); four otherwise.
 template <bool HALF, int N1>
-__global__ void __launch_bounds__(256, 5) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
+__global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
                                                 const float2 *__restrict__ tw1, const float *__restrict__ K,
                                                 const __half *__restrict__ Kh, const float *__restrict__ kscale) {
     extern __shared__ float2 sm[];
@@ -516,7 +669,7 @@ __global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ 
 
 // C2: undo along k2 (positions -> natural), first n2 rows kept, back into z1 rows
 template <int N2>
-__global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, int n1p,
+__global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ xa, int n1, int n2, int L3h, int n1p,
                                                   FftLen F2, const float2 *__restrict__ tw2, int KB,
                                                   float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
@@ -555,6 +708,11 @@ __global__ void __launch_bounds__(256) k_dim2_inv(const float2 *__restrict__ xa,
         }
     }
     __syncthreads();
+    if constexpr (N2 == 144) {
+        ct_inverse<144, 2, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+        dim2_144_store(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1, threadIdx.x, blockDim.x);
+        return;
+    }
     fft_inv_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     // store: kk fastest (coalesced along k3)
     for (int t = threadIdx.x; t < D2_IB * n2 * nk; t += blockDim.x) {
@@ -607,6 +765,11 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
         }
     }
     __syncthreads();
+    if constexpr (N3 == 729) {
+        ct_inverse<729, 2, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
+        rows729_store(sm, nr, ps, n3, F3.tw, y + row0 * n3, threadIdx.x, blockDim.x);
+        return;
+    }
     fft_inv_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
     for (int t = threadIdx.x; t < nr * M3; t += blockDim.x) {
         int r = t / M3, m = t - r * M3;
@@ -938,7 +1101,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[1], s));
-    if (ct2) k_dim2_fwd<144><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    if (ct2) k_dim2_fwd<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
@@ -953,7 +1116,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
         k_pencil<false, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
     LAMINO_LAUNCH("k_pencil");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[3], s));
-    if (ct2) k_dim2_inv<144><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
+    if (ct2) k_dim2_inv<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
     else k_dim2_inv<0><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
     LAMINO_LAUNCH("k_dim2_inv");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[4], s));
@@ -986,7 +1149,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
     if (ct3) k_r2c_rows<729><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
-    if (ct2) k_dim2_fwd<144><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    if (ct2) k_dim2_fwd<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     for (size_t g0 = 0; g0 < parts.size(); g0 += kMaxQuadSets) {
