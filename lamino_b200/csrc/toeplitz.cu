@@ -423,16 +423,15 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         __syncthreads();
         fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     }
-    // store: one thread per (p2, kk) writes its 8 i1 values (64 B)
-    for (int t = threadIdx.x; t < L2 * nk; t += blockDim.x) {
-        int kk = t % nk, p2 = t / nk;
+    // store: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each,
+    // so a warp writes 8 runs rather than 32
+    for (int t = threadIdx.x; t < L2 * nk * (D2_IB / 2); t += blockDim.x) {
+        const int h = t % (D2_IB / 2), it = t / (D2_IB / 2);
+        const int kk = it % nk, p2 = it / nk;
         float4 *dst = reinterpret_cast<float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
-#pragma unroll
-        for (int h = 0; h < D2_IB / 2; ++h) {
-            float2 a = sm[((2 * h) * KB + kk) * ps + p2];
-            float2 b = sm[((2 * h + 1) * KB + kk) * ps + p2];
-            dst[h] = make_float4(a.x, a.y, b.x, b.y);
-        }
+        const float2 a = sm[((2 * h) * KB + kk) * ps + p2];
+        const float2 b = sm[((2 * h + 1) * KB + kk) * ps + p2];
+        dst[h] = make_float4(a.x, a.y, b.x, b.y);
     }
 }
 
@@ -677,33 +676,29 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
     const int ps = d2_stride(L2, KB), half = L2 / 2;
-    // load: one thread per (p2, kk) reads its 8 i1 values (64 B); two tasks in flight
-    for (int t0 = threadIdx.x; t0 < L2 * KB; t0 += 2 * blockDim.x) {
-        float4 q[2][D2_IB / 2];
+    // load: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each, so a
+    // warp reads 8 runs rather than 32; D2_LD runs in flight per thread
+    constexpr int D2_LD = 4;
+    const int ltotal = L2 * KB * (D2_IB / 2);
+    for (int t0 = threadIdx.x; t0 < ltotal; t0 += D2_LD * blockDim.x) {
+        float4 q[D2_LD];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            int t = t0 + u * blockDim.x;
-            int kk = t % KB, p2 = t / KB;
-            if (t < L2 * KB && kk < nk) {
-                const float4 *src =
-                    reinterpret_cast<const float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
-#pragma unroll
-                for (int h = 0; h < D2_IB / 2; ++h) q[u][h] = src[h];
-            } else {
-#pragma unroll
-                for (int h = 0; h < D2_IB / 2; ++h) q[u][h] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+        for (int u = 0; u < D2_LD; ++u) {
+            const int t = t0 + u * blockDim.x;
+            const int h = t % (D2_IB / 2), it = t / (D2_IB / 2);
+            const int kk = it % KB, p2 = it / KB;
+            q[u] = (t < ltotal && kk < nk)
+                       ? reinterpret_cast<const float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b)[h]
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            int t = t0 + u * blockDim.x;
-            if (t < L2 * KB) {
-                int kk = t % KB, p2 = t / KB;
-#pragma unroll
-                for (int h = 0; h < D2_IB / 2; ++h) {
-                    sm[((2 * h) * KB + kk) * ps + p2] = make_float2(q[u][h].x, q[u][h].y);
-                    sm[((2 * h + 1) * KB + kk) * ps + p2] = make_float2(q[u][h].z, q[u][h].w);
-                }
+        for (int u = 0; u < D2_LD; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < ltotal) {
+                const int h = t % (D2_IB / 2), it = t / (D2_IB / 2);
+                const int kk = it % KB, p2 = it / KB;
+                sm[((2 * h) * KB + kk) * ps + p2] = make_float2(q[u].x, q[u].y);
+                sm[((2 * h + 1) * KB + kk) * ps + p2] = make_float2(q[u].z, q[u].w);
             }
         }
     }
