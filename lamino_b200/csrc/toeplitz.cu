@@ -545,34 +545,46 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
         fft_fwd_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
     }
     const float sc = HALF ? kscale[pen] : 1.f;
-    constexpr int KU = 2;  // p1 values whose 6 spectra are in flight together
-    for (int q0 = threadIdx.x; q0 < L1; q0 += KU * blockDim.x) {
-        float kv[KU][6];
+    // two adjacent positions per thread (L1 is even): 8-byte spectrum loads and
+    // 16-byte shared accesses; KU pairs whose 6 spectra are in flight together
+    constexpr int KU = 2;
+    const int L1h = L1 / 2;
+    for (int q0 = threadIdx.x; q0 < L1h; q0 += KU * blockDim.x) {
+        float2 kv[KU][6];
 #pragma unroll
         for (int u = 0; u < KU; ++u) {
-            int p1 = q0 + u * blockDim.x;
-            if (p1 < L1) {
+            const int pp = q0 + u * blockDim.x;
+            if (pp < L1h) {
                 if (HALF) {
-                    const __half *Kp = Kh + pen * 6 * L1 + p1;
+                    const __half2 *Kp = reinterpret_cast<const __half2 *>(Kh + pen * 6 * L1) + pp;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) kv[u][q] = __half2float(Kp[q * L1]) * sc;
+                    for (int q = 0; q < 6; ++q) {
+                        const float2 k = __half22float2(Kp[q * L1h]);
+                        kv[u][q] = make_float2(k.x * sc, k.y * sc);
+                    }
                 } else {
-                    const float *Kp = K + pen * 6 * L1 + p1;
+                    const float2 *Kp = reinterpret_cast<const float2 *>(K + pen * 6 * L1) + pp;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) kv[u][q] = Kp[q * L1];
+                    for (int q = 0; q < 6; ++q) kv[u][q] = Kp[q * L1h];
                 }
             }
         }
 #pragma unroll
         for (int u = 0; u < KU; ++u) {
-            int p1 = q0 + u * blockDim.x;
-            if (p1 < L1) {
-                const float k00 = kv[u][0], k11 = kv[u][1], k22 = kv[u][2], k01 = kv[u][3], k02 = kv[u][4],
-                            k12 = kv[u][5];
-                float2 a = sm[p1], b = sm[L1 + p1], c = sm[2 * L1 + p1];
-                sm[p1] = make_float2(k00 * a.x + k01 * b.x + k02 * c.x, k00 * a.y + k01 * b.y + k02 * c.y);
-                sm[L1 + p1] = make_float2(k01 * a.x + k11 * b.x + k12 * c.x, k01 * a.y + k11 * b.y + k12 * c.y);
-                sm[2 * L1 + p1] = make_float2(k02 * a.x + k12 * b.x + k22 * c.x, k02 * a.y + k12 * b.y + k22 * c.y);
+            const int pp = q0 + u * blockDim.x;
+            if (pp < L1h) {
+                float4 *s0 = reinterpret_cast<float4 *>(sm) + pp;
+                float4 *s1 = reinterpret_cast<float4 *>(sm + L1) + pp;
+                float4 *s2 = reinterpret_cast<float4 *>(sm + 2 * L1) + pp;
+                const float4 a = *s0, b = *s1, c = *s2;
+                const float2 k00 = kv[u][0], k11 = kv[u][1], k22 = kv[u][2], k01 = kv[u][3], k02 = kv[u][4],
+                             k12 = kv[u][5];
+                *s0 = make_float4(k00.x * a.x + k01.x * b.x + k02.x * c.x, k00.x * a.y + k01.x * b.y + k02.x * c.y,
+                                  k00.y * a.z + k01.y * b.z + k02.y * c.z, k00.y * a.w + k01.y * b.w + k02.y * c.w);
+                *s1 = make_float4(k01.x * a.x + k11.x * b.x + k12.x * c.x, k01.x * a.y + k11.x * b.y + k12.x * c.y,
+                                  k01.y * a.z + k11.y * b.z + k12.y * c.z, k01.y * a.w + k11.y * b.w + k12.y * c.w);
+                *s2 = make_float4(k02.x * a.x + k12.x * b.x + k22.x * c.x, k02.x * a.y + k12.x * b.y + k22.x * c.y,
+                                  k02.y * a.z + k12.y * b.z + k22.y * c.z, k02.y * a.w + k12.y * b.w + k22.y * c.w);
             }
         }
     }
