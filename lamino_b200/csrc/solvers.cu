@@ -144,6 +144,30 @@ void vec_lin2(float *out, float a, const float *x, float b, const float *y, int6
 }
 void vec_scale(float *out, float a, const float *x, int64_t n, cudaStream_t s) { vec_lin2(out, a, x, 0.f, nullptr, n, s); }
 
+// One thread per (k, j) column of voxels (and component): k = blockIdx.x * kVoxX +
+// threadIdx.x, j = blockIdx.y, and a contiguous run of the planes z = comp * n1 + i
+// for blockIdx.z (PlaneRun), so no thread divides its index.  About 148 x 64 CTAs in all.
+struct Idx3 {
+    int i, j, k;
+};
+constexpr int kVoxX = 128;
+// this CTA's contiguous run of planes [z0, z1) of nz: neighbouring planes follow
+// each other in one thread, so their shared rows are still in L1
+struct PlaneRun {
+    int z0, z1;
+    __device__ PlaneRun(int nz) {
+        const int per = (nz + (int)gridDim.z - 1) / (int)gridDim.z;
+        z0 = (int)blockIdx.z * per;
+        z1 = min(nz, z0 + per);
+    }
+};
+static dim3 vox_grid(Dims3 d, int ncomp) {
+    if (d.n2 > 65535) throw Error(ERR_ARG, "n2 above 65535 is not supported by the voxel kernels");
+    const int64_t gx = (d.n3 + kVoxX - 1) / kVoxX, gy = d.n2;
+    const int64_t gz = std::max<int64_t>(1, std::min<int64_t>({d.n1 * ncomp, 65535, 148LL * 64 / (gx * gy) + 1}));
+    return dim3((unsigned)gx, (unsigned)gy, (unsigned)gz);
+}
+
 // ---------------------------------------------------------------------------
 // qGGMRF (src/qggmrf.cpp:25-95)
 // ---------------------------------------------------------------------------
@@ -173,15 +197,15 @@ __device__ __forceinline__ float d_potential(float delta, const QgConst &k) {
     return a * (2.0f - k.qmp * t1 * r);
 }
 
-__global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2, int n3, QgConst kq) {
-    const int64_t ni = (int64_t)(n1 - 2) * (n2 - 2) * (n3 - 2);
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ni; t += (int64_t)gridDim.x * blockDim.x) {
-        int k = (int)(t % (n3 - 2)) + 1;
-        int64_t r = t / (n3 - 2);
-        int j = (int)(r % (n2 - 2)) + 1;
-        int i = (int)(r / (n2 - 2)) + 1;
-        int64_t c = ((int64_t)i * n2 + j) * n3 + k;
-        float u = x[c];
+__global__ void __launch_bounds__(kVoxX) k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2,
+                                                  int n3, QgConst kq) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
+    if (k < 1 || k > n3 - 2 || j < 1 || j > n2 - 2) return;  // interior voxels only
+    const PlaneRun pr(n1);
+    for (int i = pr.z0; i < pr.z1; ++i) {
+        if (i < 1 || i > n1 - 2) continue;
+        const int64_t c = ((int64_t)i * n2 + j) * n3 + k;
+        const float u = x[c];
         float sum = 0.f;
 #pragma unroll
         for (int dx = -1; dx < 2; ++dx)
@@ -190,8 +214,8 @@ __global__ void k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int
 #pragma unroll
                 for (int dz = -1; dz < 2; ++dz) {
                     if (dx == 0 && dy == 0 && dz == 0) continue;
-                    float v = x[c + ((int64_t)dx * n2 + dy) * n3 + dz];
-                    float w = c_qggmrf_w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
+                    const float v = x[c + ((int64_t)dx * n2 + dy) * n3 + dz];
+                    const float w = c_qggmrf_w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
                     sum += w * d_potential(v - u, kq);
                 }
         g[c] += sum;
@@ -202,13 +226,12 @@ void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStr
     if (d.n1 < 3 || d.n2 < 3 || d.n3 < 3) return;  // no interior voxels
     float sigma_q = std::pow(sigma, 2.0f);
     float sigma_qp = std::pow(sigma, 2.0f - p);
-    int64_t ni = (d.n1 - 2) * (d.n2 - 2) * (d.n3 - 2);
     QgConst kq;
     kq.qmp = 2.0f - p;
     kq.inv_sqp = (float)(1.0 / (double)sigma_qp);
     kq.inv_sq = (float)(1.0 / (double)sigma_q);
     kq.at_zero = (float)(2.0 / ((double)sigma_q * 0.001));
-    k_qggmrf<<<grid_for(ni, 256), 256, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, kq);
+    k_qggmrf<<<vox_grid(d, 1), kVoxX, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, kq);
     LAMINO_LAUNCH("k_qggmrf");
 }
 
@@ -216,17 +239,6 @@ void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStr
 // finite differences (src/finitediff.cpp:8-71, include/bregman.h:34-36)
 // ---------------------------------------------------------------------------
 
-struct Idx3 {
-    int i, j, k;
-};
-__device__ __forceinline__ Idx3 unravel(int64_t idx, int n2, int n3) {
-    Idx3 r;
-    r.k = (int)(idx % n3);
-    int64_t q = idx / n3;
-    r.j = (int)(q % n2);
-    r.i = (int)(q / n2);
-    return r;
-}
 __device__ __forceinline__ bool interior(int i, int j, int k, int n1, int n2, int n3) {
     return i >= 1 && i < n1 - 1 && j >= 1 && j < n2 - 1 && k >= 1 && k < n3 - 1;
 }
@@ -237,14 +249,18 @@ __device__ __forceinline__ float gdir(const float *__restrict__ u, int i, int j,
     if (!interior(i, j, k, n1, n2, n3)) return 0.f;
     int64_t c = ((int64_t)i * n2 + j) * n3 + k;
     int64_t st = dim == 0 ? (int64_t)n2 * n3 : (dim == 1 ? n3 : 1);
-    return (float)((double)(u[c + st] - u[c - st]) / 2.0);
+    return (u[c + st] - u[c - st]) * 0.5f;  // the reference's (float diff) / 2.0: halving is exact
 }
 
-__global__ void k_grad_u(const float *__restrict__ u, int n1, int n2, int n3, float *__restrict__ out3) {
+__global__ void __launch_bounds__(kVoxX) k_grad_u(const float *__restrict__ u, int n1, int n2, int n3,
+                                                  float *__restrict__ out3) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
+    if (k >= n3) return;
     const int64_t V = (int64_t)n1 * n2 * n3;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
-        Idx3 p = unravel(t, n2, n3);
-        for (int dim = 0; dim < 3; ++dim) out3[dim * V + t] = gdir(u, p.i, p.j, p.k, n1, n2, n3, dim);
+    const PlaneRun pr(n1);
+    for (int i = pr.z0; i < pr.z1; ++i) {
+        const int64_t t = ((int64_t)i * n2 + j) * n3 + k;
+        for (int dim = 0; dim < 3; ++dim) out3[dim * V + t] = gdir(u, i, j, k, n1, n2, n3, dim);
     }
 }
 
@@ -258,52 +274,64 @@ __device__ __forceinline__ float neg_div(const F &f, int i, int j, int k, int n1
     return (float)(a - b - c);
 }
 
-__global__ void k_divergence(const float *__restrict__ du3, int n1, int n2, int n3, float *__restrict__ out) {
+__global__ void __launch_bounds__(kVoxX) k_divergence(const float *__restrict__ du3, int n1, int n2, int n3,
+                                                      float *__restrict__ out) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
+    if (k >= n3) return;
     const int64_t V = (int64_t)n1 * n2 * n3;
     auto f = [&](int dim, int i, int j, int k) { return du3[dim * V + ((int64_t)i * n2 + j) * n3 + k]; };
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
-        Idx3 p = unravel(t, n2, n3);
-        out[t] = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
-    }
+    const PlaneRun pr(n1);
+    for (int i = pr.z0; i < pr.z1; ++i) out[((int64_t)i * n2 + j) * n3 + k] = neg_div(f, i, j, k, n1, n2, n3);
 }
 
 // y += mu * divergence(grad_u(u)) for NC contiguous components
-__global__ void k_laplacian_axpy(float *__restrict__ y, float mu, const float *__restrict__ u, int n1, int n2,
-                                 int n3) {
+__global__ void __launch_bounds__(kVoxX) k_laplacian_axpy(float *__restrict__ y, float mu, const float *__restrict__ u,
+                                                          int n1, int n2, int n3) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
+    if (k >= n3) return;
     const int64_t V = (int64_t)n1 * n2 * n3;
-    const int comp = blockIdx.y;
-    const float *uc = u + comp * V;
-    auto f = [&](int dim, int i, int j, int k) { return gdir(uc, i, j, k, n1, n2, n3, dim); };
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
-        Idx3 p = unravel(t, n2, n3);
-        float l = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
-        y[comp * V + t] += l * mu;
+    const PlaneRun pr(3 * n1);
+    for (int z = pr.z0; z < pr.z1; ++z) {
+        const int comp = z / n1, i = z - comp * n1;
+        const float *uc = u + comp * V;
+        auto f = [&](int dim, int ii, int jj, int kk) { return gdir(uc, ii, jj, kk, n1, n2, n3, dim); };
+        const float l = neg_div(f, i, j, k, n1, n2, n3);
+        y[comp * V + ((int64_t)i * n2 + j) * n3 + k] += l * mu;
     }
 }
 
-__global__ void k_sb_rhs(const float *__restrict__ yT, const float *__restrict__ d9, const float *__restrict__ b9,
-                         float mu, int n1, int n2, int n3, float *__restrict__ rhs) {
+__global__ void __launch_bounds__(kVoxX) k_sb_rhs(const float *__restrict__ yT, const float *__restrict__ d9,
+                                                  const float *__restrict__ b9, float mu, int n1, int n2, int n3,
+                                                  float *__restrict__ rhs) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
+    if (k >= n3) return;
     const int64_t V = (int64_t)n1 * n2 * n3;
-    const int comp = blockIdx.y;
-    const float *dc = d9 + 3 * comp * V, *bc = b9 + 3 * comp * V;
-    auto f = [&](int dim, int i, int j, int k) {
-        int64_t c = dim * V + ((int64_t)i * n2 + j) * n3 + k;
-        return dc[c] - bc[c];
-    };
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
-        Idx3 p = unravel(t, n2, n3);
-        float dv = neg_div(f, p.i, p.j, p.k, n1, n2, n3);
+    const PlaneRun pr(3 * n1);
+    for (int z = pr.z0; z < pr.z1; ++z) {
+        const int comp = z / n1, i = z - comp * n1;
+        const float *dc = d9 + 3 * comp * V, *bc = b9 + 3 * comp * V;
+        auto f = [&](int dim, int ii, int jj, int kk) {
+            int64_t c = dim * V + ((int64_t)ii * n2 + jj) * n3 + kk;
+            return dc[c] - bc[c];
+        };
+        const int64_t t = ((int64_t)i * n2 + j) * n3 + k;
+        const float dv = neg_div(f, i, j, k, n1, n2, n3);
         rhs[comp * V + t] = yT[comp * V + t] + dv * mu;
     }
 }
 
-__global__ void k_sb_shrink(const float *__restrict__ x3, float *__restrict__ d9, float *__restrict__ b9, float lam,
-                            float mu, int n1, int n2, int n3) {
+__global__ void __launch_bounds__(kVoxX) k_sb_shrink(const float *__restrict__ x3, float *__restrict__ d9,
+                                                     float *__restrict__ b9, float lam, float mu, int n1, int n2,
+                                                     int n3) {
+    const int k = blockIdx.x * kVoxX + threadIdx.x, jj = blockIdx.y;
+    if (k >= n3) return;
     const int64_t V = (int64_t)n1 * n2 * n3;
     const float eps = 1e-8f;
     const float thr = lam / mu;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < V; t += (int64_t)gridDim.x * blockDim.x) {
-        Idx3 p = unravel(t, n2, n3);
+    const PlaneRun prn(n1);
+    for (int ii = prn.z0; ii < prn.z1; ++ii) {
+        const int64_t t = ((int64_t)ii * n2 + jj) * n3 + k;
+        const Idx3 p{ii, jj, k};
         float gx[9], tb[9];
         float sk = 1.0f * eps;
 #pragma unroll
@@ -326,26 +354,24 @@ __global__ void k_sb_shrink(const float *__restrict__ x3, float *__restrict__ d9
 }
 
 void grad_u(const float *u, Dims3 d, float *out3, cudaStream_t s) {
-    k_grad_u<<<grid_for(d.size(), 256), 256, 0, s>>>(u, (int)d.n1, (int)d.n2, (int)d.n3, out3);
+    k_grad_u<<<vox_grid(d, 1), kVoxX, 0, s>>>(u, (int)d.n1, (int)d.n2, (int)d.n3, out3);
     LAMINO_LAUNCH("k_grad_u");
 }
 void divergence(const float *du3, Dims3 d, float *out, cudaStream_t s) {
-    k_divergence<<<grid_for(d.size(), 256), 256, 0, s>>>(du3, (int)d.n1, (int)d.n2, (int)d.n3, out);
+    k_divergence<<<vox_grid(d, 1), kVoxX, 0, s>>>(du3, (int)d.n1, (int)d.n2, (int)d.n3, out);
     LAMINO_LAUNCH("k_divergence");
 }
 void laplacian_axpy(float *y, float mu, const float *u, Dims3 d, cudaStream_t s) {
-    dim3 g(grid_for(d.size(), 256), 3);
-    k_laplacian_axpy<<<g, 256, 0, s>>>(y, mu, u, (int)d.n1, (int)d.n2, (int)d.n3);
+    k_laplacian_axpy<<<vox_grid(d, 3), kVoxX, 0, s>>>(y, mu, u, (int)d.n1, (int)d.n2, (int)d.n3);
     LAMINO_LAUNCH("k_laplacian_axpy");
 }
 void sb_rhs(const float *yT3, const float *d9, const float *b9, float mu, Dims3 dims, float *rhs3, cudaStream_t s) {
-    dim3 g(grid_for(dims.size(), 256), 3);
-    k_sb_rhs<<<g, 256, 0, s>>>(yT3, d9, b9, mu, (int)dims.n1, (int)dims.n2, (int)dims.n3, rhs3);
+    k_sb_rhs<<<vox_grid(dims, 3), kVoxX, 0, s>>>(yT3, d9, b9, mu, (int)dims.n1, (int)dims.n2, (int)dims.n3, rhs3);
     LAMINO_LAUNCH("k_sb_rhs");
 }
 void sb_shrink(const float *x3, float *d9, float *b9, float lam, float mu, Dims3 dims, cudaStream_t s) {
-    k_sb_shrink<<<grid_for(dims.size(), 256), 256, 0, s>>>(x3, d9, b9, lam, mu, (int)dims.n1, (int)dims.n2,
-                                                           (int)dims.n3);
+    k_sb_shrink<<<vox_grid(dims, 1), kVoxX, 0, s>>>(x3, d9, b9, lam, mu, (int)dims.n1, (int)dims.n2,
+                                                    (int)dims.n3);
     LAMINO_LAUNCH("k_sb_shrink");
 }
 
@@ -361,6 +387,74 @@ __global__ void k_filter_mul(float2 *__restrict__ S, const float *__restrict__ f
     }
 }
 
+// Along n2 the filter step (forward DFT, multiply by the ramp, inverse DFT) is a
+// circulant convolution for each k3 column, z(:, k3) = G_k3 (*) x(:, k3), with
+// G_k3[d] = sum_k2 f(k2, k3) cos(2 pi k2 d / n2): f is real and even in k2, so G_k3
+// is real (and even).  One CTA per (n1 slice, RC_KB consecutive k3 columns): the
+// column tile twice over in shared memory (so m - d + n2 needs no wrap), lanes on
+// columns, warps on output rows, taps summed in order d = 0 .. n2-1.
+constexpr int RC_KB = 32;
+constexpr int RC_WARPS = 8;
+constexpr int RC_ROWS = 9;  // output rows per thread: 8 warps x 9 rows cover n2 <= 72 in one pass
+constexpr int kRampConvMaxN2 = 128;
+
+__global__ void __launch_bounds__(RC_WARPS * 32) k_ramp_cols(float2 *__restrict__ S, const float *__restrict__ G,
+                                                             int n2, int h3) {
+    extern __shared__ float2 xs[];                                // [2 n2][RC_KB]
+    float *gs = reinterpret_cast<float *>(xs + 2 * n2 * RC_KB);   // [n2][RC_KB]
+    const int k3b = blockIdx.x * RC_KB;
+    const int nk = min(RC_KB, h3 - k3b);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2 *Sp = S + (int64_t)blockIdx.y * n2 * h3 + k3b;
+    // load: the column tile (twice) and the kernels, 8 independent loads in flight per thread
+    constexpr int LB = 8;
+    const int total = n2 * RC_KB;
+    for (int t0 = threadIdx.x; t0 < total; t0 += LB * RC_WARPS * 32) {
+        float2 v[LB];
+        float gv[LB];
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int t = t0 + u * RC_WARPS * 32;
+            const int j = t / RC_KB, kk = t - j * RC_KB;
+            const bool ok = t < total && kk < nk;
+            v[u] = ok ? Sp[(int64_t)j * h3 + kk] : make_float2(0.f, 0.f);
+            gv[u] = ok ? __ldg(G + (int64_t)j * h3 + k3b + kk) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int t = t0 + u * RC_WARPS * 32;
+            if (t < total) {
+                const int j = t / RC_KB, kk = t - j * RC_KB;
+                xs[j * RC_KB + kk] = v[u];
+                xs[(j + n2) * RC_KB + kk] = v[u];
+                gs[j * RC_KB + kk] = gv[u];
+            }
+        }
+    }
+    __syncthreads();
+    for (int m0 = warp * RC_ROWS; m0 < n2; m0 += RC_ROWS * RC_WARPS) {
+        float2 acc[RC_ROWS];
+#pragma unroll
+        for (int r = 0; r < RC_ROWS; ++r) acc[r] = make_float2(0.f, 0.f);
+        for (int dd = 0; dd < n2; ++dd) {
+            const float g = gs[dd * RC_KB + lane];
+            const float2 *xr = xs + (m0 - dd + n2) * RC_KB + lane;
+#pragma unroll
+            for (int r = 0; r < RC_ROWS; ++r) {
+                // rows past n2 - 1 re-read row n2 - 1 (inside the tile) and are never stored
+                const float2 x = xr[min(r, n2 - 1 - m0) * RC_KB];
+                acc[r].x = fmaf(g, x.x, acc[r].x);
+                acc[r].y = fmaf(g, x.y, acc[r].y);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RC_ROWS; ++r) {
+            const int m = m0 + r;
+            if (m < n2 && lane < nk) Sp[(int64_t)m * h3 + lane] = acc[r];
+        }
+    }
+}
+
 RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
     int64_t n2 = d.n2, n3 = d.n3, h3 = n3 / 2 + 1;
     std::vector<float> xf(h3), yf(n2), f(n2 * h3);
@@ -370,12 +464,32 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
     float scale = (float)(1.0 / (double)(n2 * n3));
     for (int64_t j = 0; j < n2; ++j)
         for (int64_t i = 0; i < h3; ++i) f[j * h3 + i] = std::sqrt(xf[i] * xf[i] + yf[j] * yf[j]) * scale;
-    filt.alloc(n2 * h3);
-    upload(filt.p, f.data(), f.size());
     spec.alloc(3 * d.n1 * n2 * h3);
-    int n[2] = {(int)n2, (int)n3};
-    r2c.make(2, n, CUFFT_R2C, (int)(3 * d.n1));
-    c2r.make(2, n, CUFFT_C2R, (int)(3 * d.n1));
+    cols = n2 <= kRampConvMaxN2 && 3 * d.n1 <= 65535;
+    if (cols) {
+        // G[dd * h3 + k3] = sum_k2 f(k2, k3) cos(2 pi k2 dd / n2), in double
+        std::vector<double> cs(n2);
+        for (int64_t t = 0; t < n2; ++t) cs[t] = std::cos(2.0 * M_PI * (double)t / (double)n2);
+        std::vector<float> g(n2 * h3);
+        for (int64_t dd2 = 0; dd2 < n2; ++dd2)
+            for (int64_t i = 0; i < h3; ++i) {
+                double acc = 0.0;
+                for (int64_t j = 0; j < n2; ++j) acc += (double)f[j * h3 + i] * cs[(j * dd2) % n2];
+                g[dd2 * h3 + i] = (float)acc;
+            }
+        filt.alloc(n2 * h3);
+        upload(filt.p, g.data(), g.size());
+        int n[1] = {(int)n3};
+        r2c.make(1, n, CUFFT_R2C, (int)(3 * d.n1 * n2));
+        c2r.make(1, n, CUFFT_C2R, (int)(3 * d.n1 * n2));
+        raise_smem_limit((const void *)k_ramp_cols, (int)(n2 * RC_KB * (2 * sizeof(float2) + sizeof(float))));
+    } else {
+        filt.alloc(n2 * h3);
+        upload(filt.p, f.data(), f.size());
+        int n[2] = {(int)n2, (int)n3};
+        r2c.make(2, n, CUFFT_R2C, (int)(3 * d.n1));
+        c2r.make(2, n, CUFFT_C2R, (int)(3 * d.n1));
+    }
 }
 
 void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
@@ -383,8 +497,15 @@ void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
     LAMINO_CUFFT(cufftSetStream(r2c.h, s));
     LAMINO_CUFFT(cufftSetStream(c2r.h, s));
     LAMINO_CUFFT(cufftExecR2C(r2c.h, const_cast<float *>(r3), (cufftComplex *)spec.p));
-    k_filter_mul<<<grid_for(3 * d.n1 * plane, 256), 256, 0, s>>>(spec.p, filt.p, plane, 3 * d.n1 * plane);
-    LAMINO_LAUNCH("k_filter_mul");
+    if (cols) {
+        const dim3 grid((unsigned)((h3 + RC_KB - 1) / RC_KB), (unsigned)(3 * d.n1));
+        const int smem = (int)(d.n2 * RC_KB * (2 * sizeof(float2) + sizeof(float)));
+        k_ramp_cols<<<grid, RC_WARPS * 32, smem, s>>>(spec.p, filt.p, (int)d.n2, (int)h3);
+        LAMINO_LAUNCH("k_ramp_cols");
+    } else {
+        k_filter_mul<<<grid_for(3 * d.n1 * plane, 256), 256, 0, s>>>(spec.p, filt.p, plane, 3 * d.n1 * plane);
+        LAMINO_LAUNCH("k_filter_mul");
+    }
     LAMINO_CUFFT(cufftExecC2R(c2r.h, (cufftComplex *)spec.p, z3));
 }
 

@@ -49,7 +49,8 @@ struct RampPrecond {
     Dims3 d;
     FftPlan r2c, c2r;
     DevBuf<float2> spec;
-    DevBuf<float> filt;
+    DevBuf<float> filt;  // the filter (2-D path) or the n2 convolution kernels (column path)
+    bool cols = false;   // 1-D transforms along n3 and a circulant convolution along n2
     explicit RampPrecond(Dims3 d);
     void apply3(const float *r3, float *z3, cudaStream_t s);  // all 3 components
 };

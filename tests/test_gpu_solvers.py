@@ -36,9 +36,11 @@ def test_demag_vs_oracle(L, O, dims):
     assert rel(L.opt.demag(h), -want) < 1e-5
 
 
-def test_ramp_preconditioner_vs_oracle(L, O):
+@pytest.mark.parametrize("dims", [(5, 9, 12), (3, 71, 721), (2, 130, 6)])
+def test_ramp_preconditioner_vs_oracle(L, O, dims):
+    """Both forms: n2 <= 128 runs 1-D transforms along n3 and a circulant
+    convolution along n2 (the first two cases), larger n2 the 2-D transforms."""
     rng = np.random.default_rng(1)
-    dims = (5, 9, 12)
     r = rng.standard_normal((3,) + dims).astype(np.float32)
     M = O.RampPreconditioner(dims)
     want = np.stack([M.apply(r[i]) for i in range(3)])
