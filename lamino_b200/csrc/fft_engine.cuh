@@ -347,6 +347,76 @@ __device__ __forceinline__ void ct_inverse(float2 *data, int P, int ps, const fl
     }
 }
 
+// Transforms of length 1458 (schedule 2, 9, 9, 9) whose input is zero from 729 on
+// and of which only outputs below 729 are kept: the zero-padded radix-2 stage and
+// the first radix-9 stage (two blocks of 729, 81 offsets each) run in registers
+// between the caller's loads and shared memory, and their inverses between
+// shared memory and the caller's stores, two round trips through shared memory
+// fewer each way.  Thread (c, n) of 3 x 81 handles values n + 81 j of row c of
+// sm (rows 1458 apart); rows.get(c, i) gives input i (zero past the data),
+// rows.want(i) / rows.put(c, i, v) take output i.  tw: the 1458-point table.
+constexpr int F1458_OFS = 81;
+
+template <class Rows>
+__device__ __forceinline__ void fft1458_load(const Rows &rows, const float2 *__restrict__ tw,
+                                             float2 *__restrict__ sm, int tid) {
+    if (tid >= 3 * F1458_OFS) return;
+    const int c = tid / F1458_OFS, n = tid - c * F1458_OFS;
+    float2 x[9], u[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) x[j] = rows.get(c, n + F1458_OFS * j);
+    // radix-2 stage over the zero-padded half: block 0 = x, block 1 = x w^i
+#pragma unroll
+    for (int j = 0; j < 9; ++j) u[j] = c_mul(x[j], __ldg(tw + n + F1458_OFS * j));
+    dft_small<9, false>(x);
+    dft_small<9, false>(u);
+    if (n != 0) {
+        float2 w[9];
+        twiddle_powers<9>(tw, 2 * n, w);
+#pragma unroll
+        for (int k = 1; k < 9; ++k) {
+            x[k] = c_mul(x[k], w[k]);
+            u[k] = c_mul(u[k], w[k]);
+        }
+    }
+    float2 *s = sm + c * 1458 + n;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        s[F1458_OFS * k] = x[k];
+        s[729 + F1458_OFS * k] = u[k];
+    }
+}
+
+template <class Rows>
+__device__ __forceinline__ void fft1458_store(const Rows &rows, const float2 *__restrict__ tw,
+                                              const float2 *__restrict__ sm, int tid) {
+    if (tid >= 3 * F1458_OFS) return;
+    const int c = tid / F1458_OFS, n = tid - c * F1458_OFS;
+    const float2 *s = sm + c * 1458 + n;
+    float2 a[9], b[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        a[k] = s[F1458_OFS * k];
+        b[k] = s[729 + F1458_OFS * k];
+    }
+    if (n != 0) {
+        float2 w[9];
+        twiddle_powers<9>(tw, 2 * n, w);
+#pragma unroll
+        for (int k = 1; k < 9; ++k) {
+            a[k] = c_mulc(a[k], w[k]);
+            b[k] = c_mulc(b[k], w[k]);
+        }
+    }
+    dft_small<9, true>(a);
+    dft_small<9, true>(b);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+        const int i = n + F1458_OFS * j;
+        if (rows.want(i)) rows.put(c, i, c_add(a[j], c_mulc(b[j], __ldg(tw + i))));
+    }
+}
+
 // Forward / inverse with a compile-time schedule when N != 0, else the runtime one.
 template <int N, int S_BEGIN>
 __device__ __forceinline__ void fft_fwd_any(float2 *data, int P, int ps, const FftLen &F, int tid, int nth) {

@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "fft_engine.cuh"
 #include "solvers.cuh"
 
 namespace lamino {
@@ -455,6 +456,169 @@ __global__ void __launch_bounds__(RC_WARPS * 32) k_ramp_cols(float2 *__restrict_
     }
 }
 
+// Real transforms along n3 = N (365 <= N <= 729) as Bluestein convolutions through
+// the 1458-point pipeline: X[k] = sum_n x[n] e^{-2 pi i k n / N}
+// = conj(w_k) sum_n (x_n conj(w_n)) w_{k-n} with w_m = e^{i pi m^2 / N}, a circular
+// convolution of length M = 1458 >= 2N - 1, taken as undo(FWD(u) . V) with V the
+// transform of v (v_m = w_m for m < N, v_{M-m} = w_m for 0 < m < N, zero between),
+// divided by M and stored in DIF position order.  The inverse uses conj(w) in
+// place of w.  Two real rows travel as one complex row (a + i b), three complex
+// rows per CTA; the spectra keep the R2C layout [row][N/2 + 1].
+constexpr int kBlueM = 1458;
+constexpr int kBlueHalf = 729;
+
+struct BlueR2CRows {
+    const float *x;
+    int64_t nrows, q0;
+    int N;
+    const float2 *chirp;
+    float2 *zb;  // 3 x 729 results in shared memory
+    __device__ __forceinline__ float2 get(int c, int i) const {
+        const int64_t r = 2 * (q0 + c);
+        if (i >= N || r >= nrows) return make_float2(0.f, 0.f);
+        const float a = x[r * N + i], b = r + 1 < nrows ? x[(r + 1) * N + i] : 0.f;
+        return c_mulc(make_float2(a, b), __ldg(chirp + i));
+    }
+    __device__ __forceinline__ bool want(int i) const { return i < N; }
+    __device__ __forceinline__ void put(int c, int i, float2 v) const {
+        zb[c * kBlueHalf + i] = c_mulc(v, __ldg(chirp + i));
+    }
+};
+
+__global__ void __launch_bounds__(256, 4) k_blue_r2c(const float *__restrict__ x, int64_t nrows, int N,
+                                                     const float2 *__restrict__ chirp,
+                                                     const float2 *__restrict__ V,
+                                                     const float2 *__restrict__ tw, float2 *__restrict__ S) {
+    extern __shared__ float2 sm[];  // 3 transform rows of 1458, then 3 x 729 results
+    const int h = N / 2 + 1;
+    const int64_t q0 = (int64_t)blockIdx.x * 3;
+    const BlueR2CRows rows{x, nrows, q0, N, chirp, sm + 3 * kBlueM};
+    fft1458_load(rows, tw, sm, threadIdx.x);
+    __syncthreads();
+    ct_forward<kBlueM, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+    for (int p = threadIdx.x; p < kBlueM; p += blockDim.x) {
+        const float2 v = __ldg(V + p);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sm[c * kBlueM + p] = c_mul(sm[c * kBlueM + p], v);
+    }
+    __syncthreads();
+    ct_inverse<kBlueM, 3, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+    fft1458_store(rows, tw, sm, threadIdx.x);
+    __syncthreads();
+    // A = (Z_k + conj Z_{N-k}) / 2, B = (Z_k - conj Z_{N-k}) / 2i
+    const float2 *zb = sm + 3 * kBlueM;
+    for (int t = threadIdx.x; t < 3 * h; t += blockDim.x) {
+        const int c = t / h, k = t - c * h;
+        const int64_t r = 2 * (q0 + c);
+        if (r >= nrows) continue;
+        const float2 zk = zb[c * kBlueHalf + k];
+        const float2 zm = zb[c * kBlueHalf + (k == 0 ? 0 : N - k)];
+        S[r * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        if (r + 1 < nrows) S[(r + 1) * h + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+}
+
+struct BlueC2RRows {
+    const float2 *S;
+    float *y;
+    int64_t nrows, q0;
+    int N, h;
+    const float2 *chirp;
+    __device__ __forceinline__ float2 get(int c, int i) const {
+        const int64_t r = 2 * (q0 + c);
+        if (i >= N || r >= nrows) return make_float2(0.f, 0.f);
+        const bool lo = i < h;
+        const int k = lo ? i : N - i;
+        float2 A = S[r * h + k];
+        float2 B = r + 1 < nrows ? S[(r + 1) * h + k] : make_float2(0.f, 0.f);
+        if (k == 0 || 2 * k == N) A.y = B.y = 0.f;  // as a C2R reads them: real
+        if (!lo) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        return c_mul(make_float2(A.x - B.y, A.y + B.x), __ldg(chirp + i));  // (A + i B) w
+    }
+    __device__ __forceinline__ bool want(int i) const { return i < N; }
+    __device__ __forceinline__ void put(int c, int i, float2 v) const {
+        const int64_t r = 2 * (q0 + c);
+        if (r >= nrows) return;
+        const float2 z = c_mul(v, __ldg(chirp + i));
+        y[r * N + i] = z.x;
+        if (r + 1 < nrows) y[(r + 1) * N + i] = z.y;
+    }
+};
+
+__global__ void __launch_bounds__(256, 5) k_blue_c2r(const float2 *__restrict__ S, int64_t nrows, int N,
+                                                     const float2 *__restrict__ chirp,
+                                                     const float2 *__restrict__ V,
+                                                     const float2 *__restrict__ tw, float *__restrict__ y) {
+    extern __shared__ float2 sm[];  // 3 transform rows of 1458
+    const BlueC2RRows rows{S, y, nrows, (int64_t)blockIdx.x * 3, N, N / 2 + 1, chirp};
+    fft1458_load(rows, tw, sm, threadIdx.x);
+    __syncthreads();
+    ct_forward<kBlueM, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+    for (int p = threadIdx.x; p < kBlueM; p += blockDim.x) {
+        const float2 v = __ldg(V + p);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sm[c * kBlueM + p] = c_mul(sm[c * kBlueM + p], v);
+    }
+    __syncthreads();
+    ct_inverse<kBlueM, 3, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+    fft1458_store(rows, tw, sm, threadIdx.x);
+}
+
+// chirp w_n = e^{i pi n^2 / N}, the convolution kernels' spectra in DIF position
+// order (forward: v; inverse: conj v; both / M) and the 1458-point twiddles, in FP64
+static void blue_tables(int N, std::vector<float2> &chirp, std::vector<float2> &vf, std::vector<float2> &vi,
+                        std::vector<float2> &tw) {
+    const int M = kBlueM;
+    std::vector<double> wc(N), ws(N);
+    for (int64_t n = 0; n < N; ++n) {
+        const double a = M_PI * (double)((n * n) % (2 * (int64_t)N)) / (double)N;
+        wc[n] = std::cos(a);
+        ws[n] = std::sin(a);
+    }
+    chirp.resize(N);
+    for (int n = 0; n < N; ++n) chirp[n] = make_float2((float)wc[n], (float)ws[n]);
+    std::vector<double> vr(M, 0.0), vim(M, 0.0);
+    for (int m = 0; m < N; ++m) {
+        vr[m] = wc[m];
+        vim[m] = ws[m];
+        if (m > 0) {
+            vr[M - m] = wc[m];
+            vim[M - m] = ws[m];
+        }
+    }
+    std::vector<double> cs(M), sn(M);
+    for (int e = 0; e < M; ++e) {
+        cs[e] = std::cos(-2.0 * M_PI * e / M);
+        sn[e] = std::sin(-2.0 * M_PI * e / M);
+    }
+    const std::vector<int> pos = fft_positions(M, fft_schedule(M, true));
+    vf.assign(M, make_float2(0.f, 0.f));
+    vi.assign(M, make_float2(0.f, 0.f));
+    std::vector<double> Fr(M), Fi(M);
+    for (int k = 0; k < M; ++k) {
+        double re = 0.0, im = 0.0;
+        for (int m = 0; m < M; ++m) {
+            if (vr[m] == 0.0 && vim[m] == 0.0) continue;
+            const int e = (int)(((int64_t)k * m) % M);
+            re += vr[m] * cs[e] - vim[m] * sn[e];
+            im += vr[m] * sn[e] + vim[m] * cs[e];
+        }
+        Fr[k] = re;
+        Fi[k] = im;
+    }
+    for (int k = 0; k < M; ++k) {
+        // transform of conj v at k = conj(transform of v at -k)
+        const int km = (M - k) % M;
+        vf[pos[k]] = make_float2((float)(Fr[k] / M), (float)(Fi[k] / M));
+        vi[pos[k]] = make_float2((float)(Fr[km] / M), (float)(-Fi[km] / M));
+    }
+    tw.resize(M);
+    for (int e = 0; e < M; ++e) tw[e] = make_float2((float)cs[e], (float)sn[e]);
+}
+
 RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
     int64_t n2 = d.n2, n3 = d.n3, h3 = n3 / 2 + 1;
     std::vector<float> xf(h3), yf(n2), f(n2 * h3);
@@ -479,9 +643,25 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
             }
         filt.alloc(n2 * h3);
         upload(filt.p, g.data(), g.size());
-        int n[1] = {(int)n3};
-        r2c.make(1, n, CUFFT_R2C, (int)(3 * d.n1 * n2));
-        c2r.make(1, n, CUFFT_C2R, (int)(3 * d.n1 * n2));
+        blue = n3 >= 365 && n3 <= kBlueHalf;
+        if (blue) {
+            std::vector<float2> hc, hvf, hvi, htw;
+            blue_tables((int)n3, hc, hvf, hvi, htw);
+            chirp.alloc(hc.size());
+            upload(chirp.p, hc.data(), hc.size());
+            vfwd.alloc(hvf.size());
+            upload(vfwd.p, hvf.data(), hvf.size());
+            vinv.alloc(hvi.size());
+            upload(vinv.p, hvi.data(), hvi.size());
+            tw.alloc(htw.size());
+            upload(tw.p, htw.data(), htw.size());
+            raise_smem_limit((const void *)k_blue_r2c, (int)(3 * (kBlueM + kBlueHalf) * sizeof(float2)));
+            raise_smem_limit((const void *)k_blue_c2r, (int)(3 * kBlueM * sizeof(float2)));
+        } else {
+            int n[1] = {(int)n3};
+            r2c.make(1, n, CUFFT_R2C, (int)(3 * d.n1 * n2));
+            c2r.make(1, n, CUFFT_C2R, (int)(3 * d.n1 * n2));
+        }
         raise_smem_limit((const void *)k_ramp_cols, (int)(n2 * RC_KB * (2 * sizeof(float2) + sizeof(float))));
     } else {
         filt.alloc(n2 * h3);
@@ -494,9 +674,16 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
 
 void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
     int64_t h3 = d.n3 / 2 + 1, plane = d.n2 * h3;
-    LAMINO_CUFFT(cufftSetStream(r2c.h, s));
-    LAMINO_CUFFT(cufftSetStream(c2r.h, s));
-    LAMINO_CUFFT(cufftExecR2C(r2c.h, const_cast<float *>(r3), (cufftComplex *)spec.p));
+    const int64_t nrows = 3 * d.n1 * d.n2;
+    const unsigned gblue = (unsigned)(((nrows + 1) / 2 + 2) / 3);
+    if (blue) {
+        k_blue_r2c<<<gblue, 256, 3 * (kBlueM + kBlueHalf) * sizeof(float2), s>>>(
+            r3, nrows, (int)d.n3, chirp.p, vfwd.p, tw.p, spec.p);
+        LAMINO_LAUNCH("k_blue_r2c");
+    } else {
+        LAMINO_CUFFT(cufftSetStream(r2c.h, s));
+        LAMINO_CUFFT(cufftExecR2C(r2c.h, const_cast<float *>(r3), (cufftComplex *)spec.p));
+    }
     if (cols) {
         const dim3 grid((unsigned)((h3 + RC_KB - 1) / RC_KB), (unsigned)(3 * d.n1));
         const int smem = (int)(d.n2 * RC_KB * (2 * sizeof(float2) + sizeof(float)));
@@ -506,7 +693,14 @@ void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
         k_filter_mul<<<grid_for(3 * d.n1 * plane, 256), 256, 0, s>>>(spec.p, filt.p, plane, 3 * d.n1 * plane);
         LAMINO_LAUNCH("k_filter_mul");
     }
-    LAMINO_CUFFT(cufftExecC2R(c2r.h, (cufftComplex *)spec.p, z3));
+    if (blue) {
+        k_blue_c2r<<<gblue, 256, 3 * kBlueM * sizeof(float2), s>>>(spec.p, nrows, (int)d.n3, chirp.p, vinv.p,
+                                                                   tw.p, z3);
+        LAMINO_LAUNCH("k_blue_c2r");
+    } else {
+        LAMINO_CUFFT(cufftSetStream(c2r.h, s));
+        LAMINO_CUFFT(cufftExecC2R(c2r.h, (cufftComplex *)spec.p, z3));
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -51,6 +51,8 @@ struct RampPrecond {
     DevBuf<float2> spec;
     DevBuf<float> filt;  // the filter (2-D path) or the n2 convolution kernels (column path)
     bool cols = false;   // 1-D transforms along n3 and a circulant convolution along n2
+    bool blue = false;   // (with cols) the n3 transforms as Bluestein convolutions of 1458
+    DevBuf<float2> chirp, vfwd, vinv, tw;  // Bluestein tables: chirp, kernel spectra, twiddles
     explicit RampPrecond(Dims3 d);
     void apply3(const float *r3, float *z3, cudaStream_t s);  // all 3 components
 };

@@ -435,74 +435,18 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
     }
 }
 
-// Pencils of L1 = 1458 (schedule 2, 9, 9, 9): the zero-padded radix-2 stage and
-// the first radix-9 stage (two blocks of 729, 81 offsets each) run in registers
-// between global memory and shared memory, and so do their inverses in the store:
-// two round trips of the pencil through shared memory fewer each way.  Thread
-// (c, n) of 3 x 81 holds the 9 input values n + 81 j of component c.
-constexpr int P1458_OFS = 81;
-
-__device__ __forceinline__ void pencil1458_load(const float2 *__restrict__ pv, int64_t cs, int n1,
-                                                const float2 *__restrict__ tw1, float2 *__restrict__ sm, int tid) {
-    if (tid >= 3 * P1458_OFS) return;
-    const int c = tid / P1458_OFS, n = tid - c * P1458_OFS;
-    float2 x[9], u[9];
-#pragma unroll
-    for (int j = 0; j < 9; ++j) {
-        const int i = n + P1458_OFS * j;
-        x[j] = i < n1 ? pv[c * cs + i] : make_float2(0.f, 0.f);
+// Pencil rows for fft1458_load / fft1458_store: component c of the pencil at pv,
+// n1 values, components cs apart.
+struct PencilRows {
+    float2 *pv;
+    int64_t cs;
+    int n1;
+    __device__ __forceinline__ float2 get(int c, int i) const {
+        return i < n1 ? pv[c * cs + i] : make_float2(0.f, 0.f);
     }
-    // radix-2 stage over the zero-padded half: block 0 = x, block 1 = x w^i
-#pragma unroll
-    for (int j = 0; j < 9; ++j) u[j] = c_mul(x[j], __ldg(tw1 + n + P1458_OFS * j));
-    dft_small<9, false>(x);
-    dft_small<9, false>(u);
-    if (n != 0) {
-        float2 w[9];
-        twiddle_powers<9>(tw1, 2 * n, w);
-#pragma unroll
-        for (int k = 1; k < 9; ++k) {
-            x[k] = c_mul(x[k], w[k]);
-            u[k] = c_mul(u[k], w[k]);
-        }
-    }
-    float2 *s = sm + c * 1458 + n;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        s[P1458_OFS * k] = x[k];
-        s[729 + P1458_OFS * k] = u[k];
-    }
-}
-
-__device__ __forceinline__ void pencil1458_store(float2 *__restrict__ pv, int64_t cs, int n1,
-                                                 const float2 *__restrict__ tw1, const float2 *__restrict__ sm,
-                                                 int tid) {
-    if (tid >= 3 * P1458_OFS) return;
-    const int c = tid / P1458_OFS, n = tid - c * P1458_OFS;
-    const float2 *s = sm + c * 1458 + n;
-    float2 a[9], b[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        a[k] = s[P1458_OFS * k];
-        b[k] = s[729 + P1458_OFS * k];
-    }
-    if (n != 0) {
-        float2 w[9];
-        twiddle_powers<9>(tw1, 2 * n, w);
-#pragma unroll
-        for (int k = 1; k < 9; ++k) {
-            a[k] = c_mulc(a[k], w[k]);
-            b[k] = c_mulc(b[k], w[k]);
-        }
-    }
-    dft_small<9, true>(a);
-    dft_small<9, true>(b);
-#pragma unroll
-    for (int j = 0; j < 9; ++j) {
-        const int i = n + P1458_OFS * j;
-        if (i < n1) pv[c * cs + i] = c_add(a[j], c_mulc(b[j], __ldg(tw1 + i)));
-    }
-}
+    __device__ __forceinline__ bool want(int i) const { return i < n1; }
+    __device__ __forceinline__ void put(int c, int i, float2 v) const { pv[c * cs + i] = v; }
+};
 
 // B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
 // symmetric multiply with the spectra (same position order), undo, first n1 kept.
@@ -519,7 +463,7 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
     const int64_t cs = (int64_t)L2 * L3h * n1p;  // component stride in xa
     float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
-        pencil1458_load(pv, cs, n1, tw1, sm, threadIdx.x);
+        fft1458_load(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
         __syncthreads();
         ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
     } else {
@@ -591,7 +535,7 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
     __syncthreads();
     if constexpr (N1 == 1458) {
         ct_inverse<1458, 3, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
-        pencil1458_store(pv, cs, n1, tw1, sm, threadIdx.x);
+        fft1458_store(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
     } else {
         fft_inv_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
         for (int t = threadIdx.x; t < 3 * n1; t += blockDim.x) {
@@ -622,7 +566,7 @@ __global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ 
     const int64_t cs = (int64_t)L2 * L3h * n1p;
     const float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
-        pencil1458_load(pv, cs, n1, tw1, sm, threadIdx.x);
+        fft1458_load(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm, threadIdx.x);  // reads only
         __syncthreads();
         ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
     } else {
