@@ -285,19 +285,49 @@ __global__ void __launch_bounds__(kVoxX) k_divergence(const float *__restrict__ 
     for (int i = pr.z0; i < pr.z1; ++i) out[((int64_t)i * n2 + j) * n3 + k] = neg_div(f, i, j, k, n1, n2, n3);
 }
 
-// y += mu * divergence(grad_u(u)) for NC contiguous components
+// y += mu * divergence(grad_u(u)) for the 3 contiguous components.  The stencil
+// reaches the centre and +-2 along each axis; a thread marches along i through a
+// run of planes of one component (blockIdx.z = comp * runs + run) with
+// u[i-2 .. i+2] of its (j, k) column in registers, so each voxel loads u[i+3]
+// and the j and k neighbours only.  Same arithmetic as gdir / neg_div: float
+// differences halved in float, combined in double.
 __global__ void __launch_bounds__(kVoxX) k_laplacian_axpy(float *__restrict__ y, float mu, const float *__restrict__ u,
                                                           int n1, int n2, int n3) {
     const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
     if (k >= n3) return;
-    const int64_t V = (int64_t)n1 * n2 * n3;
-    const PlaneRun pr(3 * n1);
-    for (int z = pr.z0; z < pr.z1; ++z) {
-        const int comp = z / n1, i = z - comp * n1;
-        const float *uc = u + comp * V;
-        auto f = [&](int dim, int ii, int jj, int kk) { return gdir(uc, ii, jj, kk, n1, n2, n3, dim); };
-        const float l = neg_div(f, i, j, k, n1, n2, n3);
-        y[comp * V + ((int64_t)i * n2 + j) * n3 + k] += l * mu;
+    const int runs = (int)gridDim.z / 3;
+    const int comp = (int)blockIdx.z / runs, run = (int)blockIdx.z - comp * runs;
+    const int per = (n1 + runs - 1) / runs;
+    const int i0 = run * per, i1 = min(n1, i0 + per);
+    if (i0 >= i1) return;
+    const int64_t V = (int64_t)n1 * n2 * n3, s1 = (int64_t)n2 * n3;
+    const bool jk_in = j >= 1 && j <= n2 - 2 && k >= 1 && k <= n3 - 2;
+    const int64_t col = (int64_t)j * n3 + k;
+    const float *uc = u + comp * V + col;
+    float *yc = y + comp * V + col;
+    auto ld = [&](int ii) { return (ii >= 0 && ii < n1) ? uc[ii * s1] : 0.f; };
+    float w0 = ld(i0 - 2), w1 = ld(i0 - 1), w2 = ld(i0), w3 = ld(i0 + 1), w4 = ld(i0 + 2);
+    for (int i = i0; i < i1; ++i) {
+        float l = 0.f;
+        if (jk_in && i >= 1 && i <= n1 - 2) {
+            const float *pc = uc + (int64_t)i * s1;
+            const float g0p = i + 1 <= n1 - 2 ? (w4 - w2) * 0.5f : 0.f;
+            const float g0m = i - 1 >= 1 ? (w2 - w0) * 0.5f : 0.f;
+            const float g1p = j + 1 <= n2 - 2 ? (pc[2 * n3] - w2) * 0.5f : 0.f;
+            const float g1m = j - 1 >= 1 ? (w2 - pc[-2 * n3]) * 0.5f : 0.f;
+            const float g2p = k + 1 <= n3 - 2 ? (pc[2] - w2) * 0.5f : 0.f;
+            const float g2m = k - 1 >= 1 ? (w2 - pc[-2]) * 0.5f : 0.f;
+            const double a = -(double)(g0p - g0m) / 2.0;
+            const double b = (double)(g1p - g1m) / 2.0;
+            const double c = (double)(g2p - g2m) / 2.0;
+            l = (float)(a - b - c);
+        }
+        yc[(int64_t)i * s1] += l * mu;
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
+        w3 = w4;
+        w4 = ld(i + 3);
     }
 }
 
@@ -363,7 +393,9 @@ void divergence(const float *du3, Dims3 d, float *out, cudaStream_t s) {
     LAMINO_LAUNCH("k_divergence");
 }
 void laplacian_axpy(float *y, float mu, const float *u, Dims3 d, cudaStream_t s) {
-    k_laplacian_axpy<<<vox_grid(d, 3), kVoxX, 0, s>>>(y, mu, u, (int)d.n1, (int)d.n2, (int)d.n3);
+    dim3 g = vox_grid(d, 1);  // runs of planes per component, 3 components
+    g.z = (unsigned)std::max<int64_t>(1, std::min<int64_t>(g.z, 65535 / 3)) * 3;
+    k_laplacian_axpy<<<g, kVoxX, 0, s>>>(y, mu, u, (int)d.n1, (int)d.n2, (int)d.n3);
     LAMINO_LAUNCH("k_laplacian_axpy");
 }
 void sb_rhs(const float *yT3, const float *d9, const float *b9, float mu, Dims3 dims, float *rhs3, cudaStream_t s) {

@@ -14,6 +14,14 @@ def test_qggmrf_vs_reference(L, gold_ref):
     assert rel(g, gold_ref["qg_g"]) < 1e-6
 
 
+def test_laplacian_plane_runs(L, O):
+    """A volume large enough that each thread of the Laplacian marches through
+    runs of several planes (sizes of the 51x511x511 case's padded n2, n3)."""
+    rng = np.random.default_rng(21)
+    u = rng.standard_normal((20, 71, 721)).astype(np.float32)
+    assert np.allclose(L.opt.laplacian(u), O.laplacian(u.astype(np.float64)), rtol=0, atol=2e-6)
+
+
 def test_finite_differences_vs_reference(L, gold_ref):
     assert np.allclose(L.opt.grad_u(gold_ref["fd_u"]), gold_ref["fd_grad"], rtol=0, atol=1e-6)
     assert np.allclose(L.opt.divergence(gold_ref["fd_du"]), gold_ref["fd_div"], rtol=0, atol=1e-6)
