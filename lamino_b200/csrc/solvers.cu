@@ -465,19 +465,31 @@ __global__ void __launch_bounds__(RC_WARPS * 32) k_ramp_cols(float2 *__restrict_
         }
     }
     __syncthreads();
+    // rows m0 .. m0 + 8 of a thread need x[m0 + r - dd]: as dd grows the window
+    // shifts by one, so it lives in a rotating register buffer, slot (r - dd) mod 9,
+    // and each tap loads one new x (smem tile index m - dd + n2 stays in [1, 2 n2))
     for (int m0 = warp * RC_ROWS; m0 < n2; m0 += RC_ROWS * RC_WARPS) {
-        float2 acc[RC_ROWS];
+        float2 acc[RC_ROWS], buf[RC_ROWS];
 #pragma unroll
-        for (int r = 0; r < RC_ROWS; ++r) acc[r] = make_float2(0.f, 0.f);
-        for (int dd = 0; dd < n2; ++dd) {
-            const float g = gs[dd * RC_KB + lane];
-            const float2 *xr = xs + (m0 - dd + n2) * RC_KB + lane;
+        for (int r = 0; r < RC_ROWS; ++r) {
+            acc[r] = make_float2(0.f, 0.f);
+            // rows past n2 - 1 start from row n2 - 1 (inside the tile) and are never stored
+            buf[r] = xs[(min(m0 + r, n2 - 1) + n2) * RC_KB + lane];
+        }
+        for (int d0 = 0; d0 < n2; d0 += RC_ROWS) {
 #pragma unroll
-            for (int r = 0; r < RC_ROWS; ++r) {
-                // rows past n2 - 1 re-read row n2 - 1 (inside the tile) and are never stored
-                const float2 x = xr[min(r, n2 - 1 - m0) * RC_KB];
-                acc[r].x = fmaf(g, x.x, acc[r].x);
-                acc[r].y = fmaf(g, x.y, acc[r].y);
+            for (int u = 0; u < RC_ROWS; ++u) {
+                const int dd = d0 + u;
+                if (dd < n2) {
+                    if (dd > 0) buf[(RC_ROWS - u) % RC_ROWS] = xs[(m0 - dd + n2) * RC_KB + lane];
+                    const float g = gs[dd * RC_KB + lane];
+#pragma unroll
+                    for (int r = 0; r < RC_ROWS; ++r) {
+                        const float2 x = buf[(r - u + RC_ROWS) % RC_ROWS];
+                        acc[r].x = fmaf(g, x.x, acc[r].x);
+                        acc[r].y = fmaf(g, x.y, acc[r].y);
+                    }
+                }
             }
         }
 #pragma unroll
