@@ -44,12 +44,12 @@ def test_demag_vs_oracle(L, O, dims):
     assert rel(L.opt.demag(h), -want) < 1e-5
 
 
-@pytest.mark.parametrize("dims", [(5, 9, 12), (3, 71, 721), (3, 5, 400), (1, 3, 365), (2, 130, 6)])
+@pytest.mark.parametrize("dims", [(5, 9, 12), (3, 71, 721), (3, 5, 400), (1, 3, 365), (2, 128, 400), (2, 130, 6)])
 def test_ramp_preconditioner_vs_oracle(L, O, dims):
     """Every form: n2 <= 128 runs 1-D transforms along n3 and a circulant
     convolution along n2, the n3 transforms as Bluestein convolutions of 1458
-    when 365 <= n3 <= 729 (odd and even n3, an odd number of rows), larger n2
-    the 2-D transforms."""
+    when 365 <= n3 <= 729 (odd and even n3, an odd number of rows; n2 = 128 takes
+    the column kernel's second pass over rows), larger n2 the 2-D transforms."""
     rng = np.random.default_rng(1)
     r = rng.standard_normal((3,) + dims).astype(np.float32)
     M = O.RampPreconditioner(dims)
