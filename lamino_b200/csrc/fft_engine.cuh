@@ -14,6 +14,7 @@
 // last undo stage (outputs < n/2 only) into the store.
 #pragma once
 
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -22,10 +23,29 @@ namespace lamino {
 
 constexpr int FFT_MAX_STAGES = 16;
 
+// Division of 0 <= x < 2^31 by a runtime d >= 1 as a multiply-high, an add and a
+// shift: q = (umulhi(x, mul) + x) >> sh, sh = ceil(log2 d),
+// mul = floor(2^32 (2^sh - d) / d) + 1 (the round-up method).
+struct FastDiv {
+    uint32_t mul = 1, sh = 0;
+    static FastDiv make(uint32_t d) {
+        FastDiv f;
+        while ((1ull << f.sh) < d) ++f.sh;
+        f.mul = (uint32_t)((((1ull << 32) * ((1ull << f.sh) - d)) / d) + 1);
+        return f;
+    }
+    __device__ __forceinline__ int div(int x) const {
+        return (int)((__umulhi((uint32_t)x, mul) + (uint32_t)x) >> sh);
+    }
+};
+
 struct FftLen {  // POD, passed by value to kernels
     int n, ns;
     int radix[FFT_MAX_STAGES];
     int bsz[FFT_MAX_STAGES];
+    // per stage: division by the offsets per block (B / R), the butterflies per
+    // pencil (n / R) and the blocks per pencil (n / B)
+    FastDiv dm[FFT_MAX_STAGES], dnb[FFT_MAX_STAGES], dblk[FFT_MAX_STAGES];
     const float2 *tw;  // exp(-2 pi i e / n), e in [0, n)
 };
 
@@ -173,19 +193,32 @@ __device__ __forceinline__ void dft_small(float2 (&v)[R]) {
     }
 }
 
-// One stage over P pencils of length n (pencil stride ps) in shared memory.
+// One stage over P pencils of length n (pencil stride ps) in shared memory, the
+// runtime-length counterpart of fft_stage_fixed: the butterfly index is split with
+// multiply-high divisions, the twiddles come from two table loads and products,
+// and with fewer than 16 offsets per odd-sized block the blocks run fastest (lanes
+// B apart, distinct banks).
 template <int R, bool INV>
 __device__ __forceinline__ void fft_stage(float2 *__restrict__ data, int P, int ps, int n, int B,
-                                          const float2 *__restrict__ tw, int tid, int nth) {
+                                          const float2 *__restrict__ tw, FastDiv dm, FastDiv dnb, FastDiv dblk,
+                                          int tid, int nth) {
     const int m = B / R;
     const int nb = n / R;
     const int ts = n / B;
+    const int nblk = ts;
+    const bool b_fast = (m > 1) && (m < 16) && (B & 1);
     const int total = P * nb;
     for (int t = tid; t < total; t += nth) {
-        int pen = t / nb;
-        int u = t - pen * nb;
-        int b = u / m;
-        int n1 = u - b * m;
+        const int pen = dnb.div(t);
+        const int u = t - pen * nb;
+        int b, n1;
+        if (b_fast) {
+            n1 = dblk.div(u);
+            b = u - n1 * nblk;
+        } else {
+            b = dm.div(u);
+            n1 = u - b * m;
+        }
         float2 *base = data + pen * ps + b * B + n1;
         float2 v[R];
         if constexpr (!INV) {
@@ -193,8 +226,10 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ data, int P, int 
             for (int j = 0; j < R; ++j) v[j] = base[m * j];
             dft_small<R, false>(v);
             if (n1 != 0) {
+                float2 w[R];
+                twiddle_powers<R>(tw, n1 * ts, w);
 #pragma unroll
-                for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], __ldg(tw + n1 * k * ts));
+                for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], w[k]);
             }
 #pragma unroll
             for (int k = 0; k < R; ++k) base[m * k] = v[k];
@@ -202,8 +237,10 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ data, int P, int 
 #pragma unroll
             for (int k = 0; k < R; ++k) v[k] = base[m * k];
             if (n1 != 0) {
+                float2 w[R];
+                twiddle_powers<R>(tw, n1 * ts, w);
 #pragma unroll
-                for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], __ldg(tw + n1 * k * ts));
+                for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], w[k]);
             }
             dft_small<R, true>(v);
 #pragma unroll
@@ -213,15 +250,17 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ data, int P, int 
 }
 
 template <bool INV>
-__device__ __forceinline__ void fft_stage_rt(int r, float2 *data, int P, int ps, int n, int B, const float2 *tw,
-                                             int tid, int nth) {
-    switch (r) {
-        case 2: fft_stage<2, INV>(data, P, ps, n, B, tw, tid, nth); break;
-        case 3: fft_stage<3, INV>(data, P, ps, n, B, tw, tid, nth); break;
-        case 4: fft_stage<4, INV>(data, P, ps, n, B, tw, tid, nth); break;
-        case 5: fft_stage<5, INV>(data, P, ps, n, B, tw, tid, nth); break;
-        case 8: fft_stage<8, INV>(data, P, ps, n, B, tw, tid, nth); break;
-        default: fft_stage<9, INV>(data, P, ps, n, B, tw, tid, nth); break;
+__device__ __forceinline__ void fft_stage_rt(const FftLen &F, int s, float2 *data, int P, int ps, int tid,
+                                             int nth) {
+    const int n = F.n, B = F.bsz[s];
+    const FastDiv dm = F.dm[s], dnb = F.dnb[s], dblk = F.dblk[s];
+    switch (F.radix[s]) {
+        case 2: fft_stage<2, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
+        case 3: fft_stage<3, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
+        case 4: fft_stage<4, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
+        case 5: fft_stage<5, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
+        case 8: fft_stage<8, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
+        default: fft_stage<9, INV>(data, P, ps, n, B, F.tw, dm, dnb, dblk, tid, nth); break;
     }
 }
 
@@ -229,7 +268,7 @@ __device__ __forceinline__ void fft_stage_rt(int r, float2 *data, int P, int ps,
 __device__ __forceinline__ void fft_forward(float2 *data, int P, int ps, const FftLen &F, int s_begin, int tid,
                                             int nth) {
     for (int s = s_begin; s < F.ns; ++s) {
-        fft_stage_rt<false>(F.radix[s], data, P, ps, F.n, F.bsz[s], F.tw, tid, nth);
+        fft_stage_rt<false>(F, s, data, P, ps, tid, nth);
         __syncthreads();
     }
 }
@@ -238,7 +277,7 @@ __device__ __forceinline__ void fft_forward(float2 *data, int P, int ps, const F
 __device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const FftLen &F, int s_end, int tid,
                                             int nth) {
     for (int s = F.ns - 1; s >= s_end; --s) {
-        fft_stage_rt<true>(F.radix[s], data, P, ps, F.n, F.bsz[s], F.tw, tid, nth);
+        fft_stage_rt<true>(F, s, data, P, ps, tid, nth);
         __syncthreads();
     }
 }

@@ -796,6 +796,9 @@ static FftLen make_len(int n, bool lead2, DevBuf<float2> &tw, std::vector<int> *
     for (int s = 0; s < F.ns; ++s) {
         F.radix[s] = r[s];
         F.bsz[s] = b;
+        F.dm[s] = FastDiv::make((uint32_t)(b / r[s]));
+        F.dnb[s] = FastDiv::make((uint32_t)(n / r[s]));
+        F.dblk[s] = FastDiv::make((uint32_t)(n / b));
         b /= r[s];
     }
     std::vector<float2> h(n);
