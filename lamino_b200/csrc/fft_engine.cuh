@@ -456,6 +456,94 @@ __device__ __forceinline__ void fft1458_store(const Rows &rows, const float2 *__
     }
 }
 
+// The same register stages for a runtime length L (schedule 2, R1, ...): the
+// zero-padded radix-2 stage and the first radix-R1 stage (two blocks of L / 2,
+// m1 = L / (2 R1) offsets each) between the caller's loads / stores and shared
+// memory; rows of sm are ps apart, items (c, n) of 3 x m1 are spread over the
+// nth threads.  The caller runs stages 2 .. ns-1 (fft_forward / fft_inverse).
+template <int R1, class Rows>
+__device__ __forceinline__ void fftlead_load(const Rows &rows, const float2 *__restrict__ tw, float2 *__restrict__ sm,
+                                             int L, int ps, int tid, int nth) {
+    const int half = L / 2, m1 = half / R1;
+    for (int t = tid; t < 3 * m1; t += nth) {
+        const int c = t / m1, n = t - c * m1;
+        float2 x[R1], u[R1];
+#pragma unroll
+        for (int j = 0; j < R1; ++j) x[j] = rows.get(c, n + m1 * j);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) u[j] = c_mul(x[j], __ldg(tw + n + m1 * j));
+        dft_small<R1, false>(x);
+        dft_small<R1, false>(u);
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                x[k] = c_mul(x[k], w[k]);
+                u[k] = c_mul(u[k], w[k]);
+            }
+        }
+        float2 *sp = sm + c * ps + n;
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            sp[m1 * k] = x[k];
+            sp[half + m1 * k] = u[k];
+        }
+    }
+}
+
+template <int R1, class Rows>
+__device__ __forceinline__ void fftlead_store(const Rows &rows, const float2 *__restrict__ tw,
+                                              const float2 *__restrict__ sm, int L, int ps, int tid, int nth) {
+    const int half = L / 2, m1 = half / R1;
+    for (int t = tid; t < 3 * m1; t += nth) {
+        const int c = t / m1, n = t - c * m1;
+        const float2 *sp = sm + c * ps + n;
+        float2 a[R1], b[R1];
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            a[k] = sp[m1 * k];
+            b[k] = sp[half + m1 * k];
+        }
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                a[k] = c_mulc(a[k], w[k]);
+                b[k] = c_mulc(b[k], w[k]);
+            }
+        }
+        dft_small<R1, true>(a);
+        dft_small<R1, true>(b);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int i = n + m1 * j;
+            if (rows.want(i)) rows.put(c, i, c_add(a[j], c_mulc(b[j], __ldg(tw + i))));
+        }
+    }
+}
+
+// dispatch on the runtime first radix after the lead 2
+template <bool STORE, class Rows>
+__device__ __forceinline__ void fftlead_any(const Rows &rows, const FftLen &F, float2 *sm, int ps, int tid,
+                                            int nth) {
+#define LAMINO_LEAD_CASE(R)                                                       \
+    case R:                                                                       \
+        if constexpr (STORE) fftlead_store<R>(rows, F.tw, sm, F.n, ps, tid, nth); \
+        else fftlead_load<R>(rows, F.tw, sm, F.n, ps, tid, nth);                  \
+        break;
+    switch (F.radix[1]) {
+        LAMINO_LEAD_CASE(2)
+        LAMINO_LEAD_CASE(3)
+        LAMINO_LEAD_CASE(4)
+        LAMINO_LEAD_CASE(5)
+        LAMINO_LEAD_CASE(8)
+        default: LAMINO_LEAD_CASE(9)
+    }
+#undef LAMINO_LEAD_CASE
+}
+
 // Forward / inverse with a compile-time schedule when N != 0, else the runtime one.
 template <int N, int S_BEGIN>
 __device__ __forceinline__ void fft_fwd_any(float2 *data, int P, int ps, const FftLen &F, int tid, int nth) {

@@ -466,6 +466,10 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
         fft1458_load(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
         __syncthreads();
         ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
+    } else if (F1.ns >= 2) {  // runtime length: the outer stages in registers as well
+        fftlead_any<false>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
+        __syncthreads();
+        fft_forward(sm, 3, L1, F1, 2, threadIdx.x, blockDim.x);
     } else {
         for (int t0 = threadIdx.x; t0 < 3 * half; t0 += LD_BATCH * blockDim.x) {
             float2 v[LD_BATCH];
@@ -536,6 +540,9 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
     if constexpr (N1 == 1458) {
         ct_inverse<1458, 3, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
         fft1458_store(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
+    } else if (F1.ns >= 2) {
+        fft_inverse(sm, 3, L1, F1, 2, threadIdx.x, blockDim.x);
+        fftlead_any<true>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
     } else {
         fft_inv_any<N1, 1>(sm, 3, L1, F1, threadIdx.x, blockDim.x);
         for (int t = threadIdx.x; t < 3 * n1; t += blockDim.x) {
@@ -569,6 +576,10 @@ __global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ 
         fft1458_load(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm, threadIdx.x);  // reads only
         __syncthreads();
         ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
+    } else if (F1.ns >= 2) {
+        fftlead_any<false>(PencilRows{const_cast<float2 *>(pv), cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
+        __syncthreads();
+        fft_forward(sm, 3, L1, F1, 2, threadIdx.x, blockDim.x);
     } else {
         for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
             int c = t / half, i1 = t - c * half;
