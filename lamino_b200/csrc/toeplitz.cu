@@ -224,10 +224,88 @@ __device__ __forceinline__ void rows729_store(const float2 *__restrict__ sm, int
     }
 }
 
+// The first stage of a runtime-length row transform (radix R0 over the whole
+// packed row of M3, m0 = M3 / R0 offsets) in registers on the way in and its
+// inverse on the way out, as rows729_load / rows729_store for other lengths.
+template <int R0>
+__device__ __forceinline__ void rowslead_load(const float *__restrict__ xb, int nr, int n3, int M3,
+                                              const float2 *__restrict__ tw3, float2 *__restrict__ sm, int ps,
+                                              int tid, int nth) {
+    const int m0 = M3 / R0;
+    for (int t = tid; t < nr * m0; t += nth) {
+        const int r = t / m0, n = t - r * m0;
+        const float *xr = xb + (int64_t)r * n3;
+        float2 x[R0];
+#pragma unroll
+        for (int j = 0; j < R0; ++j) {
+            const int i = 2 * (n + m0 * j);
+            x[j].x = i < n3 ? xr[i] : 0.f;
+            x[j].y = i + 1 < n3 ? xr[i + 1] : 0.f;
+        }
+        dft_small<R0, false>(x);
+        if (n != 0) {
+            float2 w[R0];
+            twiddle_powers<R0>(tw3, n, w);
+#pragma unroll
+            for (int k = 1; k < R0; ++k) x[k] = c_mul(x[k], w[k]);
+        }
+        float2 *sp = sm + r * ps + n;
+#pragma unroll
+        for (int k = 0; k < R0; ++k) sp[m0 * k] = x[k];
+    }
+}
+
+template <int R0>
+__device__ __forceinline__ void rowslead_store(const float2 *__restrict__ sm, int nr, int ps, int n3, int M3,
+                                               const float2 *__restrict__ tw3, float *__restrict__ yb, int tid,
+                                               int nth) {
+    const int m0 = M3 / R0;
+    for (int t = tid; t < nr * m0; t += nth) {
+        const int r = t / m0, n = t - r * m0;
+        const float2 *sp = sm + r * ps + n;
+        float2 a[R0];
+#pragma unroll
+        for (int k = 0; k < R0; ++k) a[k] = sp[m0 * k];
+        if (n != 0) {
+            float2 w[R0];
+            twiddle_powers<R0>(tw3, n, w);
+#pragma unroll
+            for (int k = 1; k < R0; ++k) a[k] = c_mulc(a[k], w[k]);
+        }
+        dft_small<R0, true>(a);
+        float *yr = yb + (int64_t)r * n3;
+#pragma unroll
+        for (int j = 0; j < R0; ++j) {
+            const int i = 2 * (n + m0 * j);
+            if (i < n3) yr[i] = a[j].x;
+            if (i + 1 < n3) yr[i + 1] = a[j].y;
+        }
+    }
+}
+
+template <bool STORE>
+__device__ __forceinline__ void rowslead_any(const FftLen &F3, const float *xb, const float2 *smc, float2 *sm,
+                                             float *yb, int nr, int n3, int ps, int tid, int nth) {
+#define LAMINO_ROWS_CASE(R)                                                            \
+    case R:                                                                            \
+        if constexpr (STORE) rowslead_store<R>(smc, nr, ps, n3, F3.n, F3.tw, yb, tid, nth); \
+        else rowslead_load<R>(xb, nr, n3, F3.n, F3.tw, sm, ps, tid, nth);               \
+        break;
+    switch (F3.radix[0]) {
+        LAMINO_ROWS_CASE(2)
+        LAMINO_ROWS_CASE(3)
+        LAMINO_ROWS_CASE(4)
+        LAMINO_ROWS_CASE(5)
+        LAMINO_ROWS_CASE(8)
+        default: LAMINO_ROWS_CASE(9)
+    }
+#undef LAMINO_ROWS_CASE
+}
+
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
-__global__ void __launch_bounds__(256, 6) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
+__global__ void __launch_bounds__(256, N3 == 729 ? 6 : 4) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh,
                                                   int R, float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
@@ -239,6 +317,10 @@ __global__ void __launch_bounds__(256, 6) k_r2c_rows(const float *__restrict__ x
         rows729_load(x + row0 * n3, nr, n3, F3.tw, sm, ps, threadIdx.x, blockDim.x);
         __syncthreads();
         ct_forward<729, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
+    } else if (F3.ns >= 1) {  // runtime length: the first stage in registers as well
+        rowslead_any<false>(F3, x + row0 * n3, nullptr, sm, nullptr, nr, n3, ps, threadIdx.x, blockDim.x);
+        __syncthreads();
+        fft_forward(sm, nr, ps, F3, 1, threadIdx.x, blockDim.x);
     } else {
         const int total = nr * M3;
         const float *xb = x + row0 * n3;
@@ -730,6 +812,11 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
     if constexpr (N3 == 729) {
         ct_inverse<729, 2, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
         rows729_store(sm, nr, ps, n3, F3.tw, y + row0 * n3, threadIdx.x, blockDim.x);
+        return;
+    }
+    if (F3.ns >= 1) {
+        fft_inverse(sm, nr, ps, F3, 1, threadIdx.x, blockDim.x);
+        rowslead_any<true>(F3, nullptr, sm, nullptr, y + row0 * n3, nr, n3, ps, threadIdx.x, blockDim.x);
         return;
     }
     fft_inv_any<N3, 0>(sm, nr, ps, F3, threadIdx.x, blockDim.x);
