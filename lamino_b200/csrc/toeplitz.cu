@@ -457,6 +457,98 @@ __device__ __forceinline__ void dim2_144_store(const float2 *__restrict__ sm, in
     }
 }
 
+// The same register stages for a runtime L2 (schedule 2, R1, ...): item (ii, n, kk),
+// kk fastest, holds the values i2 = n + m1 j of tile pencil ii * KB + kk,
+// m1 = L2 / (2 R1); the stages from 2 on run in shared memory.
+template <int R1>
+__device__ __forceinline__ void dim2lead_load(const float2 *__restrict__ z1, int n1, int n2, int L3h, int c, int i1b,
+                                              int k3b, int nk, int KB, int ps, int L2,
+                                              const float2 *__restrict__ tw2, float2 *__restrict__ sm, int tid,
+                                              int nth) {
+    const int half = L2 / 2, m1 = half / R1;
+    const int total = D2_IB * m1 * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int ii = r / m1, n = r - ii * m1;
+        const int i1 = i1b + ii;
+        const bool live = kk < nk && i1 < n1;
+        float2 x[R1], u[R1];
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int i2 = n + m1 * j;
+            x[j] = (live && i2 < n2) ? z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < R1; ++j) u[j] = c_mul(x[j], __ldg(tw2 + n + m1 * j));
+        dft_small<R1, false>(x);
+        dft_small<R1, false>(u);
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                x[k] = c_mul(x[k], w[k]);
+                u[k] = c_mul(u[k], w[k]);
+            }
+        }
+        float2 *sp = sm + (ii * KB + kk) * ps + n;
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            sp[m1 * k] = x[k];
+            sp[half + m1 * k] = u[k];
+        }
+    }
+}
+
+template <int R1>
+__device__ __forceinline__ void dim2lead_store(const float2 *__restrict__ sm, int n1, int n2, int L3h, int c,
+                                               int i1b, int k3b, int nk, int KB, int ps, int L2,
+                                               const float2 *__restrict__ tw2, float2 *__restrict__ z1, int tid,
+                                               int nth) {
+    const int half = L2 / 2, m1 = half / R1;
+    const int total = D2_IB * m1 * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int ii = r / m1, n = r - ii * m1;
+        const int i1 = i1b + ii;
+        if (kk >= nk || i1 >= n1) continue;
+        const float2 *sp = sm + (ii * KB + kk) * ps + n;
+        float2 a[R1], b[R1];
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            a[k] = sp[m1 * k];
+            b[k] = sp[half + m1 * k];
+        }
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                a[k] = c_mulc(a[k], w[k]);
+                b[k] = c_mulc(b[k], w[k]);
+            }
+        }
+        dft_small<R1, true>(a);
+        dft_small<R1, true>(b);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int i2 = n + m1 * j;
+            if (i2 < n2)
+                z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] = c_add(a[j], c_mulc(b[j], __ldg(tw2 + i2)));
+        }
+    }
+}
+
+#define LAMINO_DIM2_LEAD(FN, R1SEL, ...)                       \
+    switch (R1SEL) {                                           \
+        case 2: FN<2>(__VA_ARGS__); break;                     \
+        case 3: FN<3>(__VA_ARGS__); break;                     \
+        case 4: FN<4>(__VA_ARGS__); break;                     \
+        case 5: FN<5>(__VA_ARGS__); break;                     \
+        case 8: FN<8>(__VA_ARGS__); break;                     \
+        default: FN<9>(__VA_ARGS__); break;                    \
+    }
+
 // A2: columns along n2 (zero-padded to L2) -> pencil-major xa[((c L2 + p2) L3h + k3) n1p + i1]
 template <int N2>
 __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ z1, int n1, int n2, int L3h, int n1p,
@@ -471,6 +563,11 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         dim2_144_load(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm, threadIdx.x, blockDim.x);
         __syncthreads();
         ct_forward<144, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+    } else if (F2.ns >= 2) {  // runtime length: the outer stages in registers as well
+        LAMINO_DIM2_LEAD(dim2lead_load, F2.radix[1], z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, sm,
+                         (int)threadIdx.x, (int)blockDim.x)
+        __syncthreads();
+        fft_forward(sm, D2_IB * KB, ps, F2, 2, threadIdx.x, blockDim.x);
     } else {
         // load: kk fastest (coalesced along k3); D2_BATCH independent loads in flight per thread
         constexpr int D2_BATCH = 4;
@@ -755,6 +852,12 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
     if constexpr (N2 == 144) {
         ct_inverse<144, 2, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
         dim2_144_store(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1, threadIdx.x, blockDim.x);
+        return;
+    }
+    if (F2.ns >= 2) {
+        fft_inverse(sm, D2_IB * KB, ps, F2, 2, threadIdx.x, blockDim.x);
+        LAMINO_DIM2_LEAD(dim2lead_store, F2.radix[1], sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, z1,
+                         (int)threadIdx.x, (int)blockDim.x)
         return;
     }
     fft_inv_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
