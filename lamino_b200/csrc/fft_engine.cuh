@@ -561,5 +561,7 @@ __device__ __forceinline__ void fft_inv_any(float2 *data, int P, int ps, const F
 std::vector<int> fft_schedule(int n, bool lead2);
 // natural frequency k -> DIF output position
 std::vector<int> fft_positions(int n, const std::vector<int> &radix);
+// smallest even 2,3,5-smooth length >= n (defined with the NUFFT plans)
+int64_t next_smooth_even(int64_t n);
 
 }  // namespace lamino

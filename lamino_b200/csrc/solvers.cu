@@ -500,23 +500,28 @@ __global__ void __launch_bounds__(RC_WARPS * 32) k_ramp_cols(float2 *__restrict_
     }
 }
 
-// Real transforms along n3 = N (365 <= N <= 729) as Bluestein convolutions through
-// the 1458-point pipeline: X[k] = sum_n x[n] e^{-2 pi i k n / N}
+// Real transforms along n3 = N as Bluestein convolutions through the pencil's FFT
+// pipeline: X[k] = sum_n x[n] e^{-2 pi i k n / N}
 // = conj(w_k) sum_n (x_n conj(w_n)) w_{k-n} with w_m = e^{i pi m^2 / N}, a circular
-// convolution of length M = 1458 >= 2N - 1, taken as undo(FWD(u) . V) with V the
+// convolution of length M >= 2N - 1, taken as undo(FWD(u) . V) with V the
 // transform of v (v_m = w_m for m < N, v_{M-m} = w_m for 0 < m < N, zero between),
 // divided by M and stored in DIF position order.  The inverse uses conj(w) in
-// place of w.  Two real rows travel as one complex row (a + i b), three complex
-// rows per CTA; the spectra keep the R2C layout [row][N/2 + 1].
+// place of w.  M = 1458 (the compile-time pipeline, fused outer stages) for
+// 365 <= N <= 729; otherwise M = the next 2,3,5-smooth even length >= 2N - 1 on
+// the runtime pipeline (same fused outer stages, FIXED = false), used for N with a
+// prime factor above 7, where cuFFT slows down.  Two real rows travel as one
+// complex row (a + i b), three complex rows per CTA; the spectra keep the R2C
+// layout [row][N/2 + 1].
 constexpr int kBlueM = 1458;
 constexpr int kBlueHalf = 729;
+constexpr int kBlueMaxM = 4096;
 
 struct BlueR2CRows {
     const float *x;
     int64_t nrows, q0;
-    int N;
+    int N, hm;  // hm: M / 2, the stride of zb
     const float2 *chirp;
-    float2 *zb;  // 3 x 729 results in shared memory
+    float2 *zb;  // 3 x M/2 results in shared memory
     __device__ __forceinline__ float2 get(int c, int i) const {
         const int64_t r = 2 * (q0 + c);
         if (i >= N || r >= nrows) return make_float2(0.f, 0.f);
@@ -525,38 +530,59 @@ struct BlueR2CRows {
     }
     __device__ __forceinline__ bool want(int i) const { return i < N; }
     __device__ __forceinline__ void put(int c, int i, float2 v) const {
-        zb[c * kBlueHalf + i] = c_mulc(v, __ldg(chirp + i));
+        zb[c * hm + i] = c_mulc(v, __ldg(chirp + i));
     }
 };
 
+// FWD(u), the pointwise product with V, undo: rows loaded and stored by `rows`
+template <bool FIXED, class Rows>
+__device__ __forceinline__ void blue_convolve(const Rows &rows, const FftLen &F, const float2 *__restrict__ V,
+                                              const float2 *__restrict__ tw, float2 *sm, int M) {
+    if constexpr (FIXED) {
+        fft1458_load(rows, tw, sm, threadIdx.x);
+        __syncthreads();
+        ct_forward<kBlueM, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+    } else {
+        fftlead_any<false>(rows, F, sm, M, threadIdx.x, blockDim.x);
+        __syncthreads();
+        fft_forward(sm, 3, M, F, 2, threadIdx.x, blockDim.x);
+    }
+    for (int p = threadIdx.x; p < M; p += blockDim.x) {
+        const float2 v = __ldg(V + p);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sm[c * M + p] = c_mul(sm[c * M + p], v);
+    }
+    __syncthreads();
+    if constexpr (FIXED) {
+        ct_inverse<kBlueM, 3, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
+        fft1458_store(rows, tw, sm, threadIdx.x);
+    } else {
+        fft_inverse(sm, 3, M, F, 2, threadIdx.x, blockDim.x);
+        fftlead_any<true>(rows, F, sm, M, threadIdx.x, blockDim.x);
+    }
+}
+
+template <bool FIXED>
 __global__ void __launch_bounds__(256, 4) k_blue_r2c(const float *__restrict__ x, int64_t nrows, int N,
                                                      const float2 *__restrict__ chirp,
                                                      const float2 *__restrict__ V,
-                                                     const float2 *__restrict__ tw, float2 *__restrict__ S) {
-    extern __shared__ float2 sm[];  // 3 transform rows of 1458, then 3 x 729 results
+                                                     const float2 *__restrict__ tw, FftLen F,
+                                                     float2 *__restrict__ S) {
+    extern __shared__ float2 sm[];  // 3 transform rows of M, then 3 x M/2 results
+    const int M = FIXED ? kBlueM : F.n, hm = M / 2;
     const int h = N / 2 + 1;
     const int64_t q0 = (int64_t)blockIdx.x * 3;
-    const BlueR2CRows rows{x, nrows, q0, N, chirp, sm + 3 * kBlueM};
-    fft1458_load(rows, tw, sm, threadIdx.x);
-    __syncthreads();
-    ct_forward<kBlueM, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
-    for (int p = threadIdx.x; p < kBlueM; p += blockDim.x) {
-        const float2 v = __ldg(V + p);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sm[c * kBlueM + p] = c_mul(sm[c * kBlueM + p], v);
-    }
-    __syncthreads();
-    ct_inverse<kBlueM, 3, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
-    fft1458_store(rows, tw, sm, threadIdx.x);
+    const BlueR2CRows rows{x, nrows, q0, N, hm, chirp, sm + 3 * M};
+    blue_convolve<FIXED>(rows, F, V, tw, sm, M);
     __syncthreads();
     // A = (Z_k + conj Z_{N-k}) / 2, B = (Z_k - conj Z_{N-k}) / 2i
-    const float2 *zb = sm + 3 * kBlueM;
+    const float2 *zb = sm + 3 * M;
     for (int t = threadIdx.x; t < 3 * h; t += blockDim.x) {
         const int c = t / h, k = t - c * h;
         const int64_t r = 2 * (q0 + c);
         if (r >= nrows) continue;
-        const float2 zk = zb[c * kBlueHalf + k];
-        const float2 zm = zb[c * kBlueHalf + (k == 0 ? 0 : N - k)];
+        const float2 zk = zb[c * hm + k];
+        const float2 zm = zb[c * hm + (k == 0 ? 0 : N - k)];
         S[r * h + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         if (r + 1 < nrows) S[(r + 1) * h + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
     }
@@ -592,30 +618,22 @@ struct BlueC2RRows {
     }
 };
 
-__global__ void __launch_bounds__(256, 5) k_blue_c2r(const float2 *__restrict__ S, int64_t nrows, int N,
+template <bool FIXED>
+__global__ void __launch_bounds__(256, FIXED ? 5 : 4) k_blue_c2r(const float2 *__restrict__ S, int64_t nrows, int N,
                                                      const float2 *__restrict__ chirp,
                                                      const float2 *__restrict__ V,
-                                                     const float2 *__restrict__ tw, float *__restrict__ y) {
-    extern __shared__ float2 sm[];  // 3 transform rows of 1458
+                                                     const float2 *__restrict__ tw, FftLen F,
+                                                     float *__restrict__ y) {
+    extern __shared__ float2 sm[];  // 3 transform rows of M
+    const int M = FIXED ? kBlueM : F.n;
     const BlueC2RRows rows{S, y, nrows, (int64_t)blockIdx.x * 3, N, N / 2 + 1, chirp};
-    fft1458_load(rows, tw, sm, threadIdx.x);
-    __syncthreads();
-    ct_forward<kBlueM, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
-    for (int p = threadIdx.x; p < kBlueM; p += blockDim.x) {
-        const float2 v = __ldg(V + p);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sm[c * kBlueM + p] = c_mul(sm[c * kBlueM + p], v);
-    }
-    __syncthreads();
-    ct_inverse<kBlueM, 3, 2>(sm, 3, kBlueM, tw, threadIdx.x, blockDim.x);
-    fft1458_store(rows, tw, sm, threadIdx.x);
+    blue_convolve<FIXED>(rows, F, V, tw, sm, M);
 }
 
 // chirp w_n = e^{i pi n^2 / N}, the convolution kernels' spectra in DIF position
-// order (forward: v; inverse: conj v; both / M) and the 1458-point twiddles, in FP64
-static void blue_tables(int N, std::vector<float2> &chirp, std::vector<float2> &vf, std::vector<float2> &vi,
+// order (forward: v; inverse: conj v; both / M) and the M-point twiddles, in FP64
+static void blue_tables(int N, int M, std::vector<float2> &chirp, std::vector<float2> &vf, std::vector<float2> &vi,
                         std::vector<float2> &tw) {
-    const int M = kBlueM;
     std::vector<double> wc(N), ws(N);
     for (int64_t n = 0; n < N; ++n) {
         const double a = M_PI * (double)((n * n) % (2 * (int64_t)N)) / (double)N;
@@ -663,6 +681,36 @@ static void blue_tables(int N, std::vector<float2> &chirp, std::vector<float2> &
     for (int e = 0; e < M; ++e) tw[e] = make_float2((float)cs[e], (float)sn[e]);
 }
 
+// largest prime factor of n
+static int64_t largest_prime_factor(int64_t n) {
+    int64_t p = 1;
+    for (int64_t q = 2; q * q <= n; ++q)
+        while (n % q == 0) {
+            p = q;
+            n /= q;
+        }
+    return n > 1 ? std::max(p, n) : p;
+}
+
+// schedule of the runtime Bluestein length M (lead 2) over the device twiddles
+static FftLen blue_len(int M, const float2 *tw_dev) {
+    const std::vector<int> r = fft_schedule(M, true);
+    FftLen F{};
+    F.n = M;
+    F.ns = (int)r.size();
+    int b = M;
+    for (int s = 0; s < F.ns; ++s) {
+        F.radix[s] = r[s];
+        F.bsz[s] = b;
+        F.dm[s] = FastDiv::make((uint32_t)(b / r[s]));
+        F.dnb[s] = FastDiv::make((uint32_t)(M / r[s]));
+        F.dblk[s] = FastDiv::make((uint32_t)(M / b));
+        b /= r[s];
+    }
+    F.tw = tw_dev;
+    return F;
+}
+
 RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
     int64_t n2 = d.n2, n3 = d.n3, h3 = n3 / 2 + 1;
     std::vector<float> xf(h3), yf(n2), f(n2 * h3);
@@ -687,10 +735,14 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
             }
         filt.alloc(n2 * h3);
         upload(filt.p, g.data(), g.size());
-        blue = n3 >= 365 && n3 <= kBlueHalf;
+        const bool fixed = n3 >= 365 && n3 <= kBlueHalf;
+        const int64_t mrt = next_smooth_even(2 * n3 - 1);
+        blue = fixed || (n3 >= 16 && largest_prime_factor(n3) > 7 && mrt <= kBlueMaxM);
+        blue_fixed = fixed;
         if (blue) {
+            const int M = fixed ? kBlueM : (int)mrt;
             std::vector<float2> hc, hvf, hvi, htw;
-            blue_tables((int)n3, hc, hvf, hvi, htw);
+            blue_tables((int)n3, M, hc, hvf, hvi, htw);
             chirp.alloc(hc.size());
             upload(chirp.p, hc.data(), hc.size());
             vfwd.alloc(hvf.size());
@@ -699,8 +751,11 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
             upload(vinv.p, hvi.data(), hvi.size());
             tw.alloc(htw.size());
             upload(tw.p, htw.data(), htw.size());
-            raise_smem_limit((const void *)k_blue_r2c, (int)(3 * (kBlueM + kBlueHalf) * sizeof(float2)));
-            raise_smem_limit((const void *)k_blue_c2r, (int)(3 * kBlueM * sizeof(float2)));
+            blue_f = blue_len(M, tw.p);
+            raise_smem_limit((const void *)k_blue_r2c<true>, (int)(3 * (kBlueM + kBlueHalf) * sizeof(float2)));
+            raise_smem_limit((const void *)k_blue_c2r<true>, (int)(3 * kBlueM * sizeof(float2)));
+            raise_smem_limit((const void *)k_blue_r2c<false>, (int)(3 * (M + M / 2) * sizeof(float2)));
+            raise_smem_limit((const void *)k_blue_c2r<false>, (int)(3 * M * sizeof(float2)));
         } else {
             int n[1] = {(int)n3};
             r2c.make(1, n, CUFFT_R2C, (int)(3 * d.n1 * n2));
@@ -720,9 +775,14 @@ void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
     int64_t h3 = d.n3 / 2 + 1, plane = d.n2 * h3;
     const int64_t nrows = 3 * d.n1 * d.n2;
     const unsigned gblue = (unsigned)(((nrows + 1) / 2 + 2) / 3);
-    if (blue) {
-        k_blue_r2c<<<gblue, 256, 3 * (kBlueM + kBlueHalf) * sizeof(float2), s>>>(
-            r3, nrows, (int)d.n3, chirp.p, vfwd.p, tw.p, spec.p);
+    const int M = blue_f.n;
+    if (blue && blue_fixed) {
+        k_blue_r2c<true><<<gblue, 256, 3 * (kBlueM + kBlueHalf) * sizeof(float2), s>>>(
+            r3, nrows, (int)d.n3, chirp.p, vfwd.p, tw.p, blue_f, spec.p);
+        LAMINO_LAUNCH("k_blue_r2c");
+    } else if (blue) {
+        k_blue_r2c<false><<<gblue, 256, 3 * (M + M / 2) * sizeof(float2), s>>>(r3, nrows, (int)d.n3, chirp.p,
+                                                                              vfwd.p, tw.p, blue_f, spec.p);
         LAMINO_LAUNCH("k_blue_r2c");
     } else {
         LAMINO_CUFFT(cufftSetStream(r2c.h, s));
@@ -737,9 +797,13 @@ void RampPrecond::apply3(const float *r3, float *z3, cudaStream_t s) {
         k_filter_mul<<<grid_for(3 * d.n1 * plane, 256), 256, 0, s>>>(spec.p, filt.p, plane, 3 * d.n1 * plane);
         LAMINO_LAUNCH("k_filter_mul");
     }
-    if (blue) {
-        k_blue_c2r<<<gblue, 256, 3 * kBlueM * sizeof(float2), s>>>(spec.p, nrows, (int)d.n3, chirp.p, vinv.p,
-                                                                   tw.p, z3);
+    if (blue && blue_fixed) {
+        k_blue_c2r<true><<<gblue, 256, 3 * kBlueM * sizeof(float2), s>>>(spec.p, nrows, (int)d.n3, chirp.p,
+                                                                         vinv.p, tw.p, blue_f, z3);
+        LAMINO_LAUNCH("k_blue_c2r");
+    } else if (blue) {
+        k_blue_c2r<false><<<gblue, 256, 3 * M * sizeof(float2), s>>>(spec.p, nrows, (int)d.n3, chirp.p, vinv.p,
+                                                                     tw.p, blue_f, z3);
         LAMINO_LAUNCH("k_blue_c2r");
     } else {
         LAMINO_CUFFT(cufftSetStream(c2r.h, s));

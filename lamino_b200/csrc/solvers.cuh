@@ -5,6 +5,7 @@
 #include <functional>
 
 #include "common.cuh"
+#include "fft_engine.cuh"
 
 namespace lamino {
 
@@ -51,8 +52,10 @@ struct RampPrecond {
     DevBuf<float2> spec;
     DevBuf<float> filt;  // the filter (2-D path) or the n2 convolution kernels (column path)
     bool cols = false;   // 1-D transforms along n3 and a circulant convolution along n2
-    bool blue = false;   // (with cols) the n3 transforms as Bluestein convolutions of 1458
+    bool blue = false;        // (with cols) the n3 transforms as Bluestein convolutions
+    bool blue_fixed = false;  // of length 1458 on the compile-time pipeline (else runtime M)
     DevBuf<float2> chirp, vfwd, vinv, tw;  // Bluestein tables: chirp, kernel spectra, twiddles
+    FftLen blue_f{};                       // schedule of the Bluestein length M
     explicit RampPrecond(Dims3 d);
     void apply3(const float *r3, float *z3, cudaStream_t s);  // all 3 components
 };

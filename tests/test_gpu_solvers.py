@@ -44,12 +44,15 @@ def test_demag_vs_oracle(L, O, dims):
     assert rel(L.opt.demag(h), -want) < 1e-5
 
 
-@pytest.mark.parametrize("dims", [(5, 9, 12), (3, 71, 721), (3, 5, 400), (1, 3, 365), (2, 128, 400), (2, 130, 6)])
+@pytest.mark.parametrize("dims", [(5, 9, 12), (3, 71, 721), (3, 5, 400), (1, 3, 365), (2, 128, 400), (2, 5, 179),
+                                  (1, 3, 1001), (2, 130, 6)])
 def test_ramp_preconditioner_vs_oracle(L, O, dims):
     """Every form: n2 <= 128 runs 1-D transforms along n3 and a circulant
     convolution along n2, the n3 transforms as Bluestein convolutions of 1458
     when 365 <= n3 <= 729 (odd and even n3, an odd number of rows; n2 = 128 takes
-    the column kernel's second pass over rows), larger n2 the 2-D transforms."""
+    the column kernel's second pass over rows) and as Bluestein convolutions of a
+    runtime length for n3 with a prime factor above 7 (179 -> 360, 1001 -> 2000),
+    larger n2 the 2-D transforms."""
     rng = np.random.default_rng(1)
     r = rng.standard_normal((3,) + dims).astype(np.float32)
     M = O.RampPreconditioner(dims)
