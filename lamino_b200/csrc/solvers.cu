@@ -508,8 +508,8 @@ __global__ void __launch_bounds__(RC_WARPS * 32) k_ramp_cols(float2 *__restrict_
 // divided by M and stored in DIF position order.  The inverse uses conj(w) in
 // place of w.  M = 1458 (the compile-time pipeline, fused outer stages) for
 // 365 <= N <= 729; otherwise M = the next 2,3,5-smooth even length >= 2N - 1 on
-// the runtime pipeline (same fused outer stages, FIXED = false), used for N with a
-// prime factor above 7, where cuFFT slows down.  Two real rows travel as one
+// the runtime pipeline (same fused outer stages, FIXED = false), used for N >= 128
+// with a prime factor above 7, where cuFFT slows down.  Two real rows travel as one
 // complex row (a + i b), three complex rows per CTA; the spectra keep the R2C
 // layout [row][N/2 + 1].
 constexpr int kBlueM = 1458;
@@ -737,7 +737,7 @@ RampPrecond::RampPrecond(Dims3 dd) : d(dd) {
         upload(filt.p, g.data(), g.size());
         const bool fixed = n3 >= 365 && n3 <= kBlueHalf;
         const int64_t mrt = next_smooth_even(2 * n3 - 1);
-        blue = fixed || (n3 >= 16 && largest_prime_factor(n3) > 7 && mrt <= kBlueMaxM);
+        blue = fixed || (n3 >= 128 && largest_prime_factor(n3) > 7 && mrt <= kBlueMaxM);
         blue_fixed = fixed;
         if (blue) {
             const int M = fixed ? kBlueM : (int)mrt;
