@@ -111,7 +111,12 @@ int lamino_residual(lamino_plan_t p, lamino_geom_t g, const float *f3, const flo
  * larger volumes are rejected with LAMINO_ERR_ARG.  f3 and yT3 must be device
  * pointers (host pointers are rejected); res is host memory.  The first call on
  * a device resolves the array's device address (with that device current) and
- * should come before any stream capture.  Every call shares the array and it
+ * should come before any stream capture; the address is kept for the life of
+ * the process, so after cudaDeviceReset (which ends the context the address
+ * belongs to) this entry point must not be called again in that process.  A
+ * plan that has not sorted the geometry (no earlier lamino_residual /
+ * lamino_sysmat with it) uses an unsorted point kernel, which needs no buffer
+ * either.  Every call shares the array and it
  * keeps the last call's contents (the reduction slots are cleared at the start
  * of each call); calls that overlap on the GPU, on any stream, race. */
 int lamino_residual_noalloc(lamino_plan_t p, lamino_geom_t g, const float *f3, const float *yT3, float yTy,

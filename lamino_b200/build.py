@@ -39,26 +39,48 @@ def needs_build() -> bool:
 
 
 def build(verbose: bool = False, force: bool = False, ptxas_v: bool = False) -> str:
+    """Compile each .cu into an object in parallel (lamino_b200/_build/), then link
+    the shared library."""
     if not force and not needs_build():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
     nvcc = nvcc_path()
     cuda_lib = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "lib64")
-    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-cudart", "static", "-o", LIB + ".tmp", *sources(),
-           f"-L{cuda_lib}", "-lcufft", "-Xlinker", f"-rpath={cuda_lib}"]
-    if ptxas_v:
-        cmd[1:1] = ["-Xptxas", "-v"]
+    bdir = os.path.join(HERE, "_build")
+    os.makedirs(bdir, exist_ok=True)
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3"]
+    if ptxas_v:
+        flags = ["-Xptxas", "-v", *flags]
+
+    def compile_one(src):
+        obj = os.path.join(bdir, os.path.basename(src) + ".o")
+        cmd = [nvcc, *flags, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+        return src, obj, r
+
+    srcs = sources()
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for src, _, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
+        if verbose or ptxas_v:
+            sys.stderr.write(r.stderr)
+    cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", LIB + ".tmp", *[o for _, o, _ in results],
+           f"-L{cuda_lib}", "-lcufft", "-Xlinker", f"-rpath={cuda_lib}"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True, env=env)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc build of liblamino_b200.so failed")
-    if verbose or ptxas_v:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc link of liblamino_b200.so failed")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

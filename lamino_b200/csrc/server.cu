@@ -18,10 +18,12 @@ Server::Server(int64_t budget, int slots, bool dry_run, double dry_run_ms)
     if (!dry_) {
         LAMINO_CUDA(cudaGetDevice(&dev));
         // keep up to the budget cached in the stream-ordered pool between requests
-        cudaMemPool_t pool;
-        LAMINO_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        // (the previous threshold comes back when the server is destroyed: the
+        // pool is the whole process's)
+        LAMINO_CUDA(cudaDeviceGetDefaultMemPool(&pool_, dev));
+        LAMINO_CUDA(cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &old_threshold_));
         uint64_t keep = (uint64_t)budget;
-        LAMINO_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        LAMINO_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
     for (int i = 0; i < slots; ++i)
         workers_.emplace_back([this, dev, i]() {
@@ -48,6 +50,10 @@ Server::~Server() {
     for (auto &t : workers_) t.join();  // running requests finish first
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return users_ == 0; });
+    if (pool_) {
+        cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &old_threshold_);
+        cudaGetLastError();
+    }
 }
 
 Server::Use::Use(Server &sv) : s(sv) {

@@ -83,6 +83,8 @@ class Server {
     int64_t budget_;
     int slots_;
     bool dry_;
+    cudaMemPool_t pool_ = nullptr;  // the device's default pool and its release threshold before the server
+    uint64_t old_threshold_ = 0;
     double dry_ms_;
     std::mutex mu_;
     std::condition_variable cv_;

@@ -786,12 +786,14 @@ def mbir_setup(datasets, recon_dims, params, proj_pad, eps=1e-12, exact=False,
     return out_dims, plan, grids, gammas, yT
 
 
-def MBIR1(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
+def MBIR1(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0, grid_dtype=np.float32):
     """src/mbir_cg.cpp:48-128 (projections padded by PAD_FACTOR-1).  refinements > 0
     runs the mixed form's algorithm (cgsolver_refined, maxIters // refinements inner
-    iterations per cycle) with the exact operator in both roles."""
+    iterations per cycle) with the exact operator in both roles.  grid_dtype: the
+    precision of the PolarGrid points (float32 as the reference's float build,
+    float64 as its double build)."""
     pad = np.float32(params.PAD_FACTOR - 1.0)
-    out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params, pad, eps, exact)
+    out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params, pad, eps, exact, grid_dtype)
     A = lambda v: normal(v, grids, gammas, plan)
     if refinements > 0:
         x = cgsolver_refined(A, A, yT, np.zeros((3,) + out_dims), max(1, params.maxIters // refinements),
@@ -801,11 +803,11 @@ def MBIR1(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
     return np.stack([crop3d(x[i], recon_dims) for i in range(3)])
 
 
-def MBIR2(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
+def MBIR2(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0, grid_dtype=np.float32):
     """src/mbir_sb.cpp:47-114 (projections padded by PAD_FACTOR itself); refinements
     > 0 as in MBIR1 for each inner linear solve."""
     out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params,
-                                                   params.PAD_FACTOR, eps, exact)
+                                                   params.PAD_FACTOR, eps, exact, grid_dtype)
     A = lambda v: normal(v, grids, gammas, plan)
     x = split_bregman(A, yT, np.zeros((3,) + out_dims), params.lam, params.mu,
                       params.maxIters, params.innerIters, params.tol, params.xtol,
@@ -813,10 +815,10 @@ def MBIR2(datasets, recon_dims, params, eps=1e-12, exact=False, refinements=0):
     return np.stack([crop3d(x[i], recon_dims) for i in range(3)])
 
 
-def MBIR3(datasets, recon_dims, params, eps=1e-12, exact=False):
+def MBIR3(datasets, recon_dims, params, eps=1e-12, exact=False, grid_dtype=np.float32):
     """src/mbir3.cpp:47-135 (NAG + qGGMRF; `mu` passed as the Lipschitz constant)."""
     out_dims, plan, grids, gammas, yT = mbir_setup(datasets, recon_dims, params,
-                                                   params.PAD_FACTOR, eps, exact)
+                                                   params.PAD_FACTOR, eps, exact, grid_dtype)
 
     def grad(x):
         g = sum(gradient(x, yT, pg, gm, plan) for pg, gm in zip(grids, gammas))
@@ -853,3 +855,40 @@ def synthetic_magnetization(dims, seed=1234, sigma=3.0, lateral_frac=0.8):
     a3 = int(round(n3 * (1 - lateral_frac) / 2))
     mask[a1:n1 - a1, :, a3:n3 - a3] = True
     return (m * mask).astype(np.float32)
+
+
+# Config 0 of the workload set (the reference's small CPU-runnable case):
+# recon (T, H, W) = 16 x 128 x 128 (internal (n1, n2, n3) = (W, T, H) =
+# (128, 16, 128)), 2 gamma datasets (0, 45 deg) x 90 angles uniform in
+# [0, 2 pi), 128 x 128 detector, data = forward model + 1% Gaussian noise,
+# 20 CG iterations (MBIR1).
+CONFIG0_RECON = (128, 16, 128)
+CONFIG0_GAMMAS = (0.0, math.pi / 4)
+CONFIG0_NPROJ = 90
+CONFIG0_DET = (128, 128)
+
+
+def config0_datasets(seed: int = 1234):
+    """Seeded config-0 datasets [(proj float32 (90, 128, 128), angles float32, gamma float32)].
+
+    Data follow the reference's forward tool (src/forward.cpp:132-177): the
+    magnetization is padded by pad3d(sqrt(2) - 1), projected with the forward
+    model on the detector padded likewise, and cropped to 128 x 128 (crop2d);
+    then N(0, (0.01 RMS)^2) noise is added.  The forward model runs in FP64 with
+    ES gridding at eps 1e-6 (data generation only)."""
+    rng = np.random.default_rng(seed)
+    m = synthetic_magnetization(CONFIG0_RECON, seed=seed, sigma=3.0).astype(np.float64)
+    fpad = np.float32(math.sqrt(2.0) - 1.0)
+    mp = np.stack([pad3d(m[i], fpad) for i in range(3)])
+    det_p = tuple(n + _npad(n, fpad) for n in CONFIG0_DET)
+    plan = NufftPlan(mp.shape[1:], eps=1e-6)
+    out = []
+    for g in CONFIG0_GAMMAS:
+        th = rng.uniform(0, 2 * np.pi, CONFIG0_NPROJ).astype(np.float32)
+        pg = PolarGrid(th, det_p[0], det_p[1], np.float32(g), dtype=np.float64)
+        p = forward(mp, pg, float(np.float32(g)), plan)
+        p = crop2d(p, (CONFIG0_NPROJ,) + CONFIG0_DET)
+        rms = float(np.sqrt(np.mean(p * p)))
+        p = p + rng.normal(0.0, 0.01 * rms, p.shape)
+        out.append((p.astype(np.float32), th, np.float32(g)))
+    return out

@@ -51,7 +51,7 @@ def test_ramp_preconditioner_vs_oracle(L, O, dims):
     convolution along n2, the n3 transforms as Bluestein convolutions of 1458
     when 365 <= n3 <= 729 (odd and even n3, an odd number of rows; n2 = 128 takes
     the column kernel's second pass over rows) and as Bluestein convolutions of a
-    runtime length for n3 with a prime factor above 7 (179 -> 360, 1001 -> 2000),
+    runtime length for n3 with a prime factor above 7 (179 -> 360, 1001 -> 2048),
     larger n2 the 2-D transforms."""
     rng = np.random.default_rng(1)
     r = rng.standard_normal((3,) + dims).astype(np.float32)
