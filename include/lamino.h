@@ -134,6 +134,17 @@ int lamino_residual_noalloc(lamino_plan_t p, lamino_geom_t g, const float *f3, c
 int lamino_normal_create(const lamino_geom_t *geoms, int ngeom, int64_t n1, int64_t n2, int64_t n3, int precision,
                          lamino_normal_t *out, void *stream);
 int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *stream);
+/* count independent applies y3s[i] = A x3s[i] on HOST buffers (no reference
+ * counterpart; it serves callers that stream volumes through the operator, e.g.
+ * the MBIR closures of many reconstructions sharing one geometry).  The inputs
+ * are staged through two device buffers on a copy-in stream and the results
+ * through two on a copy-out stream, so the copy-in of volume i+1 and the
+ * copy-out of result i-1 overlap apply i (PCIe is full duplex); pinned
+ * (page-locked) host buffers are needed for the overlap, pageable ones work but
+ * serialise.  Returns when every result is in host memory.  Device pointers are
+ * rejected (use lamino_normal_apply). */
+int lamino_normal_apply_many(lamino_normal_t op, int count, const float *const *x3s, float *const *y3s,
+                             void *stream);
 /* Embedding-grid sizes L[3] = (L1, L2, L3) and device bytes held by the operator. */
 int lamino_normal_info(lamino_normal_t op, int64_t *L, int64_t *bytes);
 int lamino_normal_destroy(lamino_normal_t op);

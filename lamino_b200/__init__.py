@@ -67,6 +67,7 @@ def lib():
         "lamino_residual": ([vp, vp, vp, vp, f32, P(f64), vp], i32),
         "lamino_normal_create": ([P(vp), i32, i64, i64, i64, i32, P(vp), vp], i32),
         "lamino_normal_apply": ([vp, vp, vp, vp], i32),
+        "lamino_normal_apply_many": ([vp, i32, vp, vp, vp], i32),
         "lamino_normal_info": ([vp, P(i64), P(i64)], i32),
         "lamino_normal_destroy": ([vp], i32),
         "lamino_normal_quadforms": ([vp, P(vp), i32, vp, P(f64), vp], i32),
@@ -344,6 +345,26 @@ class ToeplitzNormal:
             out = _empty_like_kind(x, tuple(x.shape))
         _check(lib().lamino_normal_apply(self._h, _ptr(x), _ptr(out), _stream(x)))
         return out
+
+    def apply_many(self, xs, outs):
+        """outs[i] = A xs[i] for host volumes (numpy arrays or CPU tensors, pinned
+        for the overlap): the copy-in of the next volume and the copy-out of the
+        previous result overlap the current apply (lamino_normal_apply_many)."""
+        n = len(xs)
+        if len(outs) != n:
+            raise ValueError("xs and outs must have the same length")
+        shape = (3,) + self.dims
+        for a in list(xs) + list(outs):
+            if tuple(a.shape) != shape:
+                raise ValueError(f"every volume must have shape {shape}")
+            if _is_torch(a) and (a.is_cuda or str(a.dtype) != "torch.float32" or not a.is_contiguous()):
+                raise ValueError("apply_many takes contiguous float32 host tensors")
+            if not _is_torch(a) and (a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("apply_many takes contiguous float32 host arrays")
+        xp = (ctypes.c_void_p * max(n, 1))(*[_ptr(a).value for a in xs])
+        yp = (ctypes.c_void_p * max(n, 1))(*[_ptr(a).value for a in outs])
+        _check(lib().lamino_normal_apply_many(self._h, n, xp, yp, ctypes.c_void_p(0)))
+        return outs
 
     def profile(self, enable: bool, max_applies: int = 64):
         _check(lib().lamino_normal_profile(self._h, int(bool(enable)), int(max_applies)))

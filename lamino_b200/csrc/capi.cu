@@ -22,6 +22,22 @@ struct lamino_plan_s {
 struct lamino_normal_s {
     std::unique_ptr<Toeplitz> t;
     DevBuf<float> sx, sy;  // staging for host-pointer calls, kept across calls
+    // lamino_normal_apply_many: two input and two output stagings, a copy-in and a
+    // copy-out stream, and the events that order them (created on first use)
+    DevBuf<float> px[2], py[2];
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    cudaEvent_t ev_start = nullptr;
+    ~lamino_normal_s() {
+        for (int i = 0; i < 2; ++i) {
+            if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+            if (ev_done[i]) cudaEventDestroy(ev_done[i]);
+            if (ev_out[i]) cudaEventDestroy(ev_out[i]);
+        }
+        if (ev_start) cudaEventDestroy(ev_start);
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
+    }
 };
 struct lamino_op_s {
     OpFn fn;
@@ -329,6 +345,60 @@ int lamino_normal_apply(lamino_normal_t op, const float *x3, float *y3, void *st
     op->t->apply(xd, yd, s);
     if (yh) LAMINO_CUDA(cudaMemcpyAsync(y3, yd, n * 4, cudaMemcpyDeviceToHost, s));
     if (xh || yh) LAMINO_CUDA(cudaStreamSynchronize(s));
+    API_END
+}
+
+int lamino_normal_apply_many(lamino_normal_t op, int count, const float *const *x3s, float *const *y3s,
+                             void *stream) {
+    API_BEGIN
+    if (!op || !x3s || !y3s) throw Error(ERR_ARG, "null argument");
+    if (count < 0) throw Error(ERR_ARG, "count must be non-negative");
+    const size_t n = 3 * (size_t)op->t->vol.size();
+    for (int i = 0; i < count; ++i) {
+        if (!x3s[i] || !y3s[i]) throw Error(ERR_ARG, "null array in the batch");
+        if (is_device_ptr(x3s[i]) || is_device_ptr(y3s[i]))
+            throw Error(ERR_ARG, "lamino_normal_apply_many takes host buffers (use lamino_normal_apply on device data)");
+    }
+    if (count == 0) return 0;
+    cudaStream_t s = S(stream);
+    if (!op->h2d) {
+        LAMINO_CUDA(cudaStreamCreateWithFlags(&op->h2d, cudaStreamNonBlocking));
+        LAMINO_CUDA(cudaStreamCreateWithFlags(&op->d2h, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            LAMINO_CUDA(cudaEventCreateWithFlags(&op->ev_in[i], cudaEventDisableTiming));
+            LAMINO_CUDA(cudaEventCreateWithFlags(&op->ev_done[i], cudaEventDisableTiming));
+            LAMINO_CUDA(cudaEventCreateWithFlags(&op->ev_out[i], cudaEventDisableTiming));
+        }
+        LAMINO_CUDA(cudaEventCreateWithFlags(&op->ev_start, cudaEventDisableTiming));
+    }
+    const int nb = count > 1 ? 2 : 1;
+    for (int b = 0; b < nb; ++b) {
+        if (op->px[b].n != n) op->px[b].alloc(n);
+        if (op->py[b].n != n) op->py[b].alloc(n);
+    }
+    // the copy streams start after the work already queued on the caller's stream
+    LAMINO_CUDA(cudaEventRecord(op->ev_start, s));
+    LAMINO_CUDA(cudaStreamWaitEvent(op->h2d, op->ev_start, 0));
+    LAMINO_CUDA(cudaStreamWaitEvent(op->d2h, op->ev_start, 0));
+    for (int i = 0; i < count; ++i) {
+        const int b = i % nb;
+        // input b is free once apply i - 2 finished reading it
+        if (i >= nb) LAMINO_CUDA(cudaStreamWaitEvent(op->h2d, op->ev_done[b], 0));
+        LAMINO_CUDA(cudaMemcpyAsync(op->px[b].p, x3s[i], n * 4, cudaMemcpyHostToDevice, op->h2d));
+        LAMINO_CUDA(cudaEventRecord(op->ev_in[b], op->h2d));
+        LAMINO_CUDA(cudaStreamWaitEvent(s, op->ev_in[b], 0));
+        // output b is free once the copy-out of result i - 2 finished
+        if (i >= nb) LAMINO_CUDA(cudaStreamWaitEvent(s, op->ev_out[b], 0));
+        op->t->apply(op->px[b].p, op->py[b].p, s);
+        LAMINO_CUDA(cudaEventRecord(op->ev_done[b], s));
+        LAMINO_CUDA(cudaStreamWaitEvent(op->d2h, op->ev_done[b], 0));
+        LAMINO_CUDA(cudaMemcpyAsync(y3s[i], op->py[b].p, n * 4, cudaMemcpyDeviceToHost, op->d2h));
+        LAMINO_CUDA(cudaEventRecord(op->ev_out[b], op->d2h));
+    }
+    // join both copy streams into the caller's stream, then wait for all of it
+    LAMINO_CUDA(cudaStreamWaitEvent(s, op->ev_out[(count - 1) % nb], 0));
+    LAMINO_CUDA(cudaStreamWaitEvent(s, op->ev_in[(count - 1) % nb], 0));
+    LAMINO_CUDA(cudaStreamSynchronize(s));
     API_END
 }
 

@@ -278,3 +278,29 @@ def test_toeplitz_compiled_fft_lengths(L, O, dims):
     q = T.quadforms(x, [T])[0]
     dots = [float(np.dot(x[i].ravel().astype(np.float64), y[i].ravel())) for i in range(3)]
     assert np.allclose(q, dots, rtol=1e-5, atol=1e-6 * max(abs(d) for d in dots)), (q, dots)
+
+
+def test_toeplitz_apply_many_matches_single_applies(L, O):
+    """lamino_normal_apply_many on host volumes (pageable numpy and pinned
+    tensors; odd and even counts) gives each volume's single-apply result
+    bit for bit, and rejects device buffers."""
+    import torch
+    rng = np.random.default_rng(3)
+    dims = (17, 6, 15)
+    pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, 5).astype(np.float32), 23, 21, np.float32(g)) for g in (0.0, 0.9)]
+    T = L.ToeplitzNormal(pgs, dims)
+    xs = [rng.standard_normal((3,) + dims).astype(np.float32) for _ in range(5)]
+    want = [T(x) for x in xs]
+    for n in (1, 2, 5):
+        outs = [np.empty_like(x) for x in xs[:n]]
+        T.apply_many(xs[:n], outs)
+        for o, w in zip(outs, want):
+            assert np.array_equal(o, w)
+    xp = [torch.from_numpy(x).pin_memory() for x in xs[:3]]
+    yp = [torch.empty_like(x).pin_memory() for x in xp]
+    T.apply_many(xp, yp)
+    for o, w in zip(yp, want):
+        assert np.array_equal(o.numpy(), w)
+    xd = torch.from_numpy(xs[0]).cuda()
+    with pytest.raises(ValueError):
+        T.apply_many([xd], [torch.empty_like(xd)])
