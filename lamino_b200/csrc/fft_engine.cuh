@@ -49,19 +49,41 @@ struct FftLen {  // POD, passed by value to kernels
     const float2 *tw;  // exp(-2 pi i e / n), e in [0, n)
 };
 
-__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex arithmetic on Blackwell's packed FP32 pair instructions (add / mul /
+// fma .f32x2: one instruction for both halves of a float2, per component the
+// same rounding as the scalar operation).
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ float2 c_mulc(float2 a, float2 b) {  // a * conj(b)
     return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
 }
-__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+// a (c + i s) for constants c, s: one packed product and two scalar FMAs
+__device__ __forceinline__ float2 c_mul_k(float2 a, float c, float s) {
+    const float2 t = __fmul2_rn(a, make_float2(c, c));
+    return make_float2(fmaf(-s, a.y, t.x), fmaf(s, a.x, t.y));
+}
+// s a + b for real s
+__device__ __forceinline__ float2 c_fma(float s, float2 a, float2 b) { return __ffma2_rn(make_float2(s, s), a, b); }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>
 __device__ __forceinline__ float2 c_rot(float2 a) {
     return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// m + (-i) s d and m - (-i) s d (forward; +i for the inverse), s real: the
+// rotation swaps the halves, so these run as scalar FMAs.
+template <bool INV>
+__device__ __forceinline__ void c_rot_pm(float2 m, float2 d, float s, float2 &plus, float2 &minus) {
+    if constexpr (!INV) {
+        plus = make_float2(fmaf(s, d.y, m.x), fmaf(-s, d.x, m.y));
+        minus = make_float2(fmaf(-s, d.y, m.x), fmaf(s, d.x, m.y));
+    } else {
+        plus = make_float2(fmaf(-s, d.y, m.x), fmaf(s, d.x, m.y));
+        minus = make_float2(fmaf(s, d.y, m.x), fmaf(-s, d.x, m.y));
+    }
 }
 
 template <bool INV>
@@ -70,21 +92,18 @@ __device__ __forceinline__ void dft3(float2 &x0, float2 &x1, float2 &x2) {
     float2 t = c_add(x1, x2);
     float2 d = c_sub(x1, x2);
     float2 y0 = c_add(x0, t);
-    float2 m = make_float2(fmaf(c, t.x, x0.x), fmaf(c, t.y, x0.y));
-    float2 r = c_rot<INV>(c_scale(d, s));  // -i s d (fwd) / +i s d (inv)
+    float2 m = c_fma(c, t, x0);
     x0 = y0;
-    x1 = c_add(m, r);
-    x2 = c_sub(m, r);
+    c_rot_pm<INV>(m, d, s, x1, x2);  // m -/+ i s d
 }
 
 template <bool INV>
 __device__ __forceinline__ void dft4(float2 &x0, float2 &x1, float2 &x2, float2 &x3) {
     float2 a = c_add(x0, x2), b = c_sub(x0, x2);
-    float2 c = c_add(x1, x3), d = c_rot<INV>(c_sub(x1, x3));
+    float2 c = c_add(x1, x3), e = c_sub(x1, x3);
     x0 = c_add(a, c);
     x2 = c_sub(a, c);
-    x1 = c_add(b, d);
-    x3 = c_sub(b, d);
+    c_rot_pm<INV>(b, e, 1.f, x1, x3);  // b -/+ i e
 }
 
 template <bool INV>
@@ -94,16 +113,14 @@ __device__ __forceinline__ void dft5(float2 (&v)[5]) {
     float2 a1 = c_add(v[1], v[4]), b1 = c_sub(v[1], v[4]);
     float2 a2 = c_add(v[2], v[3]), b2 = c_sub(v[2], v[3]);
     float2 y0 = c_add(v[0], c_add(a1, a2));
-    float2 m1 = make_float2(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
-    float2 m2 = make_float2(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    float2 m1 = c_fma(c2, a2, c_fma(c1, a1, v[0]));
+    float2 m2 = c_fma(c1, a2, c_fma(c2, a1, v[0]));
     // -i (s1 b1 + s2 b2) and -i (s2 b1 - s1 b2) for the forward transform
-    float2 r1 = c_rot<INV>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
-    float2 r2 = c_rot<INV>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+    float2 p1 = c_fma(s2, b2, c_scale(b1, s1));
+    float2 p2 = c_fma(-s1, b2, c_scale(b1, s2));
     v[0] = y0;
-    v[1] = c_add(m1, r1);
-    v[4] = c_sub(m1, r1);
-    v[2] = c_add(m2, r2);
-    v[3] = c_sub(m2, r2);
+    c_rot_pm<INV>(m1, p1, 1.f, v[1], v[4]);
+    c_rot_pm<INV>(m2, p2, 1.f, v[2], v[3]);
 }
 
 template <bool INV>
@@ -114,18 +131,17 @@ __device__ __forceinline__ void dft8(float2 (&v)[8]) {
     dft4<INV>(e0, e1, e2, e3);
     dft4<INV>(o0, o1, o2, o3);
     const float h = 0.70710678118654752440f;
-    // W8^1 = (1 - i)/sqrt2 (fwd), (1 + i)/sqrt2 (inv); W8^2 = -i / +i; W8^3 = (-1 - i)/sqrt2 / (-1 + i)/sqrt2
-    float2 t1 = INV ? make_float2(h * (o1.x - o1.y), h * (o1.x + o1.y)) : make_float2(h * (o1.x + o1.y), h * (o1.y - o1.x));
-    float2 t2 = c_rot<INV>(o2);
-    float2 t3 = INV ? make_float2(-h * (o3.x + o3.y), h * (o3.x - o3.y)) : make_float2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+    // W8^1 o = h q1 with q1 = o -/+ i o (fwd / inv), W8^2 o = -/+ i o,
+    // W8^3 o = h q3 with q3 = -o -/+ i o
+    const float2 q1 = INV ? make_float2(o1.x - o1.y, o1.x + o1.y) : make_float2(o1.x + o1.y, o1.y - o1.x);
+    const float2 q3 = INV ? make_float2(-(o3.x + o3.y), o3.x - o3.y) : make_float2(o3.y - o3.x, -(o3.x + o3.y));
     v[0] = c_add(e0, o0);
     v[4] = c_sub(e0, o0);
-    v[1] = c_add(e1, t1);
-    v[5] = c_sub(e1, t1);
-    v[2] = c_add(e2, t2);
-    v[6] = c_sub(e2, t2);
-    v[3] = c_add(e3, t3);
-    v[7] = c_sub(e3, t3);
+    v[1] = c_fma(h, q1, e1);
+    v[5] = c_fma(-h, q1, e1);
+    c_rot_pm<INV>(e2, o2, 1.f, v[2], v[6]);
+    v[3] = c_fma(h, q3, e3);
+    v[7] = c_fma(-h, q3, e3);
 }
 
 template <bool INV>
@@ -143,10 +159,10 @@ __device__ __forceinline__ void dft9(float2 (&v)[9]) {
     const float c2 = 0.17364817766693034885f, s2 = 0.98480775301220805936f;   // W9^2
     const float c4 = -0.93969262078590838405f, s4 = 0.34202014332566873304f;  // W9^4
     const float sg = INV ? 1.f : -1.f;
-    a[1][1] = c_mul(a[1][1], make_float2(c1, sg * s1));
-    a[1][2] = c_mul(a[1][2], make_float2(c2, sg * s2));
-    a[2][1] = c_mul(a[2][1], make_float2(c2, sg * s2));
-    a[2][2] = c_mul(a[2][2], make_float2(c4, sg * s4));
+    a[1][1] = c_mul_k(a[1][1], c1, sg * s1);
+    a[1][2] = c_mul_k(a[1][2], c2, sg * s2);
+    a[2][1] = c_mul_k(a[2][1], c2, sg * s2);
+    a[2][2] = c_mul_k(a[2][2], c4, sg * s4);
 #pragma unroll
     for (int k2 = 0; k2 < 3; ++k2) {
         float2 y0 = a[0][k2], y1 = a[1][k2], y2 = a[2][k2];
@@ -154,6 +170,56 @@ __device__ __forceinline__ void dft9(float2 (&v)[9]) {
         v[k2] = y0;
         v[3 + k2] = y1;
         v[6 + k2] = y2;
+    }
+}
+
+// cos / sin of 2 pi m / 27, m = 0..16 (the twiddles inside the 27-point DFT);
+// called with compile-time m, so the values fold into the instructions
+__host__ __device__ constexpr float w27c(int m) {
+    constexpr float t[17] = {1.f,
+                             0.97304487057982380627f,  0.89363264032341227505f,  0.76604444311897801345f,
+                             0.59715859170278617896f,  0.39607976603915689973f,  0.17364817766693041445f,
+                             -0.05814482891047577373f, -0.28680323271109020578f, -0.49999999999999977796f,
+                             -0.68624163786873348947f, -0.83548781141293626540f, -0.93969262078590831688f,
+                             -0.99323835774194302317f, -0.99323835774194302317f, -0.93969262078590853893f,
+                             -0.83548781141293648744f};
+    return t[m];
+}
+__host__ __device__ constexpr float w27s(int m) {
+    constexpr float t[17] = {0.f,
+                             0.23061587074244016549f,  0.44879918020046216665f,  0.64278760968653925190f,
+                             0.80212319275504373461f,  0.91821610688027399672f,  0.98480775301220802032f,
+                             0.99830815827126817563f,  0.95798951231548890028f,  0.86602540378443870761f,
+                             0.72737364157304884582f,  0.54950897807080623103f,  0.34202014332566887944f,
+                             0.11609291412522992903f,  -0.11609291412523012332f, -0.34202014332566821331f,
+                             -0.54950897807080600899f};
+    return t[m];
+}
+
+// 27-point DFT in registers: j = 3 j2 + j1, k = k1 + 9 k2; 9-point DFTs over
+// j2, twiddles W27^{j1 k1}, 3-point DFTs over j1.  Natural order in and out.
+template <bool INV>
+__device__ __forceinline__ void dft27(float2 (&v)[27]) {
+    float2 a[3][9];
+#pragma unroll
+    for (int j1 = 0; j1 < 3; ++j1) {
+#pragma unroll
+        for (int j2 = 0; j2 < 9; ++j2) a[j1][j2] = v[3 * j2 + j1];
+        dft9<INV>(a[j1]);
+    }
+    const float sg = INV ? 1.f : -1.f;
+#pragma unroll
+    for (int k1 = 1; k1 < 9; ++k1) {
+        a[1][k1] = c_mul_k(a[1][k1], w27c(k1), sg * w27s(k1));
+        a[2][k1] = c_mul_k(a[2][k1], w27c(2 * k1), sg * w27s(2 * k1));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 9; ++k1) {
+        float2 y0 = a[0][k1], y1 = a[1][k1], y2 = a[2][k1];
+        dft3<INV>(y0, y1, y2);
+        v[k1] = y0;
+        v[k1 + 9] = y1;
+        v[k1 + 18] = y2;
     }
 }
 

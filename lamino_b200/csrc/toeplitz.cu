@@ -627,12 +627,149 @@ struct PencilRows {
     __device__ __forceinline__ void put(int c, int i, float2 v) const { pv[c * cs + i] = v; }
 };
 
+// ---- n1 transforms of length 1458 = 2 x 27 x 27 (the 721-voxel axis) ----
+// Six warps per pencil: warp (c, h) = (w / 2, w % 2), lanes 0..26 busy.  Forward
+// DIF with the schedule 2, 27, 27 (positions fft_positions(1458, {2, 27, 27})):
+// half h of component c holds y_h[i] = x_i w^{h i}, w = exp(-2 pi i / 1458), x_i = 0
+// from n1 on.  Lane n of warp (c, h) takes y_h[n + 27 j] = w^{h n} x_{n+27j}
+// W54^{h j} (W54 = w^27), forms the 27-point DFT of x_{n+27j} W54^{hj}, multiplies
+// output k by w^{n (2k + h)} (the common w^{hn} and the stage twiddle
+// w^{2 n k}) and stores it at position 729 h + n + 27 k; the second stage is a
+// 27-point DFT per block of 27 positions, in place.  Each value makes one trip
+// through shared memory between the stages (two with the 2, 9, 9, 9 schedule).
+// The inverse runs the stages backwards; warp (c, 1) leaves its half times
+// conj(w^i) in shared memory and warp (c, 0) adds it to its own and stores.
+constexpr int P1458_THREADS = 192;
+// cos / sin of 2 pi j / 54, j = 0..26 (compile-time j: folded into the instructions)
+__host__ __device__ constexpr float w54c(int j) {
+    constexpr float t[27] = {1.f, 0.99323835774194302317f, 0.97304487057982380627f, 0.93969262078590842791f,
+                             0.89363264032341227505f, 0.83548781141293648744f, 0.76604444311897801345f,
+                             0.68624163786873360049f, 0.59715859170278617896f, 0.50000000000000011102f,
+                             0.39607976603915689973f, 0.28680323271109031680f, 0.17364817766693041445f,
+                             0.05814482891047567659f, -0.05814482891047577373f, -0.17364817766693008139f,
+                             -0.28680323271109020578f, -0.39607976603915678870f, -0.49999999999999977796f,
+                             -0.59715859170278595691f, -0.68624163786873348947f, -0.76604444311897823550f,
+                             -0.83548781141293626540f, -0.89363264032341216403f, -0.93969262078590831688f,
+                             -0.97304487057982380627f, -0.99323835774194302317f};
+    return t[j];
+}
+__host__ __device__ constexpr float w54s(int j) {
+    constexpr float t[27] = {0.f, 0.11609291412523023435f, 0.23061587074244016549f, 0.34202014332566871291f,
+                             0.44879918020046216665f, 0.54950897807080600899f, 0.64278760968653925190f,
+                             0.72737364157304862378f, 0.80212319275504373461f, 0.86602540378443859659f,
+                             0.91821610688027399672f, 0.95798951231548890028f, 0.98480775301220802032f,
+                             0.99830815827126817563f, 0.99830815827126817563f, 0.98480775301220813134f,
+                             0.95798951231548890028f, 0.91821610688027399672f, 0.86602540378443870761f,
+                             0.80212319275504395666f, 0.72737364157304884582f, 0.64278760968653914087f,
+                             0.54950897807080623103f, 0.44879918020046233318f, 0.34202014332566887944f,
+                             0.23061587074244033202f, 0.11609291412522992903f};
+    return t[j];
+}
+
+// v[k] *= w^{n (2k + h)} (conjugated for the inverse), k = k0 + 3 k1 + 9 k2, from
+// the table values w^n, w^{2n}, w^{6n}, w^{18n} (every factor at most a few
+// products from a table value).
+template <bool INV>
+__device__ __forceinline__ void p1458_twiddle(const float2 *__restrict__ tw, int n, int h, float2 (&v)[27]) {
+    const float2 z = __ldg(tw + 2 * n), z3 = __ldg(tw + 6 * n), z9 = __ldg(tw + 18 * n);
+    float2 p0[3];
+    p0[0] = h ? __ldg(tw + n) : make_float2(1.f, 0.f);
+    p0[1] = c_mul(p0[0], z);
+    p0[2] = c_mul(p0[1], z);
+    const float2 z6 = c_mul(z3, z3), z18 = c_mul(z9, z9);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+#pragma unroll
+        for (int k0 = 0; k0 < 3; ++k0) {
+            const float2 p = k1 == 0 ? p0[k0] : c_mul(p0[k0], k1 == 1 ? z3 : z6);
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2) {
+                const int k = k0 + 3 * k1 + 9 * k2;
+                const float2 t = k2 == 0 ? p : c_mul(p, k2 == 1 ? z9 : z18);
+                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
+            }
+        }
+    }
+}
+
+// Load (zero-padded), both forward stages; ends after a barrier with the DIF
+// spectrum of the 3 components in sm[c * 1458 + p].
+__device__ __forceinline__ void p1458_forward(const PencilRows &rows, const float2 *__restrict__ tw,
+                                              float2 *__restrict__ sm) {
+    const int w = threadIdx.x >> 5, n = threadIdx.x & 31;
+    const int c = w >> 1, h = w & 1;
+    float2 *half = sm + c * 1458 + h * 729;
+    if (n < 27) {
+        float2 v[27];
+#pragma unroll
+        for (int j = 0; j < 27; ++j) v[j] = rows.get(c, n + 27 * j);
+        if (h) {
+#pragma unroll
+            for (int j = 1; j < 27; ++j) v[j] = c_mul_k(v[j], w54c(j), -w54s(j));
+        }
+        dft27<false>(v);
+        p1458_twiddle<false>(tw, n, h, v);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) half[n + 27 * k] = v[k];
+    }
+    __syncthreads();
+    if (n < 27) {
+        float2 *row = half + 27 * n;
+        float2 v[27];
+#pragma unroll
+        for (int j = 0; j < 27; ++j) v[j] = row[j];
+        dft27<false>(v);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) row[k] = v[k];
+    }
+    __syncthreads();
+}
+
+// Both inverse stages and the pruned store of the first n1 values (the caller
+// synchronises after writing the spectrum).
+__device__ __forceinline__ void p1458_inverse(const PencilRows &rows, const float2 *__restrict__ tw,
+                                              float2 *__restrict__ sm) {
+    const int w = threadIdx.x >> 5, n = threadIdx.x & 31;
+    const int c = w >> 1, h = w & 1;
+    float2 *half = sm + c * 1458 + h * 729;
+    if (n < 27) {
+        float2 *row = half + 27 * n;
+        float2 v[27];
+#pragma unroll
+        for (int k = 0; k < 27; ++k) v[k] = row[k];
+        dft27<true>(v);
+#pragma unroll
+        for (int j = 0; j < 27; ++j) row[j] = v[j];
+    }
+    __syncthreads();
+    float2 v[27];
+    if (n < 27) {
+#pragma unroll
+        for (int k = 0; k < 27; ++k) v[k] = half[n + 27 * k];
+        p1458_twiddle<true>(tw, n, h, v);
+        dft27<true>(v);
+        if (h) {  // this half times conj(w^i) = conj(w^{n}) conj(W54^j); the first factor came with the twiddles
+#pragma unroll
+            for (int j = 0; j < 27; ++j) half[n + 27 * j] = j ? c_mul_k(v[j], w54c(j), w54s(j)) : v[j];
+        }
+    }
+    __syncthreads();
+    if (h == 0 && n < 27) {
+        const float2 *other = half + 729;
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = n + 27 * j;
+            if (rows.want(i)) rows.put(c, i, c_add(v[j], other[i]));
+        }
+    }
+}
+
 // B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
 // symmetric multiply with the spectra (same position order), undo, first n1 kept.
 // In place on xa.  N1: compile-time L1 or 0.  At L1 = 1458, five CTAs of 256
 // threads per SM (48 registers, 35 KB of shared memory each); four otherwise.
 template <bool HALF, int N1>
-__global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
+__global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
                                                 const float2 *__restrict__ tw1, const float *__restrict__ K,
                                                 const __half *__restrict__ Kh, const float *__restrict__ kscale) {
     extern __shared__ float2 sm[];
@@ -642,9 +779,7 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
     const int64_t cs = (int64_t)L2 * L3h * n1p;  // component stride in xa
     float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
-        fft1458_load(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
-        __syncthreads();
-        ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
+        p1458_forward(PencilRows{pv, cs, n1}, tw1, sm);
     } else if (F1.ns >= 2) {  // runtime length: the outer stages in registers as well
         fftlead_any<false>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -717,8 +852,7 @@ __global__ void __launch_bounds__(256, N1 == 1458 ? 5 : 4) k_pencil(float2 *__re
     }
     __syncthreads();
     if constexpr (N1 == 1458) {
-        ct_inverse<1458, 3, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
-        fft1458_store(PencilRows{pv, cs, n1}, tw1, sm, threadIdx.x);
+        p1458_inverse(PencilRows{pv, cs, n1}, tw1, sm);
     } else if (F1.ns >= 2) {
         fft_inverse(sm, 3, L1, F1, 2, threadIdx.x, blockDim.x);
         fftlead_any<true>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
@@ -741,7 +875,7 @@ struct QuadSets {
 };
 
 template <int N1>
-__global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h,
+__global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256) k_pencil_quad(const float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h,
                                                      FftLen F1, const float2 *__restrict__ tw1, QuadSets ks, int ng,
                                                      double *__restrict__ acc) {
     extern __shared__ float2 sm[];
@@ -752,9 +886,7 @@ __global__ void __launch_bounds__(256) k_pencil_quad(const float2 *__restrict__ 
     const int64_t cs = (int64_t)L2 * L3h * n1p;
     const float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
-        fft1458_load(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm, threadIdx.x);  // reads only
-        __syncthreads();
-        ct_forward<1458, 2>(sm, 3, L1, tw1, threadIdx.x, blockDim.x);
+        p1458_forward(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm);  // reads only
     } else if (F1.ns >= 2) {
         fftlead_any<false>(PencilRows{const_cast<float2 *>(pv), cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -1048,7 +1180,8 @@ void Toeplitz::init_tables(Dims3 d, int prec) {
         pos3.alloc(M3);
         upload(pos3.p, p3.data(), (size_t)M3);
     }
-    r1_ = r1;
+    // the compile-time n1 transform of 1458 runs the schedule 2, 27, 27 (p1458_forward)
+    r1_ = L1 == 1458 ? std::vector<int>{2, 27, 27} : r1;
     r2_ = r2;
 }
 
@@ -1262,9 +1395,9 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
     const bool h = precision == PREC_FP16 || (precision == PREC_MIXED && low);
     if (ct1 && h)
-        k_pencil<true, 1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
+        k_pencil<true, 1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
     else if (ct1)
-        k_pencil<false, 1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
+        k_pencil<false, 1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
     else if (h)
         k_pencil<true, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
     else
@@ -1312,7 +1445,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
         const int ng = (int)std::min<size_t>(kMaxQuadSets, parts.size() - g0);
         for (int g = 0; g < ng; ++g) qs.K[g] = parts[g0 + g]->K.p;
         if (ct1)
-            k_pencil_quad<1458><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
+            k_pencil_quad<1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
         else
             k_pencil_quad<0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
         LAMINO_LAUNCH("k_pencil_quad");
