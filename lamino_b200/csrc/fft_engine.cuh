@@ -223,6 +223,32 @@ __device__ __forceinline__ void dft27(float2 (&v)[27]) {
     }
 }
 
+// v[k] *= b w^{e k} for k = 0..26 (conjugated for the inverse), w^e = tw[e]:
+// with k = k0 + 3 k1 + 9 k2 every factor is at most a few products from the
+// table values tw[e], tw[3e], tw[9e] (3 table loads for 27 twiddles).
+template <bool INV>
+__device__ __forceinline__ void twiddle27(const float2 *__restrict__ tw, int e, float2 b, float2 (&v)[27]) {
+    const float2 z = __ldg(tw + e), z3 = __ldg(tw + 3 * e), z9 = __ldg(tw + 9 * e);
+    float2 p0[3];
+    p0[0] = b;
+    p0[1] = c_mul(b, z);
+    p0[2] = c_mul(p0[1], z);
+    const float2 z6 = c_mul(z3, z3), z18 = c_mul(z9, z9);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+#pragma unroll
+        for (int k0 = 0; k0 < 3; ++k0) {
+            const float2 p = k1 == 0 ? p0[k0] : c_mul(p0[k0], k1 == 1 ? z3 : z6);
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2) {
+                const int k = k0 + 3 * k1 + 9 * k2;
+                const float2 t = k2 == 0 ? p : c_mul(p, k2 == 1 ? z9 : z18);
+                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
+            }
+        }
+    }
+}
+
 // w^k for k = 1..R-1 from two table loads (w = tw[e], w4 = tw[4e] when R > 4),
 // every power at most two complex products away from a loaded value.
 template <int R>

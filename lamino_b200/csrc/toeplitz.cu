@@ -224,6 +224,72 @@ __device__ __forceinline__ void rows729_store(const float2 *__restrict__ sm, int
     }
 }
 
+// Rows of M3 = 729 as 27 x 27 (schedule 27, 27; positions
+// fft_positions(729, {27, 27})): one warp per row, lanes 0..26 busy.  The first
+// stage (27-point DFTs over the packed values n + 27 j, twiddles w729^{n k})
+// runs between the global rows and shared memory, the second (a 27-point DFT
+// per block of 27 positions) in place in shared memory; the inverses mirror
+// them.  Each value makes one trip through shared memory between the stages.
+__device__ __forceinline__ void rows27_load(const float *__restrict__ xb, int nr, int n3,
+                                            const float2 *__restrict__ tw3, float2 *__restrict__ sm, int ps) {
+    const int r = threadIdx.x >> 5, n = threadIdx.x & 31;
+    if (r < nr && n < 27) {
+        const float *xr = xb + (int64_t)r * n3;
+        float2 v[27];
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = 2 * (n + 27 * j);
+            v[j].x = i < n3 ? xr[i] : 0.f;
+            v[j].y = i + 1 < n3 ? xr[i + 1] : 0.f;
+        }
+        dft27<false>(v);
+        twiddle27<false>(tw3, n, make_float2(1.f, 0.f), v);
+        float2 *sp = sm + r * ps + n;
+#pragma unroll
+        for (int k = 0; k < 27; ++k) sp[27 * k] = v[k];
+    }
+    __syncthreads();
+}
+
+// the second stage in shared memory (the caller synchronises before it)
+template <bool INV>
+__device__ __forceinline__ void rows27_mid(float2 *__restrict__ sm, int nr, int ps) {
+    const int r = threadIdx.x >> 5, b = threadIdx.x & 31;
+    if (r < nr && b < 27) {
+        float2 *row = sm + r * ps + 27 * b;
+        float2 v[27];
+#pragma unroll
+        for (int j = 0; j < 27; ++j) v[j] = row[j];
+        dft27<INV>(v);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) row[k] = v[k];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void rows27_store(const float2 *__restrict__ sm, int nr, int ps, int n3,
+                                             const float2 *__restrict__ tw3, float *__restrict__ yb) {
+    const int r = threadIdx.x >> 5, n = threadIdx.x & 31;
+    if (r < nr && n < 27) {
+        const float2 *sp = sm + r * ps + n;
+        float2 v[27];
+#pragma unroll
+        for (int k = 0; k < 27; ++k) v[k] = sp[27 * k];
+        twiddle27<true>(tw3, n, make_float2(1.f, 0.f), v);
+        dft27<true>(v);
+        float *yr = yb + (int64_t)r * n3;
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = 2 * (n + 27 * j);
+            if (i < n3) yr[i] = v[j].x;
+            if (i + 1 < n3) yr[i + 1] = v[j].y;
+        }
+    }
+}
+
+// threads of a rows CTA of R rows: one warp per row for M3 = 729
+__host__ __device__ constexpr int rows_threads(int M3, int R) { return M3 == 729 && R <= 8 ? 32 * R : 256; }
+
 // The first stage of a runtime-length row transform (radix R0 over the whole
 // packed row of M3, m0 = M3 / R0 offsets) in registers on the way in and its
 // inverse on the way out, as rows729_load / rows729_store for other lengths.
@@ -305,7 +371,7 @@ __device__ __forceinline__ void rowslead_any(const FftLen &F3, const float *xb, 
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
-__global__ void __launch_bounds__(256, N3 == 729 ? 6 : 4) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
+__global__ void __launch_bounds__(256, N3 == 729 ? 3 : 4) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh,
                                                   int R, float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
@@ -314,9 +380,8 @@ __global__ void __launch_bounds__(256, N3 == 729 ? 6 : 4) k_r2c_rows(const float
     const int64_t row0 = (int64_t)blockIdx.x * R;
     const int nr = (int)min((int64_t)R, nrows - row0);
     if constexpr (N3 == 729) {
-        rows729_load(x + row0 * n3, nr, n3, F3.tw, sm, ps, threadIdx.x, blockDim.x);
-        __syncthreads();
-        ct_forward<729, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
+        rows27_load(x + row0 * n3, nr, n3, F3.tw, sm, ps);
+        rows27_mid<false>(sm, nr, ps);
     } else if (F3.ns >= 1) {  // runtime length: the first stage in registers as well
         rowslead_any<false>(F3, x + row0 * n3, nullptr, sm, nullptr, nr, n3, ps, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -666,32 +731,6 @@ __host__ __device__ constexpr float w54s(int j) {
     return t[j];
 }
 
-// v[k] *= w^{n (2k + h)} (conjugated for the inverse), k = k0 + 3 k1 + 9 k2, from
-// the table values w^n, w^{2n}, w^{6n}, w^{18n} (every factor at most a few
-// products from a table value).
-template <bool INV>
-__device__ __forceinline__ void p1458_twiddle(const float2 *__restrict__ tw, int n, int h, float2 (&v)[27]) {
-    const float2 z = __ldg(tw + 2 * n), z3 = __ldg(tw + 6 * n), z9 = __ldg(tw + 18 * n);
-    float2 p0[3];
-    p0[0] = h ? __ldg(tw + n) : make_float2(1.f, 0.f);
-    p0[1] = c_mul(p0[0], z);
-    p0[2] = c_mul(p0[1], z);
-    const float2 z6 = c_mul(z3, z3), z18 = c_mul(z9, z9);
-#pragma unroll
-    for (int k1 = 0; k1 < 3; ++k1) {
-#pragma unroll
-        for (int k0 = 0; k0 < 3; ++k0) {
-            const float2 p = k1 == 0 ? p0[k0] : c_mul(p0[k0], k1 == 1 ? z3 : z6);
-#pragma unroll
-            for (int k2 = 0; k2 < 3; ++k2) {
-                const int k = k0 + 3 * k1 + 9 * k2;
-                const float2 t = k2 == 0 ? p : c_mul(p, k2 == 1 ? z9 : z18);
-                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
-            }
-        }
-    }
-}
-
 // Load (zero-padded), both forward stages; ends after a barrier with the DIF
 // spectrum of the 3 components in sm[c * 1458 + p].
 __device__ __forceinline__ void p1458_forward(const PencilRows &rows, const float2 *__restrict__ tw,
@@ -708,7 +747,7 @@ __device__ __forceinline__ void p1458_forward(const PencilRows &rows, const floa
             for (int j = 1; j < 27; ++j) v[j] = c_mul_k(v[j], w54c(j), -w54s(j));
         }
         dft27<false>(v);
-        p1458_twiddle<false>(tw, n, h, v);
+        twiddle27<false>(tw, 2 * n, h ? __ldg(tw + n) : make_float2(1.f, 0.f), v);  // w^{n (2k + h)}
 #pragma unroll
         for (int k = 0; k < 27; ++k) half[n + 27 * k] = v[k];
     }
@@ -746,7 +785,7 @@ __device__ __forceinline__ void p1458_inverse(const PencilRows &rows, const floa
     if (n < 27) {
 #pragma unroll
         for (int k = 0; k < 27; ++k) v[k] = half[n + 27 * k];
-        p1458_twiddle<true>(tw, n, h, v);
+        twiddle27<true>(tw, 2 * n, h ? __ldg(tw + n) : make_float2(1.f, 0.f), v);
         dft27<true>(v);
         if (h) {  // this half times conj(w^i) = conj(w^{n}) conj(W54^j); the first factor came with the twiddles
 #pragma unroll
@@ -1045,8 +1084,8 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
     }
     __syncthreads();
     if constexpr (N3 == 729) {
-        ct_inverse<729, 2, 1>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
-        rows729_store(sm, nr, ps, n3, F3.tw, y + row0 * n3, threadIdx.x, blockDim.x);
+        rows27_mid<true>(sm, nr, ps);
+        rows27_store(sm, nr, ps, n3, F3.tw, y + row0 * n3);
         return;
     }
     if (F3.ns >= 1) {
@@ -1168,6 +1207,7 @@ void Toeplitz::init_tables(Dims3 d, int prec) {
     f1 = make_len((int)L1, true, tw1, &r1);
     f2 = make_len((int)L2, true, tw2, &r2);
     f3 = make_len((int)M3, false, tw3, &r3);
+    if (M3 == 729) r3 = {27, 27};  // the compile-time rows (rows27_load / rows27_mid)
     {
         std::vector<float2> h(M3 + 1);
         for (int64_t k = 0; k <= M3; ++k) {
@@ -1385,7 +1425,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
     const unsigned gpen = (unsigned)(L2 * L3h);
     if (prof) LAMINO_CUDA(cudaEventRecord(E[0], s));
-    if (ct3) k_r2c_rows<729><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    if (ct3) k_r2c_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[1], s));
@@ -1408,7 +1448,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     else k_dim2_inv<0><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
     LAMINO_LAUNCH("k_dim2_inv");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[4], s));
-    if (ct3) k_c2r_rows<729><<<grows, 256, smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
+    if (ct3) k_c2r_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
     else k_c2r_rows<0><<<grows, 256, smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
     LAMINO_LAUNCH("k_c2r_rows");
     if (prof) {
@@ -1434,7 +1474,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
     const unsigned gpen = (unsigned)(L2 * L3h);
-    if (ct3) k_r2c_rows<729><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    if (ct3) k_r2c_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
     if (ct2) k_dim2_fwd<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
@@ -1454,6 +1494,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
 
 void Toeplitz::set_shape(int rows, int kb) {
     if (rows < 1 || kb < 1) throw Error(ERR_ARG, "launch shape values must be positive");
+    if (ct3 && rows > 8) throw Error(ERR_ARG, "rows of 729 run one warp per row, at most 8 per CTA");
     const int64_t smem_rows = (int64_t)rows * L3h * (int64_t)sizeof(float2);
     const int64_t smem_d2 = (int64_t)D2_IB * kb * d2_stride((int)L2, kb) * (int64_t)sizeof(float2);
     if (smem_rows > 200 * 1024 || smem_d2 > 200 * 1024) throw Error(ERR_ARG, "launch shape exceeds shared memory");
