@@ -200,6 +200,197 @@ class Plan1 {
     }
 };
 
+// Eight lines at a time, structure of arrays (re[i][lane], im[i][lane]), by the
+// Stockham autosort recursion (decimation in frequency): a stage of radix r over
+// a sequence of length n with stride s maps x to y with
+//   y[q + s (r p + k)] = w_n^{p k} sum_j x[q + s (p + j n / r)] w_r^{j k},
+// p < n / r, q < s, then continues on length n / r with stride s r, swapping
+// x and y; the result is in natural order.  Radices 4, 2, 3, 5 and any odd
+// factor up to 64 (direct DFT); the innermost loop runs over the 8 lines, so
+// it vectorises.  Used for lengths without a prime factor above 64.
+template <class R>
+class BatchPlan {
+  public:
+    static constexpr int LANES = 8;
+    explicit BatchPlan(int n) : n_(n) {
+        int m = n;
+        while (m % 4 == 0) { rad_.push_back(4); m /= 4; }
+        while (m % 2 == 0) { rad_.push_back(2); m /= 2; }
+        for (int p = 3; m > 1; p += 2)
+            while (m % p == 0) { rad_.push_back(p); m /= p; }
+        // per stage twiddles w_len^{p k} (forward sign), p < len / r, k < r
+        int len = n;
+        for (int r : rad_) {
+            const int mm = len / r;
+            std::vector<cpx<R>> t((size_t)mm * r);
+            for (int p = 0; p < mm; ++p)
+                for (int k = 0; k < r; ++k) {
+                    const double a = -2.0 * M_PI * (double)((int64_t)p * k % len) / (double)len;
+                    t[(size_t)p * r + k] = cpx<R>((R)std::cos(a), (R)std::sin(a));
+                }
+            tw_.push_back(std::move(t));
+            std::vector<cpx<R>> d((size_t)r);
+            for (int k = 0; k < r; ++k) {
+                const double a = -2.0 * M_PI * (double)k / (double)r;
+                d[k] = cpx<R>((R)std::cos(a), (R)std::sin(a));
+            }
+            dft_.push_back(std::move(d));
+            len = mm;
+        }
+    }
+    static bool usable(int n) {
+        int m = n;
+        for (int p = 2; m > 1 && p <= 64; ++p)
+            while (m % p == 0) m /= p;
+        return m == 1;
+    }
+    // x, y: 2 n LANES values each (re block then im block); the result ends in x
+    void exec(R *x, R *y, int sign) const {
+        R *a = x, *b = y;
+        int len = n_, s = 1;
+        for (size_t st = 0; st < rad_.size(); ++st) {
+            stage(rad_[st], len, s, tw_[st].data(), dft_[st].data(), a, b, sign);
+            std::swap(a, b);
+            len /= rad_[st];
+            s *= rad_[st];
+        }
+        if (a != x) std::memcpy(x, a, sizeof(R) * 2 * (size_t)n_ * LANES);
+    }
+
+  private:
+    int n_;
+    std::vector<int> rad_;
+    std::vector<std::vector<cpx<R>>> tw_, dft_;
+
+    // radix-r butterfly on 8 lanes (b = DFT_r(a)); r in {2, 3, 4} fixed at compile time
+    template <int RAD>
+    static inline void bfly(R (&ar)[RAD][LANES], R (&ai)[RAD][LANES], R (&br)[RAD][LANES], R (&bi)[RAD][LANES],
+                            R sg) {
+        if constexpr (RAD == 2) {
+            for (int l = 0; l < LANES; ++l) {
+                br[0][l] = ar[0][l] + ar[1][l];
+                bi[0][l] = ai[0][l] + ai[1][l];
+                br[1][l] = ar[0][l] - ar[1][l];
+                bi[1][l] = ai[0][l] - ai[1][l];
+            }
+        } else if constexpr (RAD == 3) {
+            const R c = (R)-0.5, sn = sg * (R)0.86602540378443864676;
+            for (int l = 0; l < LANES; ++l) {
+                const R tr = ar[1][l] + ar[2][l], ti = ai[1][l] + ai[2][l];
+                const R dr = ar[1][l] - ar[2][l], di = ai[1][l] - ai[2][l];
+                const R mr = ar[0][l] + c * tr, mi = ai[0][l] + c * ti;
+                br[0][l] = ar[0][l] + tr;
+                bi[0][l] = ai[0][l] + ti;
+                br[1][l] = mr + sn * di;  // m -/+ i sn d
+                bi[1][l] = mi - sn * dr;
+                br[2][l] = mr - sn * di;
+                bi[2][l] = mi + sn * dr;
+            }
+        } else {
+            static_assert(RAD == 4, "fixed radices 2, 3, 4");
+            for (int l = 0; l < LANES; ++l) {
+                const R t0r = ar[0][l] + ar[2][l], t0i = ai[0][l] + ai[2][l];
+                const R t1r = ar[0][l] - ar[2][l], t1i = ai[0][l] - ai[2][l];
+                const R t2r = ar[1][l] + ar[3][l], t2i = ai[1][l] + ai[3][l];
+                const R dr = ar[1][l] - ar[3][l], di = ai[1][l] - ai[3][l];
+                const R t3r = sg * di, t3i = -sg * dr;  // -i d (forward), +i d (backward)
+                br[0][l] = t0r + t2r;
+                bi[0][l] = t0i + t2i;
+                br[2][l] = t0r - t2r;
+                bi[2][l] = t0i - t2i;
+                br[1][l] = t1r + t3r;
+                bi[1][l] = t1i + t3i;
+                br[3][l] = t1r - t3r;
+                bi[3][l] = t1i - t3i;
+            }
+        }
+    }
+
+    template <int RAD>
+    void stage_fixed(int len, int s, const cpx<R> *__restrict tw, const R *__restrict x, R *__restrict y,
+                     int sign) const {
+        const int m = len / RAD;
+        const size_t N = (size_t)n_ * LANES;
+        const R *__restrict xr = x;
+        const R *__restrict xi = x + N;
+        R *__restrict yr = y;
+        R *__restrict yi = y + N;
+        const R sg = sign < 0 ? (R)1 : (R)-1;
+        for (int p = 0; p < m; ++p) {
+            R wr[RAD], wi[RAD];
+            for (int k = 0; k < RAD; ++k) {
+                wr[k] = tw[(size_t)p * RAD + k].real();
+                wi[k] = sg * tw[(size_t)p * RAD + k].imag();
+            }
+            for (int q = 0; q < s; ++q) {
+                R ar[RAD][LANES], ai[RAD][LANES], br[RAD][LANES], bi[RAD][LANES];
+                for (int j = 0; j < RAD; ++j) {
+                    const size_t o = ((size_t)q + (size_t)s * (p + (size_t)j * m)) * LANES;
+                    for (int l = 0; l < LANES; ++l) {
+                        ar[j][l] = xr[o + l];
+                        ai[j][l] = xi[o + l];
+                    }
+                }
+                bfly<RAD>(ar, ai, br, bi, sg);
+                for (int k = 0; k < RAD; ++k) {
+                    const size_t o = ((size_t)q + (size_t)s * ((size_t)RAD * p + k)) * LANES;
+                    for (int l = 0; l < LANES; ++l) {
+                        yr[o + l] = wr[k] * br[k][l] - wi[k] * bi[k][l];
+                        yi[o + l] = wr[k] * bi[k][l] + wi[k] * br[k][l];
+                    }
+                }
+            }
+        }
+    }
+
+    void stage(int r, int len, int s, const cpx<R> *tw, const cpx<R> *dft, const R *x, R *y, int sign) const {
+        if (r == 2) return stage_fixed<2>(len, s, tw, x, y, sign);
+        if (r == 3) return stage_fixed<3>(len, s, tw, x, y, sign);
+        if (r == 4) return stage_fixed<4>(len, s, tw, x, y, sign);
+        // any other odd factor up to 64: direct DFT
+        const int m = len / r;
+        const size_t N = (size_t)n_ * LANES;
+        const R *xr = x, *xi = x + N;
+        R *yr = y, *yi = y + N;
+        const R sg = sign < 0 ? (R)1 : (R)-1;
+        std::vector<R> ar((size_t)r * LANES), ai((size_t)r * LANES);
+        for (int p = 0; p < m; ++p)
+            for (int q = 0; q < s; ++q) {
+                for (int j = 0; j < r; ++j) {
+                    const size_t o = ((size_t)q + (size_t)s * (p + (size_t)j * m)) * LANES;
+                    for (int l = 0; l < LANES; ++l) {
+                        ar[j * LANES + l] = xr[o + l];
+                        ai[j * LANES + l] = xi[o + l];
+                    }
+                }
+                for (int k = 0; k < r; ++k) {
+                    R br[LANES], bi[LANES];
+                    for (int l = 0; l < LANES; ++l) {
+                        br[l] = ar[l];
+                        bi[l] = ai[l];
+                    }
+                    int e = 0;
+                    for (int j = 1; j < r; ++j) {
+                        e += k;
+                        if (e >= r) e -= r;
+                        const R wr = dft[e].real(), wi = sg * dft[e].imag();
+                        for (int l = 0; l < LANES; ++l) {
+                            br[l] += wr * ar[j * LANES + l] - wi * ai[j * LANES + l];
+                            bi[l] += wr * ai[j * LANES + l] + wi * ar[j * LANES + l];
+                        }
+                    }
+                    const cpx<R> w = tw[(size_t)p * r + k];
+                    const R wr = w.real(), wi = sg * w.imag();
+                    const size_t o = ((size_t)q + (size_t)s * ((size_t)r * p + k)) * LANES;
+                    for (int l = 0; l < LANES; ++l) {
+                        yr[o + l] = wr * br[l] - wi * bi[l];
+                        yi[o + l] = wr * bi[l] + wi * br[l];
+                    }
+                }
+            }
+    }
+};
+
 inline int threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();
@@ -212,6 +403,46 @@ inline int threads() {
 template <class R>
 void fft_axis(cpx<R> *data, int64_t outer, int64_t n, int64_t inner, int sign) {
     if (n <= 1) return;
+    if (BatchPlan<R>::usable((int)n)) {
+        // lines in groups of 8: gathered into structure-of-arrays buffers
+        constexpr int64_t B = BatchPlan<R>::LANES;
+        const BatchPlan<R> plan((int)n);
+        const int64_t nblk = (inner + B - 1) / B;
+        const int64_t groups = inner == 1 ? (outer + B - 1) / B : outer * nblk;
+#pragma omp parallel
+        {
+            std::vector<R> x(2 * n * B), y(2 * n * B);
+            R *xr = x.data(), *xi = x.data() + n * B;
+#pragma omp for schedule(static)
+            for (int64_t t = 0; t < groups; ++t) {
+                // line b of the group: element i at base + b * lstride + i * istride
+                cpx<R> *base;
+                int64_t nb, lstride, istride;
+                if (inner == 1) {
+                    base = data + t * B * n;
+                    nb = std::min(B, outer - t * B);
+                    lstride = n;
+                    istride = 1;
+                } else {
+                    const int64_t o = t / nblk, j0 = (t % nblk) * B;
+                    base = data + o * n * inner + j0;
+                    nb = std::min(B, inner - j0);
+                    lstride = 1;
+                    istride = inner;
+                }
+                for (int64_t i = 0; i < n; ++i)
+                    for (int64_t b = 0; b < B; ++b) {
+                        const cpx<R> v = b < nb ? base[b * lstride + i * istride] : cpx<R>(0, 0);
+                        xr[i * B + b] = v.real();
+                        xi[i * B + b] = v.imag();
+                    }
+                plan.exec(x.data(), y.data(), sign);
+                for (int64_t i = 0; i < n; ++i)
+                    for (int64_t b = 0; b < nb; ++b) base[b * lstride + i * istride] = cpx<R>(xr[i * B + b], xi[i * B + b]);
+            }
+        }
+        return;
+    }
     Plan1<R> plan((int)n);
     const size_t ws = plan.work_size();
     if (inner == 1) {

@@ -21,6 +21,7 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "cpu_fft.hpp"
@@ -263,7 +264,16 @@ struct Nufft {
     int execute(std::complex<R> *c, std::complex<R> *f) const {
         const int64_t n1 = nf[0], n2 = nf[1], n3 = nf[2];
         const int64_t total = n1 * n2 * n3;
-        std::vector<std::complex<R>> G(total, std::complex<R>(0, 0));
+        // the fine grid, zeroed by all threads (a serial fill of GBs would dominate small calls)
+        std::unique_ptr<std::complex<R>[]> Gbuf(new std::complex<R>[total]);
+        std::complex<R> *Gd = Gbuf.get();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < total; ++i) Gd[i] = std::complex<R>(0, 0);
+        struct {
+            std::complex<R> *p;
+            std::complex<R> *data() const { return p; }
+            std::complex<R> &operator[](int64_t i) const { return p[i]; }
+        } G{Gd};
         R *Gr = reinterpret_cast<R *>(G.data());
         if (type == 1) {
             spread(c, Gr);

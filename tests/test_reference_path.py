@@ -105,6 +105,19 @@ def test_mbir_matches_reference(O, solvers, method):
     assert rel(got, solvers[f"mbir{method}"]) < 1e-8
 
 
+def test_mbir3_toeplitz_form_matches_reference(O, solvers):
+    """The oracle's MBIR3 with FP64 Toeplitz operators (used where the NUFFT
+    form is too slow on the CPU) reproduces the reference's own MBIR3."""
+    from make_reference_golden import MBIR_PARAMS, MBIR_RECON
+    data = [(solvers[f"mbir_proj{i}"], solvers[f"mbir_angles{i}"], np.float32(solvers[f"mbir_gamma{i}"]))
+            for i in range(2)]
+    kw = MBIR_PARAMS[3]
+    po = O.ReconParams(maxIters=kw["max_iters"], innerIters=kw["inner_iters"])
+    got, L = O.MBIR3_toeplitz(data, MBIR_RECON, po, grid_dtype=np.float64)
+    assert L == po.mu
+    assert rel(got, solvers["mbir3"]) < 1e-6
+
+
 def test_reference_fixture_inputs_regenerate(O, ops, solvers):
     """The fixtures' inputs are reproducible from their seeds (the GPU tests
     rebuild them the same way)."""

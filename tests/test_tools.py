@@ -317,7 +317,8 @@ _REGULARIZERS = {
 @pytest.mark.parametrize("method", [1, 2, 3])
 def test_recon_tool_end_to_end(L, O, tmp_path, method):
     """TIFF stacks + angle files + TOML -> `python -m lamino_b200.recon` -> TIFF and
-    VTI outputs equal to the direct MBIR1/2/3 call in the reference's axis order."""
+    VTI outputs equal to the direct MBIR1/2/3 call in the reference's axis order,
+    and to the FP64 oracle's MBIR1/2/3 on the same datasets."""
     T, H, W = 5, 9, 11
     internal = (W, T, H)
     rng = np.random.default_rng(5)
@@ -350,6 +351,12 @@ max_iters = 4
     want = fn(ds, internal, L.ReconParams(maxIters=4, innerIters=2 if method == 2 else 3))
     want = np.stack([np.transpose(want[i], (1, 2, 0)) for i in range(3)])
     assert rel(got, want) < 1e-5
+    # and the FP64 oracle (pinned to the reference's own MBIR drivers) on the
+    # datasets the tool read: the reconstruction within 1e-4
+    ofn = {1: O.MBIR1, 2: O.MBIR2, 3: O.MBIR3}[method]
+    oracle = ofn(ds, internal, O.ReconParams(maxIters=4, innerIters=2 if method == 2 else 3), eps=1e-12)
+    oracle = np.stack([np.transpose(oracle[i], (1, 2, 0)) for i in range(3)])
+    assert rel(got, oracle) < 1e-4
 
 
 @pytest.mark.gpu
