@@ -65,101 +65,92 @@ def workload_config(precision: str, n: int):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle port, bounded sample, extrapolated to one apply
+# CPU baseline and reference arm: the reference's own sysmat, compiled
+# (oracle/_ref), on a bounded sample of the workload
 # ---------------------------------------------------------------------------
 
-_CPU_CACHE: dict = {}
+REF_GAMMA = 0.7853981852531433  # float32(pi / 4): the 45 deg dataset
+REF_NPROJ = (1, 4)               # projections per sample call (two counts, to fit F and P)
+_REF_STATE: dict = {}
 
 
-def cpu_sample_seconds(planes: int = 16, rows: int = 64):
-    """Time the oracle's FP32 ES-kernel NUFFT pieces at the full workload size on a
-    bounded sample and extrapolate one sum-over-gamma sysmat apply (per gamma
-    3 type-2 + 3 type-1 transforms, src/gradient.cpp:34-89; each = one fine-grid
-    3-D FFT + gridding of 361 x 1233^2 points).
-
-    Sample: the three 1-D FFT passes of the (1458, 144, 1458) complex64 fine grid
-    over `planes`-thick slabs, and ES interp + spread of `rows` detector rows of
-    one projection.  Returns (seconds per apply, threads, description)."""
-    import ctypes
-
+def reference_sample(nproj: int):
+    """One call of the reference's own tomocam::sysmat<float> (src/gradient.cpp:34-89,
+    compiled unmodified into oracle/_ref against this project's FINUFFT-API and
+    FFTW-API shims) on the full 721 x 71 x 721 volume and `nproj` projections of
+    the 1233 x 1233 padded detector.  Returns host seconds."""
     import numpy as np
-    from oracle import oracle as O
-    import scipy.fft as sfft
+    from oracle import refpath as R
+    if "x" not in _REF_STATE:  # inputs, outside the timed call
+        rng = np.random.default_rng(11)
+        _REF_STATE["x"] = rng.standard_normal((3,) + PADDED).astype(np.float32)
+        _REF_STATE["th"] = rng.uniform(0, 2 * np.pi, 8).astype(np.float32)
+    t = time.perf_counter()
+    R.sysmat(_REF_STATE["x"], _REF_STATE["th"][:nproj], DET_PADDED, DET_PADDED, np.float32(REF_GAMMA),
+             dtype=np.float32)
+    return time.perf_counter() - t
 
-    w, beta = O.es_params(1.2e-6)
-    nf = tuple(O.next_smooth_even(max(2 * n, 2 * w)) for n in PADDED)  # (z, y, x)
-    threads = O.num_threads()
-    if "G" not in _CPU_CACHE:  # one-off setup, outside the timed sample
-        rng = np.random.default_rng(0)
-        th = rng.uniform(0, 2 * np.pi, 1).astype(np.float32)
-        pg = O.PolarGrid(th, DET_PADDED, DET_PADDED, np.float32(np.pi / 4))
-        _CPU_CACHE["pts"] = (pg.x[0], pg.y[0], pg.z[0])
-        G = np.zeros(nf, np.complex64)
-        G[:64] = (rng.standard_normal((64,) + nf[1:]) + 1j).astype(np.complex64)
-        G[:, :64] = 1.0 + 0.5j
-        _CPU_CACHE["G"] = G
-    G = _CPU_CACHE["G"]
-    r0 = (DET_PADDED - rows) // 2
-    x, y, z = (np.ascontiguousarray(a[r0:r0 + rows]).ravel() for a in _CPU_CACHE["pts"])
-    fp = ctypes.POINTER(ctypes.c_float)
-    lib = O._lib()
-    c = np.zeros(x.size, np.complex64)
-    t = time.perf_counter()
-    sfft.fft(G[:planes], axis=2, workers=threads)        # x lines of `planes` z-planes
-    t_x = time.perf_counter() - t
-    t = time.perf_counter()
-    sfft.fft(G[:planes], axis=1, workers=threads)        # y lines of `planes` z-planes
-    t_y = time.perf_counter() - t
-    t = time.perf_counter()
-    sfft.fft(G[:, :planes], axis=0, workers=threads)     # z lines of `planes` y-planes
-    t_z = time.perf_counter() - t
-    t = time.perf_counter()
-    lib.oracle_es_interp_f(x.size, x.ctypes.data_as(fp), y.ctypes.data_as(fp), z.ctypes.data_as(fp),
-                           nf[2], nf[1], nf[0], G.view(np.float32).ctypes.data_as(fp), w, beta,
-                           c.view(np.float32).ctypes.data_as(fp))
-    t_int = time.perf_counter() - t
-    t = time.perf_counter()
-    lib.oracle_es_spread_f(x.size, x.ctypes.data_as(fp), y.ctypes.data_as(fp), z.ctypes.data_as(fp),
-                           c.view(np.float32).ctypes.data_as(fp), nf[2], nf[1], nf[0],
-                           G.view(np.float32).ctypes.data_as(fp), w, beta)
-    t_spr = time.perf_counter() - t
-    fft3 = t_x * nf[0] / planes + t_y * nf[0] / planes + t_z * nf[1] / planes
-    per_proj = DET_PADDED / rows
-    grid_int = t_int * per_proj * NPROJ
-    grid_spr = t_spr * per_proj * NPROJ
-    per_apply = len(GAMMAS_DEG) * (6 * fft3 + 3 * grid_int + 3 * grid_spr)
-    sample = (f"oracle port, FP32 ES kernel w={w}, full-size fine grid {nf}: 1-D FFT passes over "
-              f"{planes}-plane slabs (3-D FFT extrapolated {fft3:.2f} s) and interp/spread of {rows} of "
-              f"{DET_PADDED} rows of one projection (extrapolated {grid_int:.2f} / {grid_spr:.2f} s per "
-              f"361-angle transform); one apply = 4 gammas x (6 FFT + 3 interp + 3 spread)")
-    return per_apply, threads, sample
+
+def reference_model(samples):
+    """Fit t(p) = F + p P to (projections, seconds) samples (F: the per-call
+    fine-grid FFTs and deconvolution, P: the per-projection gridding and array
+    work) and extrapolate one sum-over-gamma apply: 4 gammas x (F + 361 P)."""
+    import numpy as np
+    p = np.array([s[0] for s in samples], float)
+    t = np.array([s[1] for s in samples], float)
+    if len(set(p.tolist())) < 2:
+        raise RuntimeError("the reference model needs samples at two projection counts")
+    A = np.stack([np.ones_like(p), p], axis=1)
+    (F, P), *_ = np.linalg.lstsq(A, t, rcond=None)
+    F, P = max(float(F), 0.0), max(float(P), 0.0)
+    return F, P, len(GAMMAS_DEG) * (F + NPROJ * P)
+
+
+def reference_threads():
+    from oracle import oracle as O
+    return O.num_threads()
+
+
+def reference_description(F, P, apply_s):
+    return (f"reference's own tomocam::sysmat<float> (oracle/_ref: src/gradient.cpp and src/projection.cpp "
+            f"compiled unmodified against this project's FINUFFT-API / FFTW-API shims) on the full 721x71x721 "
+            f"volume, 1 or 4 projections of 1233x1233 per call; fit t = F + p P: F = {F:.2f} s per call "
+            f"(fine-grid FFTs), P = {P:.3f} s per projection; one sum-over-gamma apply extrapolated as "
+            f"4 x (F + 361 P) = {apply_s:.1f} s")
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # per-step sample sized so warmup + steps stay within a few minutes
-    budget = 150.0 / (args.steps + args.warmup)
-    planes, rows = (16, 64) if budget > 1.5 else ((8, 32) if budget > 0.5 else (4, 8))
-    for _ in range(args.warmup):
-        cpu_sample_seconds(planes, rows)
+    from oracle import refpath as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtomocam_ref.so is not built "
+                          "(oracle/Makefile needs the reference tree)"}), flush=True)
+        return 0
+    # steps alternate 1 and 4 projections so the timed samples fit F and P
+    for w in range(args.warmup):
+        reference_sample(REF_NPROJ[w % 2])
     t_start = time.perf_counter()
     samples = []
-    for _ in range(args.steps):
-        sec, threads, sample = cpu_sample_seconds(planes, rows)
-        samples.append(sec)
+    for k in range(args.steps):
+        p = REF_NPROJ[k % 2]
+        samples.append((p, reference_sample(p)))
     wall = time.perf_counter() - t_start
-    mean = statistics.mean(samples)
-    v = 1.0 / mean
+    if args.steps < 2:
+        samples.append((REF_NPROJ[1], reference_sample(REF_NPROJ[1])))
+    F, P, apply_s = reference_model(samples)
+    v = 1.0 / apply_s
+    threads = reference_threads()
+    ms_step = 1e3 * sum(t for _, t in samples[:args.steps]) / args.steps
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "applies/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args.precision, args.gpus),
-        "cpu_baseline": {"value": v, "unit": "applies/s", "cores": threads, "kind": "port",
-                         "sample": sample + "; reference CPU path = this project's oracle port "
-                                            "(FINUFFT/FFTW absent, reference NUFFT path unbuildable)"},
+        "cpu_baseline": {"value": v, "unit": "applies/s", "cores": threads, "kind": "reference",
+                         "sample": reference_description(F, P, apply_s) +
+                         "; ms_per_step is the measured time of one sample call"},
         "e2e": {"value": v, "unit": "applies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": wall,
     }
@@ -395,21 +386,34 @@ def run_ours(args):
         "launch_shape": {"rows_per_cta": shape[0], "k3_per_cta": shape[1], "tuned_apply_ms": shape[2]},
     }
     if rank == 0 and world == 1 and not args.no_served:
-        # the served form against the plain loop on a short request stream (one GPU)
-        sv = serve_compare(torch, L, 16, [1.0], 2)
-        sw = sv["sweep"][0]
+        # the served form against the plain loop on a request stream (one GPU)
+        sv = serve_compare(torch, L, SERVE_LINE_REQUESTS, [0.5, 1.0, 1.5], 2)
         line["served"] = {
-            "workload": "16 requests of the mixed-size NAG + qGGMRF stream, Poisson arrivals at the plain "
-                        "loop's capacity, 2 slots, 150 GB budget",
-            "p50_s": sw["served"]["p50_s"], "p99_s": sw["served"]["p99_s"],
-            "plain_p50_s": sw["plain"]["p50_s"], "plain_p99_s": sw["plain"]["p99_s"],
+            "workload": f"{SERVE_LINE_REQUESTS} requests of the mixed-size NAG + qGGMRF stream (thickness "
+                        "8-32, lateral 64-256, 2 gammas x 60-240 angles, 40 iterations), Poisson arrivals at "
+                        "0.5 / 1.0 / 1.5 x the plain loop's saturated throughput, 2 slots, 150 GB budget; "
+                        "plain = one at a time, eager launches, default shapes; plain_tuned = one at a time "
+                        "with the served form's graphs and tuned shapes; all FP32 with FP64 reductions",
+            "rates": [{"rate_x_plain_capacity": r["rate_x_plain_capacity"],
+                       "served_p50_s": r["served"]["p50_s"], "served_p99_s": r["served"]["p99_s"],
+                       "plain_p50_s": r["plain"]["p50_s"], "plain_p99_s": r["plain"]["p99_s"],
+                       **({"plain_tuned_p50_s": r["plain_tuned"]["p50_s"],
+                           "plain_tuned_p99_s": r["plain_tuned"]["p99_s"]} if "plain_tuned" in r else {})}
+                      for r in sv["sweep"]],
             "saturated_recon_per_s": sv["saturated"]["served"]["recon_per_s"],
             "plain_saturated_recon_per_s": sv["saturated"]["plain"]["recon_per_s"],
+            "plain_tuned_saturated_recon_per_s": sv["saturated"]["plain_tuned"]["recon_per_s"],
             "max_rel_err_vs_plain": sv["max_rel_err_served_vs_plain"]}
+        at1 = [r for r in sv["sweep"] if r["rate_x_plain_capacity"] == 1.0][0]
+        line["served"].update({"p50_s": at1["served"]["p50_s"], "p99_s": at1["served"]["p99_s"],
+                               "plain_p50_s": at1["plain"]["p50_s"], "plain_p99_s": at1["plain"]["p99_s"]})
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sec, threads, sample = cpu_sample_seconds(128, DET_PADDED)
-        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "applies/s", "cores": threads, "kind": "port",
-                                "sample": sample}
+        from oracle import refpath as R
+        if R.available():
+            samples = [(p, reference_sample(p)) for p in REF_NPROJ]
+            F, P, apply_s = reference_model(samples)
+            line["cpu_baseline"] = {"value": 1.0 / apply_s, "unit": "applies/s", "cores": reference_threads(),
+                                    "kind": "reference", "sample": reference_description(F, P, apply_s)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -424,6 +428,7 @@ def run_ours(args):
 
 SERVE_BUDGET = 150 * 10**9   # HBM bytes the served form may admit at once
 SERVE_ITERS = 40             # NAG + qGGMRF iterations of a mix request
+SERVE_LINE_REQUESTS = 100    # requests of the served summary in the default bench line
 
 
 def serve_mix(n: int, seed: int = 7, big_frac: float = 0.0):
@@ -470,7 +475,7 @@ def serve_data(torch, L, spec):
 
 
 def serve_params(L, spec, form: str):
-    # plain: eager launches, default launch shapes; served: graphs, tuned shapes
+    # plain: eager launches, default launch shapes; plain_tuned and served: graphs, tuned shapes
     kw = dict(op_kind="toeplitz", use_graphs=False, autotune=False) if form == "plain" else \
         dict(op_kind="toeplitz", use_graphs=True, autotune=True)
     if spec["method"] == 3:  # mu = 0: Lipschitz constant from 30 power iterations
@@ -483,10 +488,11 @@ def _pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
 
-def run_plain_loop(L, specs, data, arrivals):
-    """One reconstruction at a time in arrival order (FP32 Toeplitz, eager
-    launches): returns results, latencies (arrival -> done), service times and
-    applies."""
+def run_plain_loop(L, specs, data, arrivals, form: str = "plain"):
+    """One reconstruction at a time in arrival order (FP32 Toeplitz; eager
+    launches and default shapes, or with form "plain_tuned" the served form's
+    graphs and tuned shapes): returns results, latencies (arrival -> done),
+    service times and applies."""
     fns = {1: L.MBIR1, 2: L.MBIR2, 3: L.MBIR3}
     res, lat, svc, app, ph = [], [], [], [], []
     t0 = time.perf_counter()
@@ -495,7 +501,7 @@ def run_plain_loop(L, specs, data, arrivals):
         if arrivals[i] > now:
             time.sleep(arrivals[i] - now)
         a = time.perf_counter()
-        res.append(fns[sp["method"]](d, sp["recon"], serve_params(L, sp, "plain")))
+        res.append(fns[sp["method"]](d, sp["recon"], serve_params(L, sp, form)))
         b = time.perf_counter()
         svc.append(b - a)
         lat.append(b - t0 - arrivals[i])
@@ -554,9 +560,11 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
             seen.add((sp["method"], tuple(sp["recon"])))
             warm.append(i)
     run_plain_loop(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm))
+    run_plain_loop(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), "plain_tuned")
     run_served(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), slots)
     zeros = [0.0] * n
     p_res, p_lat, p_svc, p_app, p_span, p_ph = run_plain_loop(L, specs, data, zeros)
+    _, _, _, t_app, t_span, _ = run_plain_loop(L, specs, data, zeros, "plain_tuned")
     s_res, s_lat, s_app, s_span, s_st, s_info = run_served(L, specs, data, zeros, slots)
     errs = [float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(s_res, p_res)]
     nonfinite = sum(int(not np.all(np.isfinite(a))) + int(not np.all(np.isfinite(b))) for a, b in zip(s_res, p_res))
@@ -572,6 +580,7 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
                 "voxels_total": int(sum(3 * np.prod(sp["recon"]) for sp in specs))},
         "saturated": {
             "plain": {"recon_per_s": mu_plain, "applies_per_s": sum(p_app) / p_span, "makespan_s": p_span},
+            "plain_tuned": {"recon_per_s": n / t_span, "applies_per_s": sum(t_app) / t_span, "makespan_s": t_span},
             "served": {"recon_per_s": n / s_span, "applies_per_s": sum(s_app) / s_span, "makespan_s": s_span,
                        "peak_active": s_st["peak_active"], "peak_bytes": s_st["peak_in_use"]},
         },
@@ -587,12 +596,18 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
         arr = [a - arr[0] for a in arr]
         _, pl, psvc, _, pspan, _ = run_plain_loop(L, specs, data, arr)
         sres, sl, _, sspan, _, sinfo = run_served(L, specs, data, arr, slots)
+        tuned = None
+        if f == 1.0:  # one rate for the tuned loop: graphs and tuning without the batching
+            _, tl, tsvc, _, tspan, _ = run_plain_loop(L, specs, data, arr, "plain_tuned")
+            tuned = {"p50_s": _pct(tl, 50), "p99_s": _pct(tl, 99), "mean_s": float(np.mean(tl)),
+                     "recon_per_s": n / tspan, "service_mean_s": float(np.mean(tsvc))}
         out["sweep"].append({
             "rate_x_plain_capacity": f, "arrivals_per_s": lam, "arrival_span_s": float(arr[-1]),
             "plain": {"p50_s": _pct(pl, 50), "p99_s": _pct(pl, 99), "mean_s": float(np.mean(pl)),
                       "recon_per_s": n / pspan, "service_mean_s": float(np.mean(psvc))},
             "served": {"p50_s": _pct(sl, 50), "p99_s": _pct(sl, 99), "mean_s": float(np.mean(sl)),
                        "recon_per_s": n / sspan, "run_mean_s": float(np.mean([t["run_s"] for t in sinfo]))},
+            **({"plain_tuned": tuned} if tuned else {}),
         })
     return out
 

@@ -49,6 +49,16 @@ struct FftLen {  // POD, passed by value to kernels
     const float2 *tw;  // exp(-2 pi i e / n), e in [0, n)
 };
 
+// Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch.L2, no
+// multicast): the range is shrunk inward to 16-byte boundaries, so only bytes
+// of the given range are touched.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+
 // Complex arithmetic on Blackwell's packed FP32 pair instructions (add / mul /
 // fma .f32x2: one instruction for both halves of a float2, per component the
 // same rounding as the scalar operation).

@@ -434,13 +434,24 @@ constexpr int D2_IB = 8;
 __host__ __device__ constexpr int d2_stride(int L2, int KB) {
     return L2 + ((((16 / KB) - L2) % 16) + 16) % 16;
 }
+// dynamic shared memory of an n2-pass CTA (float2 values): the tile plus the
+// skew of the L2 = 144 layout
+__host__ __device__ constexpr int d2_smem_values(int L2, int KB) {
+    return L2 == 144 ? D2_IB * KB * 145 + (D2_IB * KB / 16 + 1) * 4 : D2_IB * KB * d2_stride(L2, KB);
+}
 
 
 // n2 passes of L2 = 144 (schedule 2, 8, 9): the zero-padded radix-2 stage and the
 // radix-8 stage (two blocks of 72, 9 offsets each) run in registers on the way in
-// (k_dim2_fwd) and their inverses on the way out (k_dim2_inv).  Item (ii, n, kk),
-// kk fastest, holds the values i2 = n + 9 j of tile pencil ii * KB + kk.
+// (k_dim2_fwd) and their inverses on the way out (k_dim2_inv); the radix-9 stage
+// (blocks of 9 positions, no twiddles) runs in registers on the way out to xa
+// (and in from xa), fused with the transpose.  Item (ii, n, kk), kk fastest,
+// holds the values i2 = n + 9 j of tile row kk * 8 + ii; rows are 145 values
+// apart (odd) plus a skew of 4 per 16 rows, so with KB = 4 the 16 lanes of each
+// 8-byte access phase hit distinct banks in the lead (kk x n) and tail (ii x kk)
+// phases.
 constexpr int D2_144_OFS = 9;
+__device__ __forceinline__ int d2_row144(int r) { return r * 145 + (r >> 4) * 4; }
 
 // threads of an n2-pass CTA: one per item of the fused stages for L2 = 144
 __host__ __device__ constexpr int d2_threads(int L2, int KB) {
@@ -475,7 +486,7 @@ __device__ __forceinline__ void dim2_144_load(const float2 *__restrict__ z1, int
                 u[k] = c_mul(u[k], w[k]);
             }
         }
-        float2 *sp = sm + (ii * KB + kk) * ps + n;
+        float2 *sp = sm + d2_row144(kk * D2_IB + ii) + n;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             sp[D2_144_OFS * k] = x[k];
@@ -494,7 +505,7 @@ __device__ __forceinline__ void dim2_144_store(const float2 *__restrict__ sm, in
         const int n = r % D2_144_OFS, ii = r / D2_144_OFS;
         const int i1 = i1b + ii;
         if (kk >= nk || i1 >= n1) continue;
-        const float2 *sp = sm + (ii * KB + kk) * ps + n;
+        const float2 *sp = sm + d2_row144(kk * D2_IB + ii) + n;
         float2 a[8], b[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -519,6 +530,49 @@ __device__ __forceinline__ void dim2_144_store(const float2 *__restrict__ sm, in
                 z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] =
                     c_add(a[j], c_mulc(b[j], __ldg(tw2 + i2)));
         }
+    }
+}
+
+// The radix-9 stage of 144 and the transposing store of its outputs into
+// xa[((c L2 + p2) L3h + k3) n1p + i1]: item (ii, kk, b), ii fastest, so lanes
+// 0..7 write the 8 i1 values of one (p2, k3) run (64 B) for each of the 9
+// outputs p2 = 9 b + k.
+__device__ __forceinline__ void dim2_144_tail_store(const float2 *__restrict__ sm, int L3h, int n1p, int c,
+                                                    int i1b, int k3b, int nk, int KB, float2 *__restrict__ xa,
+                                                    int tid, int nth) {
+    const int64_t pstride = (int64_t)L3h * n1p;
+    for (int t = tid; t < D2_IB * KB * 16; t += nth) {
+        const int ii = t % D2_IB, r = t / D2_IB;
+        const int kk = r % KB, b = r / KB;
+        if (kk >= nk) continue;
+        const float2 *sp = sm + d2_row144(kk * D2_IB + ii) + 9 * b;
+        float2 v[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) v[j] = sp[j];
+        dft_small<9, false>(v);
+        float2 *dst = xa + (((int64_t)c * 144 + 9 * b) * L3h + k3b + kk) * n1p + i1b + ii;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dst[k * pstride] = v[k];
+    }
+}
+
+// its inverse: the transposing load from xa and the inverse radix-9 stage
+__device__ __forceinline__ void dim2_144_tail_load(const float2 *__restrict__ xa, int L3h, int n1p, int c, int i1b,
+                                                   int k3b, int nk, int KB, float2 *__restrict__ sm, int tid,
+                                                   int nth) {
+    const int64_t pstride = (int64_t)L3h * n1p;
+    for (int t = tid; t < D2_IB * KB * 16; t += nth) {
+        const int ii = t % D2_IB, r = t / D2_IB;
+        const int kk = r % KB, b = r / KB;
+        if (kk >= nk) continue;
+        const float2 *src = xa + (((int64_t)c * 144 + 9 * b) * L3h + k3b + kk) * n1p + i1b + ii;
+        float2 v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = src[k * pstride];
+        dft_small<9, true>(v);
+        float2 *sp = sm + d2_row144(kk * D2_IB + ii) + 9 * b;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) sp[j] = v[j];
     }
 }
 
@@ -627,7 +681,7 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
     if constexpr (N2 == 144) {
         dim2_144_load(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm, threadIdx.x, blockDim.x);
         __syncthreads();
-        ct_forward<144, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+        dim2_144_tail_store(sm, L3h, n1p, c, i1b, k3b, nk, KB, xa, threadIdx.x, blockDim.x);
     } else if (F2.ns >= 2) {  // runtime length: the outer stages in registers as well
         LAMINO_DIM2_LEAD(dim2lead_load, F2.radix[1], z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, sm,
                          (int)threadIdx.x, (int)blockDim.x)
@@ -667,15 +721,17 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         __syncthreads();
         fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     }
-    // store: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each,
-    // so a warp writes 8 runs rather than 32
-    for (int t = threadIdx.x; t < L2 * nk * (D2_IB / 2); t += blockDim.x) {
-        const int h = t % (D2_IB / 2), it = t / (D2_IB / 2);
-        const int kk = it % nk, p2 = it / nk;
-        float4 *dst = reinterpret_cast<float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
-        const float2 a = sm[((2 * h) * KB + kk) * ps + p2];
-        const float2 b = sm[((2 * h + 1) * KB + kk) * ps + p2];
-        dst[h] = make_float4(a.x, a.y, b.x, b.y);
+    if constexpr (N2 != 144) {
+        // store: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each,
+        // so a warp writes 8 runs rather than 32
+        for (int t = threadIdx.x; t < L2 * nk * (D2_IB / 2); t += blockDim.x) {
+            const int h = t % (D2_IB / 2), it = t / (D2_IB / 2);
+            const int kk = it % nk, p2 = it / nk;
+            float4 *dst = reinterpret_cast<float4 *>(xa + (((int64_t)c * L2 + p2) * L3h + k3b + kk) * n1p + i1b);
+            const float2 a = sm[((2 * h) * KB + kk) * ps + p2];
+            const float2 b = sm[((2 * h + 1) * KB + kk) * ps + p2];
+            dst[h] = make_float4(a.x, a.y, b.x, b.y);
+        }
     }
 }
 
@@ -817,6 +873,12 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(
     const int half = L1 / 2;
     const int64_t cs = (int64_t)L2 * L3h * n1p;  // component stride in xa
     float2 *pv = xa + pen * n1p;
+    // the pencil's 6 spectra (one contiguous range) start moving into L2 while
+    // the forward transform runs, so the multiply does not wait on HBM
+    if (threadIdx.x == 0) {
+        if constexpr (HALF) prefetch_l2(Kh + pen * 6 * L1, (size_t)6 * L1 * sizeof(__half));
+        else prefetch_l2(K + pen * 6 * L1, (size_t)6 * L1 * sizeof(float));
+    }
     if constexpr (N1 == 1458) {
         p1458_forward(PencilRows{pv, cs, n1}, tw1, sm);
     } else if (F1.ns >= 2) {  // runtime length: the outer stages in registers as well
@@ -993,6 +1055,12 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
     const int nk = min(KB, L3h - k3b);
     const int L2 = N2 ? N2 : F2.n;
     const int ps = d2_stride(L2, KB), half = L2 / 2;
+    if constexpr (N2 == 144) {
+        dim2_144_tail_load(xa, L3h, n1p, c, i1b, k3b, nk, KB, sm, threadIdx.x, blockDim.x);
+        __syncthreads();
+        dim2_144_store(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1, threadIdx.x, blockDim.x);
+        return;
+    }
     // load: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each, so a
     // warp reads 8 runs rather than 32; D2_LD runs in flight per thread
     constexpr int D2_LD = 4;
@@ -1020,11 +1088,6 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
         }
     }
     __syncthreads();
-    if constexpr (N2 == 144) {
-        ct_inverse<144, 2, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
-        dim2_144_store(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1, threadIdx.x, blockDim.x);
-        return;
-    }
     if (F2.ns >= 2) {
         fft_inverse(sm, D2_IB * KB, ps, F2, 2, threadIdx.x, blockDim.x);
         LAMINO_DIM2_LEAD(dim2lead_store, F2.radix[1], sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, z1,
@@ -1336,14 +1399,14 @@ void Toeplitz::finish(cudaStream_t s) {
     xa.alloc(3 * L2 * L3h * n1p);
     rows1 = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / (L3h * (int64_t)sizeof(float2))));
     kb2 = 4;
-    while (kb2 > 1 && D2_IB * kb2 * d2_stride((int)L2, kb2) * (int64_t)sizeof(float2) > 160 * 1024) kb2 /= 2;
-    if (D2_IB * kb2 * d2_stride((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
+    while (kb2 > 1 && d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 160 * 1024) kb2 /= 2;
+    if (d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
         throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
     ct1 = L1 == 1458 ? 1458 : 0;
     ct2 = L2 == 144 ? 144 : 0;
     ct3 = M3 == 729 ? 729 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
+    const int smem_d2 = d2_smem_values((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     auto attr = [](const void *f, int bytes) { raise_smem_limit(f, bytes); };
     attr((const void *)k_r2c_rows<0>, smem_rows);
@@ -1419,7 +1482,7 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     const int64_t nrows = 3 * vol.n1 * vol.n2;
     const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
+    const int smem_d2 = d2_smem_values((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
@@ -1469,7 +1532,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
     const int64_t nrows = 3 * vol.n1 * vol.n2;
     const unsigned grows = (unsigned)((nrows + rows1 - 1) / rows1);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
-    const int smem_d2 = D2_IB * kb2 * d2_stride((int)L2, kb2) * (int)sizeof(float2);
+    const int smem_d2 = d2_smem_values((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
@@ -1496,7 +1559,7 @@ void Toeplitz::set_shape(int rows, int kb) {
     if (rows < 1 || kb < 1) throw Error(ERR_ARG, "launch shape values must be positive");
     if (ct3 && rows > 8) throw Error(ERR_ARG, "rows of 729 run one warp per row, at most 8 per CTA");
     const int64_t smem_rows = (int64_t)rows * L3h * (int64_t)sizeof(float2);
-    const int64_t smem_d2 = (int64_t)D2_IB * kb * d2_stride((int)L2, kb) * (int64_t)sizeof(float2);
+    const int64_t smem_d2 = (int64_t)d2_smem_values((int)L2, kb) * (int64_t)sizeof(float2);
     if (smem_rows > 200 * 1024 || smem_d2 > 200 * 1024) throw Error(ERR_ARG, "launch shape exceeds shared memory");
     rows1 = rows;
     kb2 = kb;

@@ -58,3 +58,15 @@ def test_reference_arm_other_ranks_exit(monkeypatch):
     monkeypatch.setenv("RANK", "1")
     args = bench.argparse.Namespace(steps=1, warmup=1, gpus=2, precision="fp32")
     assert bench.run_reference(args) == 0
+
+
+def test_reference_model_extrapolation():
+    """The reference arm fits t(p) = F + p P to its 1- and 2-projection samples
+    and extrapolates one apply as 4 gammas x (F + 361 P)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    F, P, apply_s = bench.reference_model([(1, 10.0), (2, 12.0), (1, 10.0), (2, 12.0)])
+    assert (F, P) == pytest.approx((8.0, 2.0))
+    assert apply_s == pytest.approx(4 * (8.0 + 361 * 2.0))
+    with pytest.raises(RuntimeError):
+        bench.reference_model([(1, 10.0), (1, 11.0)])
