@@ -691,15 +691,18 @@ def run_recon_form(args):
                                   "511^2 projections, host buffers through lamino_mbir"},
            "data_generation_s": t_data}
     vols = {}
-    for name, kind in (("fp32", "toeplitz"), ("mixed", "mixed")):
-        p = L.ReconParams(maxIters=50, innerIters=3, lam=0.1, mu=10.0, op_kind=kind)
+    forms = [f for f in (("fp32", "toeplitz"), ("mixed", "mixed")) if f[0] in args.recon_forms.split(",")]
+    for name, kind in forms:
+        p = L.ReconParams(maxIters=args.iters, innerIters=3, lam=0.1, mu=10.0, op_kind=kind)
         torch.cuda.synchronize()
         a = time.perf_counter()
         vols[name] = L.MBIR2(data, spec["recon"], p)
         b = time.perf_counter()
         out[name] = {"seconds": b - a, **L.mbir_phases()}
-    d = vols["mixed"].astype(np.float64) - vols["fp32"]
-    out["mixed_vs_fp32_rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(vols["fp32"]))
+    if len(vols) == 2:
+        d = vols["mixed"].astype(np.float64) - vols["fp32"]
+        out["mixed_vs_fp32_rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(vols["fp32"]))
+    out["config"]["outer_iterations"] = args.iters
     print(json.dumps(out), flush=True)
     return 0
 
@@ -738,6 +741,8 @@ def main():
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--rates", default="0.5,1.0,1.5", help="arrival rates, x the plain loop's capacity")
     ap.add_argument("--big-frac", type=float, default=0.0, help="share of README-size requests")
+    ap.add_argument("--iters", type=int, default=50, help="recon form: split-Bregman outer iterations")
+    ap.add_argument("--recon-forms", default="fp32,mixed", help="recon form: fp32, mixed or both")
     args = ap.parse_args()
     if args.form == "served":
         return run_serve_form(args)

@@ -287,6 +287,14 @@ __device__ __forceinline__ void rows27_store(const float2 *__restrict__ sm, int 
     }
 }
 
+// DIF position of packed frequency k: digit reversal of k = k0 + 27 k1 for the
+// 27 x 27 schedule of 729, the table otherwise
+template <int N3>
+__device__ __forceinline__ int row_pos(const int *__restrict__ pos3, int k) {
+    if constexpr (N3 == 729) return 27 * (k % 27) + k / 27;
+    else return __ldg(pos3 + k);
+}
+
 // threads of a rows CTA of R rows: one warp per row for M3 = 729
 __host__ __device__ constexpr int rows_threads(int M3, int R) { return M3 == 729 && R <= 8 ? 32 * R : 256; }
 
@@ -414,8 +422,8 @@ __global__ void __launch_bounds__(256, N3 == 729 ? 3 : 4) k_r2c_rows(const float
         int r = t / (M3 + 1), k = t - r * (M3 + 1);
         int ka = (k == M3) ? 0 : k;
         int kb = (k == 0) ? 0 : M3 - k;
-        float2 Zk = sm[r * ps + __ldg(pos3 + ka)];
-        float2 Zm = sm[r * ps + __ldg(pos3 + kb)];
+        float2 Zk = sm[r * ps + row_pos<N3>(pos3, ka)];
+        float2 Zm = sm[r * ps + row_pos<N3>(pos3, kb)];
         Zm.y = -Zm.y;
         float2 sum = c_add(Zk, Zm), dif = c_sub(Zk, Zm);
         float2 wd = c_mul(__ldg(twh + k), dif);
@@ -561,18 +569,33 @@ __device__ __forceinline__ void dim2_144_tail_load(const float2 *__restrict__ xa
                                                    int k3b, int nk, int KB, float2 *__restrict__ sm, int tid,
                                                    int nth) {
     const int64_t pstride = (int64_t)L3h * n1p;
-    for (int t = tid; t < D2_IB * KB * 16; t += nth) {
-        const int ii = t % D2_IB, r = t / D2_IB;
-        const int kk = r % KB, b = r / KB;
-        if (kk >= nk) continue;
-        const float2 *src = xa + (((int64_t)c * 144 + 9 * b) * L3h + k3b + kk) * n1p + i1b + ii;
-        float2 v[9];
+    const int total = D2_IB * KB * 16;
+    // two items per pass: their 18 loads are in flight together
+    for (int t0 = tid; t0 < total; t0 += 2 * nth) {
+        float2 v[2][9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = src[k * pstride];
-        dft_small<9, true>(v);
-        float2 *sp = sm + d2_row144(kk * D2_IB + ii) + 9 * b;
+        for (int u = 0; u < 2; ++u) {
+            const int t = t0 + u * nth;
+            const int ii = t % D2_IB, r = t / D2_IB;
+            const int kk = r % KB, b = r / KB;
+            if (t < total && kk < nk) {
+                const float2 *src = xa + (((int64_t)c * 144 + 9 * b) * L3h + k3b + kk) * n1p + i1b + ii;
 #pragma unroll
-        for (int j = 0; j < 9; ++j) sp[j] = v[j];
+                for (int k = 0; k < 9; ++k) v[u][k] = src[k * pstride];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int t = t0 + u * nth;
+            const int ii = t % D2_IB, r = t / D2_IB;
+            const int kk = r % KB, b = r / KB;
+            if (t < total && kk < nk) {
+                dft_small<9, true>(v[u]);
+                float2 *sp = sm + d2_row144(kk * D2_IB + ii) + 9 * b;
+#pragma unroll
+                for (int j = 0; j < 9; ++j) sp[j] = v[u][j];
+            }
+        }
     }
 }
 
@@ -1141,7 +1164,7 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
                 float2 xm = make_float2(Xm[u].x, -Xm[u].y);
                 float2 E = c_add(Xk[u], xm);
                 float2 O = c_mulc(c_sub(Xk[u], xm), __ldg(twh + k));
-                sm[r * ps + __ldg(pos3 + k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+                sm[r * ps + row_pos<N3>(pos3, k)] = make_float2(E.x - O.y, E.y + O.x);  // E + i O
             }
         }
     }
