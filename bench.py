@@ -13,10 +13,12 @@ the Toeplitz operator, inputs resident in HBM.  Inputs (443 MB) and spectra
 
 N > 1 runs N independent replicas (one per rank, launched by torchrun); the
 operator has no cross-GPU exchange.  Rank 0 prints one JSON line.  At N = 1 the
-line also carries `served`: p50/p99 reconstruction latency and saturated
-reconstructions/s of the continuous-batching server against the plain
-one-at-a-time FP32 loop on a 16-request stream of uneven NAG + qGGMRF
-reconstructions (--no-served skips it).
+line also carries `nufft`: the NUFFT form's adjoint / forward / sysmat times and
+FP32 rates at half the full size (--no-nufft skips it), and `served`: p50/p99
+reconstruction latency and saturated reconstructions/s of the continuous-
+batching server and the batched form against the plain one-at-a-time FP32 loop
+on a 100-request stream of uneven NAG + qGGMRF reconstructions (--no-served
+skips it).
 
 Other forms (their own JSON line): --form served (the full plain-vs-served
 sweep), --form nufft (NUFFT-form forward / adjoint / sysmat times), --form recon
@@ -196,6 +198,33 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+class UtilSampler:
+    """nvidia-smi utilization.gpu (share of time a kernel was running) sampled
+    every 100 ms while a phase runs; mean of the samples."""
+
+    def __init__(self, gpu_index: int = 0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=utilization.gpu", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(gpu_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        vals = [float(v) for v in self.f.read().split() if v.replace(".", "").isdigit()]
+        os.unlink(self.f.name)
+        return statistics.mean(vals) if vals else None
 
 
 # ---------------------------------------------------------------------------
@@ -385,15 +414,24 @@ def run_ours(args):
         "operator_build_s": build_s,
         "launch_shape": {"rows_per_cta": shape[0], "k3_per_cta": shape[1], "tuned_apply_ms": shape[2]},
     }
+    if rank == 0 and world == 1 and not args.no_nufft:
+        # the NUFFT form's spreading and interpolation (setup adjoints, plain
+        # sysmat) with their FP32 rate, at half the full size
+        nu = nufft_measure(torch, L, "half", 2, 3)
+        line["nufft"] = {k: nu[k] for k in ("workload", "points_per_gamma", "adjoint_ms", "forward_ms",
+                                            "sysmat_sum_gamma_ms", "fp32_tflops", "fp32_peak_tflops",
+                                            "fp32_frac", "fp32_peak_source", "flop_count")}
     if rank == 0 and world == 1 and not args.no_served:
         # the served form against the plain loop on a request stream (one GPU)
-        sv = serve_compare(torch, L, SERVE_LINE_REQUESTS, [0.5, 1.0, 1.5], 2)
+        sv = serve_compare(torch, L, SERVE_LINE_REQUESTS, [0.5, 1.0, 1.5], SERVE_SLOTS)
         line["served"] = {
             "workload": f"{SERVE_LINE_REQUESTS} requests of the mixed-size NAG + qGGMRF stream (thickness "
                         "8-32, lateral 64-256, 2 gammas x 60-240 angles, 40 iterations), Poisson arrivals at "
-                        "0.5 / 1.0 / 1.5 x the plain loop's saturated throughput, 2 slots, 150 GB budget; "
+                        "0.5 / 1.0 / 1.5 x the plain loop's saturated throughput, 3 slots, 150 GB budget; "
                         "plain = one at a time, eager launches, default shapes; plain_tuned = one at a time "
-                        "with the served form's graphs and tuned shapes; all FP32 with FP64 reductions",
+                        "with the served form's graphs and tuned shapes; batched = all requests through "
+                        "lamino_mbir3_batch at once (4 preparer threads, one solver thread); all FP32 with "
+                        "FP64 reductions",
             "rates": [{"rate_x_plain_capacity": r["rate_x_plain_capacity"],
                        "served_p50_s": r["served"]["p50_s"], "served_p99_s": r["served"]["p99_s"],
                        "plain_p50_s": r["plain"]["p50_s"], "plain_p99_s": r["plain"]["p99_s"],
@@ -403,7 +441,11 @@ def run_ours(args):
             "saturated_recon_per_s": sv["saturated"]["served"]["recon_per_s"],
             "plain_saturated_recon_per_s": sv["saturated"]["plain"]["recon_per_s"],
             "plain_tuned_saturated_recon_per_s": sv["saturated"]["plain_tuned"]["recon_per_s"],
-            "max_rel_err_vs_plain": sv["max_rel_err_served_vs_plain"]}
+            "max_rel_err_vs_plain": sv["max_rel_err_served_vs_plain"],
+            **({"batched_saturated_recon_per_s": sv["saturated"]["batched"]["recon_per_s"],
+                "batched_max_rel_err_vs_plain": sv["saturated"]["batched"]["max_rel_err_vs_plain"]}
+               if "batched" in sv["saturated"] else {}),
+            "gpu_utilization_pct_saturated": sv["gpu_utilization_pct_saturated"]}
         at1 = [r for r in sv["sweep"] if r["rate_x_plain_capacity"] == 1.0][0]
         line["served"].update({"p50_s": at1["served"]["p50_s"], "p99_s": at1["served"]["p99_s"],
                                "plain_p50_s": at1["plain"]["p50_s"], "plain_p99_s": at1["plain"]["p99_s"]})
@@ -429,6 +471,8 @@ def run_ours(args):
 SERVE_BUDGET = 150 * 10**9   # HBM bytes the served form may admit at once
 SERVE_ITERS = 40             # NAG + qGGMRF iterations of a mix request
 SERVE_LINE_REQUESTS = 100    # requests of the served summary in the default bench line
+SERVE_BATCH_THREADS = 4      # preparer threads of the batched form
+SERVE_SLOTS = 3              # server slots (requests running at once) of the served line
 
 
 def serve_mix(n: int, seed: int = 7, big_frac: float = 0.0):
@@ -544,6 +588,22 @@ def run_served(L, specs, data, arrivals, slots: int):
     return res, lat, app, span, st, info
 
 
+def run_batched(L, specs, data):
+    """All requests (MBIR3) through the batched form at once (lamino_mbir3_batch:
+    preparer threads under the HBM budget, one thread driving the NAG solves); returns the
+    results, the call's info and its host wall time."""
+    reqs = [(d, sp["recon"], serve_params(L, sp, "served")) for sp, d in zip(specs, data)]
+    t0 = time.perf_counter()
+    res, info = L.mbir3_batch(reqs, SERVE_BUDGET, SERVE_BATCH_THREADS)
+    return res, info, time.perf_counter() - t0
+
+
+def _gpu_index() -> int:
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return int(visible.split(",")[local]) if visible else local
+
+
 def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, seed: int = 7):
     """Plain one-at-a-time loop against the served form on the same request
     stream: saturating throughput (all requests at t = 0), then Poisson
@@ -562,10 +622,29 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
     run_plain_loop(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm))
     run_plain_loop(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), "plain_tuned")
     run_served(L, [specs[i] for i in warm], [data[i] for i in warm], [0.0] * len(warm), slots)
+    if all(sp["method"] == 3 for sp in specs):
+        run_batched(L, [specs[i] for i in warm], [data[i] for i in warm])
     zeros = [0.0] * n
+    util = {}
+    u = UtilSampler(_gpu_index())
     p_res, p_lat, p_svc, p_app, p_span, p_ph = run_plain_loop(L, specs, data, zeros)
+    util["plain"] = u.stop()
+    u = UtilSampler(_gpu_index())
     _, _, _, t_app, t_span, _ = run_plain_loop(L, specs, data, zeros, "plain_tuned")
+    util["plain_tuned"] = u.stop()
+    u = UtilSampler(_gpu_index())
     s_res, s_lat, s_app, s_span, s_st, s_info = run_served(L, specs, data, zeros, slots)
+    util["served"] = u.stop()
+    b_out = None
+    if all(sp["method"] == 3 for sp in specs):
+        u = UtilSampler(_gpu_index())
+        b_res, b_info, b_span = run_batched(L, specs, data)
+        util["batched"] = u.stop()
+        b_err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(b_res, p_res))
+        b_out = {"recon_per_s": n / b_span, "applies_per_s": sum(b_info["applies"]) / b_span, "makespan_s": b_span,
+                 "threads": SERVE_BATCH_THREADS, "peak_live": b_info["peak_live"],
+                 "peak_bytes": b_info["peak_in_use"], "steps": b_info["steps"],
+                 "max_rel_err_vs_plain": b_err}
     errs = [float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)) for a, b in zip(s_res, p_res)]
     nonfinite = sum(int(not np.all(np.isfinite(a))) + int(not np.all(np.isfinite(b))) for a, b in zip(s_res, p_res))
     err = max(errs)
@@ -583,8 +662,10 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
             "plain_tuned": {"recon_per_s": n / t_span, "applies_per_s": sum(t_app) / t_span, "makespan_s": t_span},
             "served": {"recon_per_s": n / s_span, "applies_per_s": sum(s_app) / s_span, "makespan_s": s_span,
                        "peak_active": s_st["peak_active"], "peak_bytes": s_st["peak_in_use"]},
+            **({"batched": b_out} if b_out else {}),
         },
         "max_rel_err_served_vs_plain": err,
+        "gpu_utilization_pct_saturated": util,
         "nonfinite_results": nonfinite,
         "mean_phases": {"plain": phase_means(p_ph), "served": phase_means(s_info)},
         "sweep": [],
@@ -612,29 +693,41 @@ def serve_compare(torch, L, n: int, rates, slots: int, big_frac: float = 0.0, se
     return out
 
 
-def run_nufft_form(args):
+def fp32_peak_tflops(torch) -> float:
+    """Nominal FP32 FMA peak of the device: SMs x 128 lanes x 2 FLOP x the
+    maximum SM clock (148 x 128 x 2 x 1.965 GHz = 74.4 TFLOP/s on B200)."""
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    mhz = 1965.0
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(pynvml.nvmlDeviceGetHandleByIndex(_gpu_index()),
+                                                      pynvml.NVML_CLOCK_SM))
+    except Exception:
+        pass
+    return props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def nufft_measure(torch, L, scale: str, warmup: int, steps: int, bins=None):
     """The plain NUFFT form of the operator at a bench scale: forward and adjoint
     projection of one gamma dataset and the sum-over-gamma sysmat (interp ->
-    weight -> spread per point), CUDA-event timed with inputs in HBM.  The
-    first call of each geometry includes its bin sort (cached afterwards)."""
+    weight -> spread per point), CUDA-event timed with inputs in HBM, with the
+    FP32 rate of the taps.  The first call of each geometry includes its bin
+    sort (cached afterwards)."""
     import numpy as np
-    import torch
-    import lamino_b200 as L
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    L.lib()
-    dims, nproj, det = SCALES[args.scale]
+    dims, nproj, det = SCALES[scale]
     rng = np.random.default_rng(2026)
     pgs = [L.PolarGrid(rng.uniform(0, 2 * np.pi, nproj).astype(np.float32), det, det,
                        np.float32(np.deg2rad(g))) for g in GAMMAS_DEG]
     plan = L.NufftPlan(dims)
-    if args.bins:
-        plan.set_bins(*[int(b) for b in args.bins.split(",")])
+    if bins:
+        plan.set_bins(*bins)
     x = synthetic_magnetization_gpu(torch, dims)
     proj = torch.rand((nproj, det, det), device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
     stream = torch.cuda.current_stream()
 
     def timed(fn, k):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -649,22 +742,38 @@ def run_nufft_form(args):
     L.adjoint(proj, pgs[0], dims, plan=plan)  # includes the bin sort of pgs[0]
     torch.cuda.synchronize()
     t_sort = time.perf_counter() - t_sort
-    k = max(1, args.steps)
+    k = max(1, steps)
     ms_adj = timed(lambda: L.adjoint(proj, pgs[0], dims, plan=plan), k)
     ms_fwd = timed(lambda: L.forward(x, pgs[0], plan=plan), k)
     ms_sys = timed(lambda: L.sysmat(x, pgs, plan=plan), k)
     M = nproj * det * det
     w = 7
-    # interp + spread taps: 3 components x M points x w^3 taps x 2 (interp, spread) x 2 FMA (complex x real)
-    fma_sys = 2 * 3 * (len(pgs) * M) * w ** 3 * 2
-    line = {"form": "nufft", "metric": "NUFFT-form operator times", "unit": "ms", "higher_is_better": False,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"padded volume {dims}, {len(pgs)} gammas x {nproj} angles, {det}^2 projections",
-                       "bins": [int(b) for b in (args.bins or "4,8,16").split(",")]},
-            "points_per_gamma": M, "first_adjoint_incl_sort_s": t_sort,
+    # one spread or one interpolation: 3 components x w^3 taps x 2 FMA (real weight x complex) per point
+    flop_pass = 3 * w ** 3 * 2 * 2 * M
+    peak = fp32_peak_tflops(torch)
+    rate = {"adjoint": flop_pass / (ms_adj / 1e3) / 1e12, "forward": flop_pass / (ms_fwd / 1e3) / 1e12,
+            "sysmat": 2 * len(pgs) * flop_pass / (ms_sys / 1e3) / 1e12}
+    return {"workload": f"padded volume {dims}, {len(pgs)} gammas x {nproj} angles, {det}^2 projections",
+            "bins": list(bins or (4, 8, 16)), "points_per_gamma": M, "first_adjoint_incl_sort_s": t_sort,
             "adjoint_ms": ms_adj, "forward_ms": ms_fwd, "sysmat_sum_gamma_ms": ms_sys,
             "sysmat_applies_per_s": 1e3 / ms_sys,
-            "sysmat_tflops_fp32": 2 * fma_sys / (ms_sys / 1e3) / 1e12}
+            "fp32_tflops": rate, "fp32_peak_tflops": peak,
+            "fp32_frac": {kk: v / peak for kk, v in rate.items()},
+            "fp32_peak_source": "nominal: SMs x 128 FP32 lanes x 2 FLOP x max SM clock",
+            "flop_count": "4116 FLOP per point per spread or interpolation (343 taps x 3 components x 2 FMA)"}
+
+
+def run_nufft_form(args):
+    import torch
+    import lamino_b200 as L
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L.lib()
+    bins = tuple(int(b) for b in args.bins.split(",")) if args.bins else None
+    res = nufft_measure(torch, L, args.scale, args.warmup, args.steps, bins)
+    line = {"form": "nufft", "metric": "NUFFT-form operator times", "unit": "ms", "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": res.pop("workload"), "bins": res.pop("bins")}, **res,
+            "sysmat_tflops_fp32": res["fp32_tflops"]["sysmat"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -731,6 +840,7 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form summary of the apply line")
+    ap.add_argument("--no-nufft", action="store_true", help="skip the NUFFT-form summary of the apply line")
     ap.add_argument("--scale", choices=sorted(SCALES), default="full",
                     help="smaller cases of the same geometry for profiler captures")
     ap.add_argument("--form", choices=["apply", "served", "nufft", "recon"], default="apply",
@@ -738,7 +848,7 @@ def main():
                          "nufft: the NUFFT-form forward / adjoint / sysmat; recon: README-size MBIR2 end to end")
     ap.add_argument("--bins", default="", help="nufft form: fine-grid bin size b1,b2,b3")
     ap.add_argument("--requests", type=int, default=24)
-    ap.add_argument("--slots", type=int, default=2)
+    ap.add_argument("--slots", type=int, default=SERVE_SLOTS)
     ap.add_argument("--rates", default="0.5,1.0,1.5", help="arrival rates, x the plain loop's capacity")
     ap.add_argument("--big-frac", type=float, default=0.0, help="share of README-size requests")
     ap.add_argument("--iters", type=int, default=50, help="recon form: split-Bregman outer iterations")

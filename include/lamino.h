@@ -246,6 +246,28 @@ int lamino_mbir_phases(double *setup_s, double *build_s, double *solve_s, int64_
 int lamino_mbir_footprint(int method, int ndatasets, const int64_t *proj_dims, int64_t r1, int64_t r2, int64_t r3,
                           const lamino_recon_params *params, int64_t *bytes);
 
+/* ---- batched MBIR3 (no reference counterpart; each request is tomocam::MBIR3,
+ * src/mbir3.cpp:47-135) -------------------------------------------------------------
+ * nreq reconstructions of any sizes solved together on the calling device, from
+ * host buffers to host buffers.  Request r has nds[r] datasets; the datasets of
+ * all requests follow one another in projs / proj_dims (3 per dataset) / angles /
+ * gammas, request by request.  recon_dims: 3 per request; params: nreq entries;
+ * out3[r]: [3][recon_dims[3r]][recon_dims[3r+1]][recon_dims[3r+2]] (host).
+ * Preparer threads (`threads`) set requests up in order while the sum of their
+ * estimated footprints (lamino_mbir_footprint) fits in `budget` bytes; the
+ * calling thread drives all prepared NAG solves, each with one line-search step
+ * in flight on its own stream, deciding a step as soon as its reductions have
+ * landed.  Optional outputs: times[2r], times[2r+1] = seconds
+ * after the call started when request r was prepared and finished; counts[2r],
+ * counts[2r+1] = its NAG iterations and normal-operator applications; stats[4] =
+ * peak estimated bytes held, peak requests solving at once, line-search steps,
+ * wall-clock microseconds.  Each result equals lamino_mbir(3, ...) of the same
+ * request. */
+int lamino_mbir3_batch(int nreq, const int *nds, const float *const *projs, const int64_t *proj_dims,
+                       const float *const *angles, const float *gammas, const int64_t *recon_dims,
+                       const lamino_recon_params *params, float *const *out3, int64_t budget, int threads,
+                       double *times, int64_t *counts, int64_t *stats);
+
 /* ---- continuous-batching server (no reference counterpart) ----------------------
  * Requests are MBIR1/2/3 problems as for lamino_mbir (inputs copied at submit).
  * A request is admitted in arrival order as soon as one of `slots` workers is free

@@ -20,7 +20,7 @@ __all__ = [
     "LaminoError", "lib", "PolarGrid", "NufftPlan", "ToeplitzNormal", "beam_dir_vector",
     "forward", "adjoint", "sysmat", "gradient", "residual", "nufft3d1", "nufft3d2",
     "MBIR1", "MBIR2", "MBIR3", "ReconParams", "opt", "padded_volume_dims", "mbir_footprint",
-    "mbir_phases",
+    "mbir_phases", "mbir3_batch",
     "ReconServer",
 ]
 
@@ -89,6 +89,8 @@ def lib():
         "lamino_recon_params_default": ([vp], None),
         "lamino_mbir": ([i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, vp, vp], i32),
         "lamino_mbir_footprint": ([i32, i32, P(i64), i64, i64, i64, vp, P(i64)], i32),
+        "lamino_mbir3_batch": ([i32, P(i32), P(vp), P(i64), P(vp), P(f32), P(i64), vp, P(vp), i64, i32, P(f64),
+                                P(i64), P(i64)], i32),
         "lamino_server_create": ([i64, i32, i32, f64, P(vp)], i32),
         "lamino_server_submit": ([vp, i32, i32, P(vp), P(i64), P(vp), P(f32), i64, i64, i64, vp, P(i64)], i32),
         "lamino_server_wait": ([vp, i64, f64, vp, P(f64), P(f64), P(f64), P(f64)], i32),
@@ -612,6 +614,50 @@ def mbir_footprint(method: int, proj_shapes, recon_dims, params: ReconParams | N
     _check(lib().lamino_mbir_footprint(method, n, dims, *[int(d) for d in recon_dims], ctypes.byref(pc),
                                        ctypes.byref(out)))
     return out.value
+
+
+def mbir3_batch(requests, budget_bytes: int = 150 * 10**9, threads: int = 4):
+    """Batched MBIR3 (no reference counterpart; each request is tomocam::MBIR3,
+    src/mbir3.cpp:47-135): ``requests`` is a list of (datasets, recon_dims,
+    params or None).  Preparer threads set requests up in order under the HBM
+    budget while the calling thread drives every prepared NAG solve, one
+    line-search step in flight per request.  Returns (volumes, info): the (3, r1, r2, r3) results in request order
+    and {"ready_s", "done_s", "iterations", "applies" (per request),
+    "peak_in_use", "peak_live", "steps", "wall_s"}."""
+    nreq = len(requests)
+    keep, outs = [], []
+    all_sets = []
+    nds = (ctypes.c_int * max(nreq, 1))()
+    rdims = (ctypes.c_int64 * max(3 * nreq, 1))()
+    prm = (_ReconParamsC * max(nreq, 1))()
+    outp = (ctypes.c_void_p * max(nreq, 1))()
+    for r, (datasets, recon_dims, params) in enumerate(requests):
+        if len(datasets) == 0:
+            raise ValueError("no datasets")
+        nds[r] = len(datasets)
+        all_sets += list(datasets)
+        rdims[3 * r:3 * r + 3] = [int(d) for d in recon_dims]
+        prm[r] = (params or ReconParams())._c()
+        o = np.empty((3,) + tuple(int(d) for d in recon_dims), dtype=np.float32)
+        outs.append(o)
+        outp[r] = o.ctypes.data
+    if all_sets:
+        _, projs, dims, angs, gam, keep = _datasets_c(all_sets)
+    else:
+        projs, dims, angs, gam = (ctypes.c_void_p * 1)(), (ctypes.c_int64 * 3)(), (ctypes.c_void_p * 1)(), \
+            (ctypes.c_float * 1)()
+    for p in keep:
+        if _is_torch(p) and p.is_cuda:
+            raise TypeError("mbir3_batch takes host inputs (numpy arrays or CPU tensors)")
+    times = (ctypes.c_double * max(2 * nreq, 1))()
+    counts = (ctypes.c_int64 * max(2 * nreq, 1))()
+    stats = (ctypes.c_int64 * 4)()
+    _check(lib().lamino_mbir3_batch(nreq, nds, projs, dims, angs, gam, rdims, prm, outp, int(budget_bytes),
+                                    int(threads), times, counts, stats))
+    info = {"ready_s": [times[2 * r] for r in range(nreq)], "done_s": [times[2 * r + 1] for r in range(nreq)],
+            "iterations": [counts[2 * r] for r in range(nreq)], "applies": [counts[2 * r + 1] for r in range(nreq)],
+            "peak_in_use": stats[0], "peak_live": stats[1], "steps": stats[2], "wall_s": stats[3] * 1e-6}
+    return outs, info
 
 
 class ReconServer:

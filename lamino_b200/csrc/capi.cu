@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/lamino.h"
+#include "batch.cuh"
 #include "demag.cuh"
 #include "server.cuh"
 
@@ -730,6 +731,53 @@ int lamino_mbir_footprint(int method, int nds, const int64_t *pdims, int64_t r1,
     std::vector<std::array<int64_t, 3>> pd;
     for (int i = 0; i < nds; ++i) pd.push_back({pdims[3 * i], pdims[3 * i + 1], pdims[3 * i + 2]});
     *bytes = mbir_footprint(method, pd, dims_of(r1, r2, r3), params_of(params));
+    API_END
+}
+
+int lamino_mbir3_batch(int nreq, const int *nds, const float *const *projs, const int64_t *pdims,
+                       const float *const *angles, const float *gammas, const int64_t *rdims,
+                       const lamino_recon_params *params, float *const *out3, int64_t budget, int threads,
+                       double *times, int64_t *counts, int64_t *stats) {
+    API_BEGIN
+    if (nreq < 0) throw Error(ERR_ARG, "negative request count");
+    if (nreq > 0 && (!nds || !projs || !pdims || !angles || !gammas || !rdims || !params || !out3))
+        throw Error(ERR_ARG, "null argument");
+    std::vector<BatchRequest> reqs((size_t)nreq);
+    int64_t k = 0;  // running dataset index
+    for (int r = 0; r < nreq; ++r) {
+        if (nds[r] <= 0) throw Error(ERR_ARG, "every request needs at least one dataset");
+        BatchRequest &q = reqs[(size_t)r];
+        for (int i = 0; i < nds[r]; ++i, ++k) {
+            const int64_t np = pdims[3 * k], nr = pdims[3 * k + 1], nc = pdims[3 * k + 2];
+            if (np <= 0 || nr <= 0 || nc <= 0) throw Error(ERR_ARG, "projection dims must be positive");
+            if (!projs[k] || !angles[k]) throw Error(ERR_ARG, "null dataset pointer");
+            q.projs.push_back(projs[k]);
+            q.pdims.push_back({np, nr, nc});
+            q.angles.push_back(angles[k]);
+            q.gammas.push_back(gammas[k]);
+        }
+        q.recon = dims_of(rdims[3 * r], rdims[3 * r + 1], rdims[3 * r + 2]);
+        q.prm = params_of(&params[r]);
+        q.out = out3[r];
+    }
+    BatchStats st;
+    mbir3_batch(reqs, budget, threads, &st);
+    for (int r = 0; r < nreq; ++r) {
+        if (times) {
+            times[2 * r] = reqs[(size_t)r].t_ready;
+            times[2 * r + 1] = reqs[(size_t)r].t_done;
+        }
+        if (counts) {
+            counts[2 * r] = reqs[(size_t)r].iterations;
+            counts[2 * r + 1] = reqs[(size_t)r].phases.applies;
+        }
+    }
+    if (stats) {
+        stats[0] = st.peak_in_use;
+        stats[1] = st.peak_live;
+        stats[2] = st.steps;
+        stats[3] = (int64_t)(st.wall_s * 1e6);
+    }
     API_END
 }
 

@@ -130,22 +130,32 @@ MbirPhases &last_mbir_phases() {
     return p;
 }
 
-void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
-          cudaStream_t s) {
+MbirJob::MbirJob(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
+                 cudaStream_t s, cudaStream_t solve_stream)
+    : method_(method), data_(data), recon_(recon), prm_(prm), out3_(out3), s_(s), ss_(solve_stream ? solve_stream : s) {
     if (method < 1 || method > 3) throw Error(ERR_ARG, "method must be 1 (CG), 2 (split Bregman) or 3 (NAG)");
     if (data.empty()) throw Error(ERR_ARG, "no datasets");
-    const Dims3 od = padded_dims(method, recon, prm);
-    const float pfac = proj_pad_factor(method, prm);
-    const int64_t V = od.size(), n = 3 * V;
-    const bool graphs = prm.use_graphs != 0;
-    const double t0 = now_s();
+    od_ = padded_dims(method, recon, prm);
+    V_ = od_.size();
+    n_ = 3 * V_;
+}
+MbirJob::~MbirJob() = default;
 
-    std::unique_ptr<NufftPlan> plan(new NufftPlan(od, prm.eps));
-    const double t_plan = now_s();
-    double t_adj = 0.0, t_tune = 0.0;
-    std::vector<std::unique_ptr<Geom>> geoms;
-    DevBuf<float> yT(n);
-    LAMINO_CUDA(cudaMemsetAsync(yT.p, 0, yT.bytes(), s));
+void MbirJob::prepare() {
+    const int method = method_;
+    const ReconParams &prm = prm_;
+    const std::vector<Dataset> &data = data_;
+    cudaStream_t s = s_;
+    const Dims3 od = od_;
+    const int64_t V = V_, n = n_;
+    const float pfac = proj_pad_factor(method, prm);
+    const bool graphs = prm.use_graphs != 0;
+    t0_ = now_s();
+
+    plan_.reset(new NufftPlan(od, prm.eps));
+    t_plan_ = now_s();
+    yT_.alloc(n);
+    LAMINO_CUDA(cudaMemsetAsync(yT_.p, 0, yT_.bytes(), s));
     Reducer red(8);
     for (const Dataset &ds : data) {
         red.zero(1, s);
@@ -155,145 +165,171 @@ void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const Recon
         DevBuf<float> y;
         int64_t nr, nc;
         normalize_pad2d(ds.proj, ds.nproj, ds.nrows, ds.ncols, mx, pfac, y, nr, nc, s);
-        geoms.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));
+        geoms_.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));
         const double ta = now_s();
-        plan->adjoint(*geoms.back(), y.p, yT.p, true, s);
+        plan_->adjoint(*geoms_.back(), y.p, yT_.p, true, s);
         LAMINO_CUDA(cudaStreamSynchronize(s));
-        t_adj += now_s() - ta;
+        t_adj_ += now_s() - ta;
     }
-    std::vector<const Geom *> gptr;
-    for (auto &g : geoms) gptr.push_back(g.get());
+    for (auto &g : geoms_) gptr_.push_back(g.get());
 
-    const double t_setup = now_s();
+    t_setup_ = now_s();
 
     // normal operator sum_gamma sysmat; MBIR3 also needs one operator per gamma
     // for its loss, and then the sum is formed from their spectra
-    std::unique_ptr<Toeplitz> T;
-    std::vector<std::unique_ptr<Toeplitz>> Tg;
-    OpFn A_raw, A_lo_raw;
-    std::vector<OpFn> Ag;
     const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
     if (prm.op_kind == OP_NUFFT) {
-        NufftPlan *pl = plan.get();
+        NufftPlan *pl = plan_.get();
         if (prm.autotune) {
             const double tt = now_s();
-            pl->autotune_bins(gptr, 1, s);
-            t_tune += now_s() - tt;
+            pl->autotune_bins(gptr_, 1, s);
+            t_tune_ += now_s() - tt;
         }
-        A_raw = [pl, &gptr](const float *x, float *y, cudaStream_t st) { pl->normal(gptr, x, y, st); };
+        A_raw_ = [pl, this](const float *x, float *y, cudaStream_t st) { pl->normal(gptr_, x, y, st); };
         if (method == 3)
-            for (const Geom *g : gptr)
-                Ag.push_back([pl, g](const float *xx, float *yy, cudaStream_t st) { pl->normal({g}, xx, yy, st); });
+            for (const Geom *g : gptr_)
+                Ag_.push_back([pl, g](const float *xx, float *yy, cudaStream_t st) { pl->normal({g}, xx, yy, st); });
     } else {
-        plan.reset();  // the fine grids are only needed for the setup adjoints
+        plan_.reset();  // the fine grids are only needed for the setup adjoints
         int prec = prm.op_kind == OP_TOEPLITZ_FP16 ? PREC_FP16 : (mixed ? PREC_MIXED : PREC_FP32);
         if (method == 3) {
-            std::vector<const Toeplitz *> parts;
-            for (const Geom *g : gptr) {
-                Tg.emplace_back(new Toeplitz({g}, od, PREC_FP32, s));
-                Tg.back()->drop_work();  // kept for its spectra (loss quadratic forms, the sum)
-                parts.push_back(Tg.back().get());
+            for (const Geom *g : gptr_) {
+                Tg_.emplace_back(new Toeplitz({g}, od, PREC_FP32, s));
+                Tg_.back()->drop_work();  // kept for its spectra (loss quadratic forms, the sum)
+                parts_.push_back(Tg_.back().get());
             }
-            T.reset(new Toeplitz(parts, prec, s));
+            T_.reset(new Toeplitz(parts_, prec, s));
         } else {
-            T.reset(new Toeplitz(gptr, od, prec, s));
+            T_.reset(new Toeplitz(gptr_, od, prec, s));
         }
-        Toeplitz *tp = T.get();
+        Toeplitz *tp = T_.get();
         if (prm.autotune) {
             const double tt = now_s();
             tp->autotune(s);
-            t_tune += now_s() - tt;
+            t_tune_ += now_s() - tt;
         }
-        A_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, false); };
-        if (mixed) A_lo_raw = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, true); };
+        A_raw_ = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, false); };
+        if (mixed) A_lo_raw_ = [tp](const float *x, float *y, cudaStream_t st) { tp->apply(x, y, st, true); };
     }
-    GraphedOp gA(A_raw, graphs), gA_lo(A_lo_raw ? A_lo_raw : A_raw, graphs);
-    OpFn A = gA.as_fn();
-    OpFn A_lo = mixed ? gA_lo.as_fn() : OpFn();
+    gA_.reset(new GraphedOp(A_raw_, graphs));
+    gA_lo_.reset(new GraphedOp(A_lo_raw_ ? A_lo_raw_ : A_raw_, graphs));
 
-    DevBuf<float> x(n);
-    LAMINO_CUDA(cudaMemsetAsync(x.p, 0, x.bytes(), s));
+    x_.alloc(n);
+    LAMINO_CUDA(cudaMemsetAsync(x_.p, 0, x_.bytes(), s));
     LAMINO_CUDA(cudaStreamSynchronize(s));
-    const double t_build = now_s();
-    int64_t extra_applies = 0;
-    if (method == 1) {
+    t_build_ = now_s();
+    if (method != 3) return;  // s has drained: the solve stream needs no wait
+
+    red.zero(1, s);
+    vec_dot(yT_.p, yT_.p, n, red.d, s);
+    red.fetch(1, s);
+    const double yTy = red.h[0];
+    const float ng = (float)gptr_.size();
+    // gradient: sum_gamma (sysmat x - yT) + qGGMRF (src/mbir3.cpp:91-103), one graph per input
+    gGrad_.reset(new GraphedOp(
+        [this, ng, n, V](const float *xx, float *g, cudaStream_t st) {
+            A_raw_(xx, g, st);
+            k_axpy_scalar<<<grid_for(n, 256), 256, 0, st>>>(g, -ng, yT_.p, n);
+            LAMINO_LAUNCH("k_axpy_scalar");
+            for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od_, prm_.sigma, prm_.p, st);
+        },
+        graphs));
+    GradFn grad = [this](const float *xx, float *g, cudaStream_t st) {
+        (*gGrad_)(xx, g, st);
+        ++extra_applies_;
+    };
+    // loss (src/mbir3.cpp:108-116): sum over gamma and component of
+    // sqrt(x_i . S_g x_i - 2 x_i . yT_i + yTy).  Toeplitz forms get every
+    // x_i . S_g x_i from one forward half-spectrum of x (Parseval); the NUFFT
+    // form applies each S_g.  The terms land in the caller's (zeroed) device
+    // slots; the graph is keyed by (input, slot) pointers.
+    const int ngi = (int)gptr_.size();
+    if (!T_) Sx_.alloc(n);
+    gLoss_.reset(new GraphedOp(
+        [this, ngi, V](const float *xx, float *slot, cudaStream_t st) {
+            double *acc = reinterpret_cast<double *>(slot);
+            if (T_) {
+                T_->quadforms(xx, parts_, acc, st);
+            } else {
+                for (int q = 0; q < ngi; ++q) {
+                    Ag_[q](xx, Sx_.p, st);
+                    for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, Sx_.p + i * V, V, acc + 3 * q + i, st);
+                }
+            }
+            for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, yT_.p + i * V, V, acc + 3 * ngi + i, st);
+        },
+        graphs));
+    LossTerms loss;
+    loss.nterms = 3 * ngi + 3;
+    loss.enqueue = [this, ngi](const float *xx, double *acc, cudaStream_t st) {
+        (*gLoss_)(xx, reinterpret_cast<float *>(acc), st);
+        extra_applies_ += T_ ? 0 : ngi;
+    };
+    loss.value = [ngi, yTy](const double *h) {
+        double e = 0.0;
+        for (int q = 0; q < ngi; ++q)
+            for (int i = 0; i < 3; ++i) e += std::sqrt(h[3 * q + i] - 2.0 * h[3 * ngi + i] + yTy);
+        return e;
+    };
+    float lip = prm.mu;
+    if (!(lip > 0.f)) {  // estimate: 30 power iterations of sum_gamma sysmat (qGGMRF curvature neglected)
+        lip = (float)lipschitz(gA_->as_fn(), od, 30, 0.0, 12345ULL, s);
+        if (!(lip > 0.f)) lip = 1.f;
+    }
+    if (ss_ != s) {  // the solve stream starts after the work queued on s
+        cudaEvent_t ev;
+        LAMINO_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        LAMINO_CUDA(cudaEventRecord(ev, s));
+        LAMINO_CUDA(cudaStreamWaitEvent(ss_, ev, 0));
+        LAMINO_CUDA(cudaEventDestroy(ev));
+    }
+    nag_.reset(new NagSolve(grad, loss, x_.p, od, prm.max_iters, lip, prm.tol, prm.xtol, prm.inner_iters, ss_));
+}
+
+void MbirJob::solve() {
+    const ReconParams &prm = prm_;
+    cudaStream_t s = ss_;
+    const bool mixed = prm.op_kind == OP_TOEPLITZ_MIXED;
+    OpFn A = gA_->as_fn();
+    OpFn A_lo = mixed ? gA_lo_->as_fn() : OpFn();
+    if (method_ == 1) {
         if (mixed) {
             int R = std::max(1, prm.refinements);
-            cgsolver_refined(A, A_lo, yT.p, x.p, od, std::max(1, prm.max_iters / R), R, prm.tol, s);
+            cgsolver_refined(A, A_lo, yT_.p, x_.p, od_, std::max(1, prm.max_iters / R), R, prm.tol, s);
         } else {
-            cgsolver(A, yT.p, x.p, od, prm.max_iters, prm.tol, s);
+            cgsolver(A, yT_.p, x_.p, od_, prm.max_iters, prm.tol, s);
         }
-    } else if (method == 2) {
-        split_bregman_refined(A, A_lo, mixed ? std::max(1, prm.refinements) : 0, yT.p, x.p, od, prm.lambda, prm.mu,
+    } else if (method_ == 2) {
+        split_bregman_refined(A, A_lo, mixed ? std::max(1, prm.refinements) : 0, yT_.p, x_.p, od_, prm.lambda, prm.mu,
                               prm.max_iters, prm.inner_iters, prm.tol, prm.xtol, s);
     } else {
-        red.zero(1, s);
-        vec_dot(yT.p, yT.p, n, red.d, s);
-        red.fetch(1, s);
-        const double yTy = red.h[0];
-        const float ng = (float)gptr.size();
-        // gradient: sum_gamma (sysmat x - yT) + qGGMRF (src/mbir3.cpp:91-103), one graph per input
-        GraphedOp gGrad(
-            [&](const float *xx, float *g, cudaStream_t st) {
-                A_raw(xx, g, st);
-                k_axpy_scalar<<<grid_for(n, 256), 256, 0, st>>>(g, -ng, yT.p, n);
-                LAMINO_LAUNCH("k_axpy_scalar");
-                for (int i = 0; i < 3; ++i) qggmrf_add(g + i * V, xx + i * V, od, prm.sigma, prm.p, st);
-            },
-            graphs);
-        GradFn grad = [&](const float *xx, float *g, cudaStream_t st) {
-            gGrad(xx, g, st);
-            ++extra_applies;
-        };
-        // loss (src/mbir3.cpp:108-116): sum over gamma and component of
-        // sqrt(x_i . S_g x_i - 2 x_i . yT_i + yTy).  Toeplitz forms get every
-        // x_i . S_g x_i from one forward half-spectrum of x (Parseval); the NUFFT
-        // form applies each S_g.  Device slots, one graph per input, one fetch.
-        const int ngi = (int)gptr.size();
-        std::vector<const Toeplitz *> parts;
-        for (auto &t : Tg) parts.push_back(t.get());
-        DevBuf<float> Sx(T ? 0 : n);
-        Reducer lr(3 * ngi + 3);
-        GraphedOp gLoss(
-            [&](const float *xx, float *, cudaStream_t st) {
-                lr.zero(3 * ngi + 3, st);
-                if (T) {
-                    T->quadforms(xx, parts, lr.d, st);
-                } else {
-                    for (int q = 0; q < ngi; ++q) {
-                        Ag[q](xx, Sx.p, st);
-                        for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, Sx.p + i * V, V, lr.d + 3 * q + i, st);
-                    }
-                }
-                for (int i = 0; i < 3; ++i) vec_dot(xx + i * V, yT.p + i * V, V, lr.d + 3 * ngi + i, st);
-            },
-            graphs);
-        LossFn loss = [&](const float *xx, cudaStream_t st) {
-            gLoss(xx, nullptr, st);
-            extra_applies += T ? 0 : ngi;
-            lr.fetch(3 * ngi + 3, st);
-            double e = 0.0;
-            for (int q = 0; q < ngi; ++q)
-                for (int i = 0; i < 3; ++i) e += std::sqrt(lr.h[3 * q + i] - 2.0 * lr.h[3 * ngi + i] + yTy);
-            return e;
-        };
-        float lip = prm.mu;
-        if (!(lip > 0.f)) {  // estimate: 30 power iterations of sum_gamma sysmat (qGGMRF curvature neglected)
-            lip = (float)lipschitz(A, od, 30, 0.0, 12345ULL, s);
-            if (!(lip > 0.f)) lip = 1.f;
+        while (!nag_->done()) {
+            nag_->enqueue();
+            LAMINO_CUDA(cudaStreamSynchronize(s));
+            nag_->finish();
         }
-        nagopt(grad, loss, x.p, od, prm.max_iters, lip, prm.tol, prm.xtol, prm.inner_iters, s);
     }
-    crop3d3(x.p, od, recon, out3, s);
-    LAMINO_CUDA(cudaStreamSynchronize(s));
+}
+
+void MbirJob::finish() {
+    crop3d3(x_.p, od_, recon_, out3_, ss_);
+    LAMINO_CUDA(cudaStreamSynchronize(ss_));
     MbirPhases &ph = last_mbir_phases();
-    ph.setup_s = t_setup - t0;
-    ph.build_s = t_build - t_setup;
-    ph.solve_s = now_s() - t_build;
-    ph.applies = gA.calls() + gA_lo.calls() + extra_applies;
-    ph.plan_s = t_plan - t0;
-    ph.adjoint_s = t_adj;
-    ph.tune_s = t_tune;
+    ph.setup_s = t_setup_ - t0_;
+    ph.build_s = t_build_ - t_setup_;
+    ph.solve_s = now_s() - t_build_;
+    ph.applies = gA_->calls() + gA_lo_->calls() + extra_applies_;
+    ph.plan_s = t_plan_ - t0_;
+    ph.adjoint_s = t_adj_;
+    ph.tune_s = t_tune_;
+}
+
+void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
+          cudaStream_t s) {
+    MbirJob job(method, data, recon, prm, out3, s);
+    job.prepare();
+    job.solve();
+    job.finish();
 }
 
 }  // namespace lamino

@@ -63,4 +63,51 @@ MbirPhases &last_mbir_phases();
 void mbir(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
           cudaStream_t s);
 
+class GraphedOp;
+// One reconstruction in three parts: prepare() (normalisation, padding, grids,
+// setup adjoints, operators; for MBIR3 also the Lipschitz constant and the NAG
+// state), the solve, finish() (crop into out3, phase times).  mbir() runs the
+// three in a row; the batched form steps several MBIR3 solves together.
+// prepare() runs on stream s; the solve and finish() on solve_stream (s when
+// null), which waits for the end of prepare().  Buffers allocated while an
+// AllocStreamScope is active are freed on their allocation stream when the
+// job is destroyed, after finish() has synchronised the solve stream.
+class MbirJob {
+  public:
+    MbirJob(int method, const std::vector<Dataset> &data, Dims3 recon, const ReconParams &prm, float *out3,
+            cudaStream_t s, cudaStream_t solve_stream = nullptr);
+    ~MbirJob();
+    MbirJob(const MbirJob &) = delete;
+    MbirJob &operator=(const MbirJob &) = delete;
+    void prepare();
+    void solve();
+    void finish();
+    int method() const { return method_; }
+    NagSolve *nag() { return nag_.get(); }
+    cudaStream_t solve_stream() const { return ss_; }
+
+  private:
+    int method_;
+    std::vector<Dataset> data_;
+    Dims3 recon_, od_;
+    ReconParams prm_;
+    float *out3_;
+    cudaStream_t s_, ss_;
+    int64_t V_ = 0, n_ = 0;
+    std::unique_ptr<NufftPlan> plan_;
+    std::vector<std::unique_ptr<Geom>> geoms_;
+    std::vector<const Geom *> gptr_;
+    DevBuf<float> yT_, x_, Sx_;
+    std::unique_ptr<Toeplitz> T_;
+    std::vector<std::unique_ptr<Toeplitz>> Tg_;
+    std::vector<const Toeplitz *> parts_;
+    OpFn A_raw_, A_lo_raw_;
+    std::vector<OpFn> Ag_;
+    std::unique_ptr<GraphedOp> gA_, gA_lo_, gGrad_, gLoss_;
+    std::unique_ptr<NagSolve> nag_;
+    int64_t extra_applies_ = 0;
+    double t0_ = 0, t_plan_ = 0, t_setup_ = 0, t_build_ = 0, t_adj_ = 0, t_tune_ = 0;
+};
+
+
 }  // namespace lamino

@@ -112,21 +112,35 @@ struct Fine {
     float beta;
 };
 
+// first tap of a coordinate on the fine grid (wrapped) and its offset d0 in
+// [-W/2, -W/2 + 1) from the coordinate, in grid units
 template <int W>
-__device__ __forceinline__ int es_taps(float xc, int nf, double s, float beta, float *wt) {
+__device__ __forceinline__ int es_start(float xc, int nf, double s, float &d0) {
     double u = (double)xc * s;
     double l0 = ceil(u - 0.5 * W);
-    float d0 = (float)(l0 - u);  // in [-W/2, -W/2 + 1)
+    d0 = (float)(l0 - u);
+    int64_t l = (int64_t)l0;
+    l %= nf;
+    if (l < 0) l += nf;
+    return (int)l;
+}
+
+template <int W>
+__device__ __forceinline__ void es_weights(float d0, float beta, float *wt) {
 #pragma unroll
     for (int t = 0; t < W; ++t) {
         float a = (d0 + (float)t) * (2.0f / W);
         float q = 1.0f - a * a;
         wt[t] = q > 0.f ? expf(beta * (sqrtf(q) - 1.0f)) : 0.f;
     }
-    int64_t l = (int64_t)l0;
-    l %= nf;
-    if (l < 0) l += nf;
-    return (int)l;
+}
+
+template <int W>
+__device__ __forceinline__ int es_taps(float xc, int nf, double s, float beta, float *wt) {
+    float d0;
+    const int l = es_start<W>(xc, nf, s, d0);
+    es_weights<W>(d0, beta, wt);
+    return l;
 }
 
 // deconvolve + place modes into the (zero) fine grid; real volume input
@@ -520,58 +534,105 @@ constexpr size_t point_rec_bytes(int w, int nc) { return (size_t)((12 + 12 * w +
 static_assert(sizeof(PointRec<7, 3>) == point_rec_bytes(7, 3), "record layout");
 static_assert(sizeof(PointRec<8, 1>) == point_rec_bytes(8, 1), "record layout");
 
+// Records of a staged chunk in slab order.  Every CTA of the binned kernels
+// runs kStageChunk threads, one point each.  A point whose taps fit in the
+// bin's tile starts at tile slab a1 in [0, b1) (bkt = a1; -1 otherwise); its
+// record goes to position bstart[a1] + (its rank among the chunk's points with
+// that a1, in point order), so records are sorted by a1 and the sum into every
+// cell runs in a fixed order.  The ranks come from one ballot per slab start,
+// the offsets from a scan over warps and starts by warp 0.  Returns the
+// record position (-1 for bkt < 0); called by every thread of the CTA.
+constexpr int kMaxB1 = 16;                       // largest bin extent along n1
+constexpr int kStageWarps = kStageChunk / 32;
+__device__ __forceinline__ int place_slot(int bkt, int *wcnt, int *bstart, const BinLayout &B) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int rank = 0;
+    for (int b = 0; b < B.b1; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, bkt == b);
+        if (bkt == b) rank = __popc(m & ((1u << lane) - 1u));
+        if (lane == 0) wcnt[warp * kMaxB1 + b] = __popc(m);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int tot = 0;
+        if (lane < B.b1)
+            for (int v = 0; v < kStageWarps; ++v) {
+                const int c = wcnt[v * kMaxB1 + lane];
+                wcnt[v * kMaxB1 + lane] = tot;
+                tot += c;
+            }
+        int incl = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        if (lane < B.b1) {
+            const int excl = incl - tot;
+            for (int v = 0; v < kStageWarps; ++v) wcnt[v * kMaxB1 + lane] += excl;
+            bstart[lane] = excl;
+            if (lane == B.b1 - 1) bstart[B.b1] = incl;
+        }
+    }
+    __syncthreads();
+    return bkt >= 0 ? wcnt[warp * kMaxB1 + bkt] + rank : -1;
+}
+
 // Spread the staged points into the tile without atomics: warp v owns the tile
-// slabs i1 = v, v + nwarps, ... and applies every staged point's taps that fall
-// in its slabs, its lanes covering the point's w x w (t2, t3) taps, so each
-// cell has one writer and the order of the sums is fixed.
+// slabs i1 = v, v + nwarps, ... and, slab by slab, applies the taps of the
+// points that reach the slab (those with a1 in [slab - w + 1, slab], one run
+// of the sorted records), its lanes covering a point's w x w (t2, t3) taps.
+// Each cell has one writer and its sum runs in record order.  The NR x NC
+// read-modify-writes of one point touch distinct cells, so their loads are
+// issued together, then the FMAs, then the stores.
 template <int W, int NC>
-__device__ __forceinline__ void spread_staged(float2 *tile, int tsz, const BinLayout &B,
-                                              const PointRec<W, NC> *recs, int n) {
+__device__ __forceinline__ void spread_sorted(float2 *tile, int tsz, const BinLayout &B,
+                                              const PointRec<W, NC> *recs, const int *bstart) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     constexpr int NT = W * W;
     constexpr int NR = (NT + 31) / 32;
-    int t2s[NR], t3s[NR];
+    int t2s[NR], t3s[NR], loff[NR];
+    bool act[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         const int q = lane + 32 * r;
-        t2s[r] = q < NT ? q / W : -1;
-        t3s[r] = q < NT ? q - (q / W) * W : 0;
+        act[r] = q < NT;
+        t2s[r] = act[r] ? q / W : 0;
+        t3s[r] = act[r] ? q - (q / W) * W : 0;
+        loff[r] = t2s[r] * B.r3 + t3s[r];
     }
     const int slab_stride = B.t2 * B.r3;
-    for (int q = 0; q < n; ++q) {
-        const PointRec<W, NC> &pr = recs[q];
-        const int a1 = pr.a1;
-        // this warp's slabs hit by the point (warp-uniform)
-        bool any = false;
-        for (int slab = warp; slab < B.t1; slab += nwarps) any |= (unsigned)(slab - a1) < (unsigned)W;
-        if (!any) continue;
-        float2 s[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) s[c] = pr.s[c];
-        float w23[NR];
-        int off[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            const int t2 = t2s[r] < 0 ? 0 : t2s[r];
-            w23[r] = t2s[r] < 0 ? 0.f : pr.w2[t2] * pr.w3[t3s[r]];
-            off[r] = (pr.a2 + t2) * B.r3 + pr.a3 + t3s[r];
-        }
-        for (int slab = warp; slab < B.t1; slab += nwarps) {
-            const int t1 = slab - a1;
-            if ((unsigned)t1 >= (unsigned)W) continue;
-            const float w1v = pr.w1[t1];
-            float2 *srow = tile + slab * slab_stride;
+    for (int slab = warp; slab < B.t1; slab += nwarps) {
+        const int lo = max(0, slab - (W - 1)), hi = min(B.b1 - 1, slab);
+        if (lo > hi) continue;
+        const int q1 = bstart[hi + 1];
+        float2 *srow = tile + slab * slab_stride;
+        for (int q = bstart[lo]; q < q1; ++q) {
+            const PointRec<W, NC> &pr = recs[q];
+            const float w1v = pr.w1[slab - pr.a1];
+            float2 *cell0 = srow + pr.a2 * B.r3 + pr.a3;
+            float wt[NR];
+            float2 v[NR][NC];
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                if (t2s[r] < 0) continue;
-                const float wt = w1v * w23[r];
-                float2 *cp = srow + off[r];
+                wt[r] = w1v * (pr.w2[t2s[r]] * pr.w3[t3s[r]]);
+                if (act[r]) {
 #pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    float2 v = cp[c * tsz];
-                    v.x = fmaf(wt, s[c].x, v.x);
-                    v.y = fmaf(wt, s[c].y, v.y);
-                    cp[c * tsz] = v;
+                    for (int c = 0; c < NC; ++c) v[r][c] = cell0[loff[r] + c * tsz];
+                }
+            }
+            float2 sv[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sv[c] = pr.s[c];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                if (act[r]) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        v[r][c].x = fmaf(wt[r], sv[c].x, v[r][c].x);
+                        v[r][c].y = fmaf(wt[r], sv[c].y, v[r][c].y);
+                        cell0[loff[r] + c * tsz] = v[r][c];
+                    }
                 }
             }
         }
@@ -592,7 +653,7 @@ __device__ __forceinline__ void flush_tile(const float2 *tile, int tsz, const Bi
 }
 
 template <int W, int NC, class Str>
-__global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_t *__restrict__ perm,
+__global__ void __launch_bounds__(kStageChunk, 2) k_spread_binned(GeomView g, const uint32_t *__restrict__ perm,
                                                        const uint32_t *__restrict__ start, BinLayout B, Fine F,
                                                        float2 *__restrict__ H, int64_t NF, Str str) {
     extern __shared__ float2 tile[];
@@ -603,30 +664,44 @@ __global__ void __launch_bounds__(256) k_spread_binned(GeomView g, const uint32_
     const int tsz = (int)B.tile_cells();
     PointRec<W, NC> *recs = reinterpret_cast<PointRec<W, NC> *>(tile + NC * tsz);
     for (int i = threadIdx.x; i < NC * tsz; i += blockDim.x) tile[i] = make_float2(0.f, 0.f);
+    __shared__ int wcnt[kStageWarps * kMaxB1];
+    __shared__ int bstart[kMaxB1 + 1];
     for (uint32_t base = p0; base < p1; base += kStageChunk) {
         const int n = (int)min((uint32_t)kStageChunk, p1 - base);
-        for (int t = threadIdx.x; t < n; t += blockDim.x) {
-            const uint32_t pid = __ldg(perm + base + t);
-            int p, j, k;
+        const int t = threadIdx.x;  // one point per thread (blockDim.x == kStageChunk)
+        uint32_t pid = 0;
+        int p = 0, j = 0, k = 0, a1 = -1, a2 = 0, a3 = 0;
+        float x = 0.f, y = 0.f, z = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+        bool in = false;
+        if (t < n) {
+            pid = __ldg(perm + base + t);
             decode_pid(pid, g, p, j, k);
-            PointRec<W, NC> &pr = recs[t];
+            point_xyz(g, p, j, k, x, y, z);
+            a3 = es_start<W>(x, F.nf3, F.s3, d3) - o.o3;
+            a2 = es_start<W>(y, F.nf2, F.s2, d2) - o.o2;
+            a1 = es_start<W>(z, F.nf1, F.s1, d1) - o.o1;
+            in = (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
+        }
+        const int pos = place_slot(in ? a1 : -1, wcnt, bstart, B);
+        if (t < n) {
             float2 s[NC];
             str(g, p, j, k, pid, s);
-            float x, y, z;
-            int a1, a2, a3;
-            if (point_taps<W>(g, F, B, o, p, j, k, pr.w1, pr.w2, pr.w3, a1, a2, a3, x, y, z)) {
+            if (in) {
+                PointRec<W, NC> &pr = recs[pos];
                 pr.a1 = a1;
                 pr.a2 = a2;
                 pr.a3 = a3;
+                es_weights<W>(d1, F.beta, pr.w1);
+                es_weights<W>(d2, F.beta, pr.w2);
+                es_weights<W>(d3, F.beta, pr.w3);
 #pragma unroll
                 for (int c = 0; c < NC; ++c) pr.s[c] = s[c];
             } else {
-                pr.a1 = -(1 << 20);  // matches no slab
                 spread_point_global<W, NC>(H, NF, F, x, y, z, s);
             }
         }
         __syncthreads();
-        spread_staged<W, NC>(tile, tsz, B, recs, n);
+        spread_sorted<W, NC>(tile, tsz, B, recs, bstart);
         __syncthreads();
     }
     flush_tile<NC>(tile, tsz, B, o, F, H, NF);
@@ -668,7 +743,7 @@ __global__ void __launch_bounds__(256) k_interp_binned(GeomView g, const uint32_
 // per point), combine with the beam vector, stage, then spread into the output
 // tile as k_spread_binned (src/gradient.cpp:34-89)
 template <int W>
-__global__ void __launch_bounds__(256) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
+__global__ void __launch_bounds__(kStageChunk, 2) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
                                                        const uint32_t *__restrict__ start, BinLayout B, Fine F,
                                                        const float2 *__restrict__ G, float2 *__restrict__ H,
                                                        int64_t NF, float inv_scale) {
@@ -686,19 +761,38 @@ __global__ void __launch_bounds__(256) k_sysmat_binned(GeomView g, const uint32_
         ht[i] = make_float2(0.f, 0.f);
     }
     __syncthreads();
+    __shared__ int wcnt[kStageWarps * kMaxB1];
+    __shared__ int bstart[kMaxB1 + 1];
     for (uint32_t base = p0; base < p1; base += kStageChunk) {
         const int n = (int)min((uint32_t)kStageChunk, p1 - base);
-        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int t = threadIdx.x;  // one point per thread (blockDim.x == kStageChunk)
+        int p = 0, j = 0, k = 0, a1 = -1, a2 = 0, a3 = 0;
+        float x = 0.f, y = 0.f, z = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+        bool in = false;
+        if (t < n) {
             const uint32_t pid = __ldg(perm + base + t);
-            int p, j, k;
             decode_pid(pid, g, p, j, k);
-            PointRec<W, 3> &pr = recs[t];
-            float x, y, z;
-            int a1, a2, a3;
-            const bool in = point_taps<W>(g, F, B, o, p, j, k, pr.w1, pr.w2, pr.w3, a1, a2, a3, x, y, z);
+            point_xyz(g, p, j, k, x, y, z);
+            a3 = es_start<W>(x, F.nf3, F.s3, d3) - o.o3;
+            a2 = es_start<W>(y, F.nf2, F.s2, d2) - o.o2;
+            a1 = es_start<W>(z, F.nf1, F.s1, d1) - o.o1;
+            in = (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
+        }
+        const int pos = place_slot(in ? a1 : -1, wcnt, bstart, B);
+        if (t < n) {
             float2 v[3];
-            if (in) gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, pr.w1, pr.w2, pr.w3, v);
-            else interp_point_global<W, 3>(G, NF, F, x, y, z, v);
+            if (in) {
+                PointRec<W, 3> &pr = recs[pos];
+                pr.a1 = a1;
+                pr.a2 = a2;
+                pr.a3 = a3;
+                es_weights<W>(d1, F.beta, pr.w1);
+                es_weights<W>(d2, F.beta, pr.w2);
+                es_weights<W>(d3, F.beta, pr.w3);
+                gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, pr.w1, pr.w2, pr.w3, v);
+            } else {
+                interp_point_global<W, 3>(G, NF, F, x, y, z, v);
+            }
             const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p),
                         c2 = __ldg(g.coeff + 2 * g.nproj + p);
             const float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
@@ -706,18 +800,14 @@ __global__ void __launch_bounds__(256) k_sysmat_binned(GeomView g, const uint32_
             const float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
                                  make_float2(c2 * sr, c2 * si)};
             if (in) {
-                pr.a1 = a1;
-                pr.a2 = a2;
-                pr.a3 = a3;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) pr.s[c] = s[c];
+                for (int c = 0; c < 3; ++c) recs[pos].s[c] = s[c];
             } else {
-                pr.a1 = -(1 << 20);  // matches no slab
                 spread_point_global<W, 3>(H, NF, F, x, y, z, s);
             }
         }
         __syncthreads();
-        spread_staged<W, 3>(ht, tsz, B, recs, n);
+        spread_sorted<W, 3>(ht, tsz, B, recs, bstart);
         __syncthreads();
     }
     flush_tile<3>(ht, tsz, B, o, F, H, NF);
@@ -851,6 +941,7 @@ static void with_width(int w, Fn &&fn) {
 
 void NufftPlan::set_bins(int b1, int b2, int b3) {
     if (b1 <= 0 || b2 <= 0 || b3 <= 0) throw Error(ERR_ARG, "bin sizes must be positive");
+    if (b1 > kMaxB1) throw Error(ERR_ARG, "bin extent along n1 must be at most 16");
     BinLayout B;
     B.b1 = b1; B.b2 = b2; B.b3 = b3;
     B.nb1 = (int)((nf1 + b1 - 1) / b1);
@@ -861,9 +952,11 @@ void NufftPlan::set_bins(int b1, int b2, int b3) {
         return 6 * L.tile_cells() * (int64_t)sizeof(float2) + kStageChunk * (int64_t)point_rec_bytes(w, 3);
     };
     B.r3 = B.t3 + (((w - B.t3) % 16) + 16) % 16;  // conflict-free rows when they fit
-    if (smem_need(B) > 227 * 1024) B.r3 = B.t3;
+    // 227 KB per CTA, less the binned kernels' static slab-start tables
+    constexpr int64_t kSmemMax = 227 * 1024 - (int64_t)sizeof(int) * (kStageWarps * kMaxB1 + kMaxB1 + 1);
+    if (smem_need(B) > kSmemMax) B.r3 = B.t3;
     if (B.nbins() > (int64_t)INT32_MAX - 1) throw Error(ERR_ARG, "too many bins");
-    if (smem_need(B) > 227 * 1024) throw Error(ERR_ARG, "bin tile too large for shared memory");
+    if (smem_need(B) > kSmemMax) throw Error(ERR_ARG, "bin tile too large for shared memory");
     bins = B;
     drop_sorted();
 }
@@ -1021,8 +1114,8 @@ void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumu
         constexpr int W = decltype(WC)::value;
         auto kern = k_spread_binned<W, 3, AdjointStrength>;
         raise_smem_limit((const void *)kern, smem);
-        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
-                                                        AdjointStrength{pbuf.p});
+        kern<<<(unsigned)bins.nbins(), kStageChunk, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
+                                                                AdjointStrength{pbuf.p});
         LAMINO_LAUNCH("k_spread_binned<adjoint>");
     });
     fft_fine(+1, 3, s);
@@ -1045,8 +1138,8 @@ void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cuda
             if (sp) {
                 auto kern = k_sysmat_binned<W>;
                 raise_smem_limit((const void *)kern, smem);
-                kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p, gin.p,
-                                                                nf(), inv_scale);
+                kern<<<(unsigned)bins.nbins(), kStageChunk, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p,
+                                                                        gin.p, nf(), inv_scale);
                 LAMINO_LAUNCH("k_sysmat_binned");
             } else {
                 unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
@@ -1111,8 +1204,8 @@ void NufftPlan::type1(const Geom &g, const float2 *c, float2 *modes, cudaStream_
         constexpr int W = decltype(WC)::value;
         auto kern = k_spread_binned<W, 1, RawStrength>;
         raise_smem_limit((const void *)kern, smem);
-        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
-                                                        RawStrength{c});
+        kern<<<(unsigned)bins.nbins(), kStageChunk, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
+                                                                RawStrength{c});
         LAMINO_LAUNCH("k_spread_binned<raw>");
     });
     fft_fine(+1, 1, s);

@@ -87,8 +87,20 @@ int64_t Server::submit(std::unique_ptr<ServeRequest> r) {
 
 void Server::worker(int wid) {
     (void)wid;
-    cudaStream_t s = nullptr;
-    if (!dry_ && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
+    // setup on a low-priority stream, the solve on a high-priority one: the
+    // block scheduler gives a running solve's small kernels the SMs ahead of
+    // another request's setup kernels
+    cudaStream_t s = nullptr, ss = nullptr;
+    if (!dry_) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, least) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&ss, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+            if (s) cudaStreamDestroy(s);
+            if (ss) cudaStreamDestroy(ss);
+            s = ss = nullptr;
+        }
+    }
     for (;;) {
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait(lk, [&] {
@@ -118,22 +130,39 @@ void Server::worker(int wid) {
                 r->result.assign((size_t)nv, 0.f);
             } else {
                 if (!s) throw Error(ERR_CUDA, "worker stream creation failed");
-                AllocStreamScope scope(s);
                 std::vector<DevBuf<float>> dp(r->projs.size());
                 std::vector<Dataset> data;
-                for (size_t i = 0; i < r->projs.size(); ++i) {
-                    dp[i].alloc(r->projs[i].size());
-                    LAMINO_CUDA(cudaMemcpyAsync(dp[i].p, r->projs[i].data(), r->projs[i].size() * 4,
-                                                cudaMemcpyHostToDevice, s));
-                    data.push_back(Dataset{dp[i].p, r->pdims[i][0], r->pdims[i][1], r->pdims[i][2],
-                                           r->angles[i].data(), r->gammas[i]});
+                DevBuf<float> out;
+                std::unique_ptr<MbirJob> job;
+                // destroyed first, also when a step throws: the solve stream has
+                // drained before any buffer goes back to the pool
+                struct Drain {
+                    cudaStream_t st;
+                    ~Drain() { cudaStreamSynchronize(st); }
+                } drain{ss};
+                {
+                    AllocStreamScope scope(s);
+                    for (size_t i = 0; i < r->projs.size(); ++i) {
+                        dp[i].alloc(r->projs[i].size());
+                        LAMINO_CUDA(cudaMemcpyAsync(dp[i].p, r->projs[i].data(), r->projs[i].size() * 4,
+                                                    cudaMemcpyHostToDevice, s));
+                        data.push_back(Dataset{dp[i].p, r->pdims[i][0], r->pdims[i][1], r->pdims[i][2],
+                                               r->angles[i].data(), r->gammas[i]});
+                    }
+                    out.alloc(nv);
+                    job.reset(new MbirJob(r->method, data, r->recon, r->prm, out.p, s, ss));
+                    job->prepare();
                 }
-                DevBuf<float> out(nv);
-                mbir(r->method, data, r->recon, r->prm, out.p, s);
+                {
+                    AllocStreamScope scope(ss);  // solver buffers live on the solve stream
+                    job->solve();
+                    job->finish();  // synchronises ss
+                }
                 r->phases = last_mbir_phases();
                 r->result.resize((size_t)nv);
-                LAMINO_CUDA(cudaMemcpyAsync(r->result.data(), out.p, nv * 4, cudaMemcpyDeviceToHost, s));
-                LAMINO_CUDA(cudaStreamSynchronize(s));
+                LAMINO_CUDA(cudaMemcpyAsync(r->result.data(), out.p, nv * 4, cudaMemcpyDeviceToHost, ss));
+                LAMINO_CUDA(cudaStreamSynchronize(ss));
+                job.reset();
             }
         } catch (const Error &e) {
             status = e.code;
@@ -155,6 +184,7 @@ void Server::worker(int wid) {
         cv_.notify_all();
     }
     if (s) cudaStreamDestroy(s);
+    if (ss) cudaStreamDestroy(ss);
 }
 
 bool Server::wait(int64_t id, double timeout_s, ServeRequest **out) {

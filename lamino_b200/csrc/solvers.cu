@@ -966,54 +966,87 @@ __global__ void k_extrap(float *__restrict__ y, const float *__restrict__ x, con
         y[i] = x[i] + (x[i] - xo[i]) * beta;
 }
 
-int nagopt(const GradFn &grad, const LossFn &loss, float *x, Dims3 d, int max_iters, float lipschitz, float tol,
-           float xtol, int max_inner, cudaStream_t s) {
-    const int64_t V = d.size(), n = 3 * V;
-    DevBuf<float> xold(n), y(n), g(n);
-    LAMINO_CUDA(cudaMemcpyAsync(xold.p, x, n * 4, cudaMemcpyDeviceToDevice, s));
-    Reducer red(8);
-    double t = 1, tnew = 1;
-    float step = (float)(0.1 / lipschitz), step_prev = step;
-    double xerr = 1e300;
-    int it = 0;
-    for (; it < max_iters; ++it) {
-        for (int inner = 0; inner < max_inner; ++inner) {
-            float beta = (float)(tnew * (1.0 / t - 1.0));
-            tnew = 0.5 * (std::sqrt(std::pow(t, 4) + 4 * std::pow(t, 2)) - std::pow(t, 2));
-            k_extrap<<<grid_for(n, 256), 256, 0, s>>>(y.p, x, xold.p, beta, n);
-            LAMINO_LAUNCH("k_extrap");
-            grad(y.p, g.p, s);
-            vec_lin2(x, 1.f, y.p, -step, g.p, n, s);
-            double ex = loss(x, s);
-            double ey = loss(y.p, s);
-            red.zero(3, s);
-            vec_sqdist3(g.p, nullptr, V, red.d, s);
-            red.fetch(3, s);
-            double gy = 0.0;
-            for (int i = 0; i < 3; ++i) gy += std::sqrt(red.h[i]);
-            gy *= 0.5 * step;
-            if (ex > ey + gy) {
-                step *= 0.9f;
-            } else {
-                step = step_prev;
-                t = tnew;
-                red.zero(6, s);
-                vec_sqdist3(x, xold.p, V, red.d, s);
-                vec_sqdist3(x, nullptr, V, red.d + 3, s);
-                red.fetch(6, s);
-                double xe = 0, xn = 0;
-                for (int i = 0; i < 3; ++i) { xe += std::sqrt(red.h[i]); xn += std::sqrt(red.h[3 + i]); }
-                xerr = xe / xn;
-                if (xerr < xtol) return it + 1;
-                LAMINO_CUDA(cudaMemcpyAsync(xold.p, x, n * 4, cudaMemcpyDeviceToDevice, s));
-                break;
-            }
+// One host read per line-search step: the losses of x and y, |g| and the
+// x-change norms (used when the step is accepted) are reduced on the device
+// into one buffer and fetched together, where the reference reads each as it
+// goes; the values and the decisions are the same.  The reference evaluates
+// loss(x) once more after each line search (src/nagopt.cpp); x has not changed
+// since the line search's last evaluation, so that value is reused.
+NagSolve::NagSolve(GradFn grad, LossTerms loss, float *x3, Dims3 d, int max_iters, float lipschitz, float tol,
+                   float xtol, int max_inner, cudaStream_t s)
+    : grad_(std::move(grad)), loss_(std::move(loss)), x_(x3), d_(d), max_iters_(max_iters), max_inner_(max_inner),
+      tol_(tol), xtol_(xtol), s_(s), xold_(3 * d.size()), y_(3 * d.size()), g_(3 * d.size()),
+      red_(2 * loss_.nterms + 9) {
+    step_ = step_prev_ = (float)(0.1 / lipschitz);
+    LAMINO_CUDA(cudaMemcpyAsync(xold_.p, x_, 3 * d.size() * 4, cudaMemcpyDeviceToDevice, s_));
+    done_ = max_iters_ <= 0 || max_inner_ <= 0;
+}
+
+// slots: [loss terms of x][loss terms of y][|g_c|^2][|x_c - xold_c|^2][|x_c|^2]
+void NagSolve::enqueue() {
+    const int64_t V = d_.size(), n = 3 * V;
+    const int M = loss_.nterms;
+    double *const gsl = red_.d + 2 * M;
+    const float beta = (float)(tnew_ * (1.0 / t_ - 1.0));
+    tnew_ = 0.5 * (std::sqrt(std::pow(t_, 4) + 4 * std::pow(t_, 2)) - std::pow(t_, 2));
+    k_extrap<<<grid_for(n, 256), 256, 0, s_>>>(y_.p, x_, xold_.p, beta, n);
+    LAMINO_LAUNCH("k_extrap");
+    grad_(y_.p, g_.p, s_);
+    vec_lin2(x_, 1.f, y_.p, -step_, g_.p, n, s_);
+    red_.zero(2 * M + 9, s_);
+    loss_.enqueue(x_, red_.d, s_);
+    loss_.enqueue(y_.p, red_.d + M, s_);
+    vec_sqdist3(g_.p, nullptr, V, gsl, s_);
+    vec_sqdist3(x_, xold_.p, V, gsl + 3, s_);
+    vec_sqdist3(x_, nullptr, V, gsl + 6, s_);
+    LAMINO_CUDA(cudaMemcpyAsync(red_.h, red_.d, sizeof(double) * (2 * M + 9), cudaMemcpyDeviceToHost, s_));
+}
+
+bool NagSolve::finish() {
+    const int M = loss_.nterms;
+    const double *h = red_.h;
+    const double ex = loss_.value(h), ey = loss_.value(h + M);
+    double gy = 0.0;
+    for (int i = 0; i < 3; ++i) gy += std::sqrt(h[2 * M + i]);
+    gy *= 0.5 * step_;
+    bool line_search_over = false;
+    if (ex > ey + gy) {
+        step_ *= 0.9f;
+    } else {
+        step_ = step_prev_;
+        t_ = tnew_;
+        double xe = 0, xn = 0;
+        for (int i = 0; i < 3; ++i) {
+            xe += std::sqrt(h[2 * M + 3 + i]);
+            xn += std::sqrt(h[2 * M + 6 + i]);
         }
-        double e = loss(x, s);
-        if (e < tol) { ++it; break; }
+        xerr_ = xe / xn;
+        if (xerr_ < xtol_) {
+            ++it_;
+            done_ = true;
+            return true;
+        }
+        LAMINO_CUDA(cudaMemcpyAsync(xold_.p, x_, 3 * d_.size() * 4, cudaMemcpyDeviceToDevice, s_));
+        line_search_over = true;
+    }
+    if (!line_search_over && ++inner_ < max_inner_) return false;
+    // end of an outer iteration: its loss is ex (x unchanged since)
+    inner_ = 0;
+    ++it_;
+    if (ex < tol_ || it_ >= max_iters_) done_ = true;
+    return done_;
+}
+
+int nagopt(const GradFn &grad, const LossTerms &loss, float *x, Dims3 d, int max_iters, float lipschitz, float tol,
+           float xtol, int max_inner, cudaStream_t s) {
+    NagSolve nag(grad, loss, x, d, max_iters, lipschitz, tol, xtol, max_inner, s);
+    while (!nag.done()) {
+        nag.enqueue();
+        LAMINO_CUDA(cudaStreamSynchronize(s));
+        nag.finish();
     }
     LAMINO_CUDA(cudaStreamSynchronize(s));
-    return it;
+    return nag.iterations();
 }
 
 // ---------------------------------------------------------------------------
@@ -1030,9 +1063,43 @@ __global__ void k_uniform(float *__restrict__ x, int64_t n, unsigned long long s
     }
 }
 
+// x = Ax / sqrt(*sq) with the factor formed in double and rounded to float, as
+// the host does in the loop below
+__global__ void k_scale_inv_norm(float *__restrict__ out, const float *__restrict__ x, const double *sq, int64_t n) {
+    const float a = (float)(1.0 / sqrt(*sq));
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a * x[i] + 0.f;
+}
+
 double lipschitz(const OpFn &A, Dims3 d, int max_iters, double tol, unsigned long long seed, cudaStream_t s) {
     const int64_t n = 3 * d.size();
     DevBuf<float> x(n), Ax(n);
+    if (tol == 0.0 && max_iters > 0) {
+        // no early stop: the whole iteration stays on the device (the norms into
+        // one slot each, the normalisation read from the slot) and the norms are
+        // fetched once; same arithmetic as the loop below
+        Reducer red(max_iters + 1);
+        red.zero(max_iters + 1, s);
+        k_uniform<<<grid_for(n, 256), 256, 0, s>>>(x.p, n, seed);
+        LAMINO_LAUNCH("k_uniform");
+        vec_dot(x.p, x.p, n, red.d, s);
+        k_scale_inv_norm<<<grid_for(n, 256), 256, 0, s>>>(x.p, x.p, red.d, n);
+        LAMINO_LAUNCH("k_scale_inv_norm");
+        for (int i = 0; i < max_iters; ++i) {
+            A(x.p, Ax.p, s);
+            vec_dot(Ax.p, Ax.p, n, red.d + 1 + i, s);
+            k_scale_inv_norm<<<grid_for(n, 256), 256, 0, s>>>(x.p, Ax.p, red.d + 1 + i, n);
+            LAMINO_LAUNCH("k_scale_inv_norm");
+        }
+        red.fetch(max_iters + 1, s);
+        double L = 0.0;
+        for (int i = 0; i < max_iters; ++i) {
+            const double nA = std::sqrt(red.h[1 + i]);
+            if (nA < 1e-12) return 0.0;
+            L = nA;
+        }
+        return L;
+    }
     Reducer red(2);
     k_uniform<<<grid_for(n, 256), 256, 0, s>>>(x.p, n, seed);
     LAMINO_LAUNCH("k_uniform");

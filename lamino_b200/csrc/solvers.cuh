@@ -96,9 +96,48 @@ int split_bregman(const OpFn &A, const float *yT3, float *x3, Dims3 d, float lam
 
 // src/nagopt.cpp:116-209 (vector form); grad and loss are closures.
 using GradFn = std::function<void(const float *x3, float *g3, cudaStream_t)>;
-using LossFn = std::function<double(const float *x3, cudaStream_t)>;
-int nagopt(const GradFn &grad, const LossFn &loss, float *x3, Dims3 d, int max_iters, float lipschitz, float tol,
+// A loss split so that several evaluations share one host read: enqueue(x, acc)
+// adds the loss's nterms partial sums of x into device doubles acc[0..nterms)
+// (zeroed by the caller) without reading them; value(terms) forms the loss from
+// the fetched sums on the host.
+struct LossTerms {
+    int nterms = 0;
+    std::function<void(const float *x3, double *acc, cudaStream_t)> enqueue;
+    std::function<double(const double *terms)> value;
+};
+int nagopt(const GradFn &grad, const LossTerms &loss, float *x3, Dims3 d, int max_iters, float lipschitz, float tol,
            float xtol, int max_inner, cudaStream_t s);
+
+// The same solve advanced one line-search step at a time, so that several
+// solves on their own streams can share host synchronisation: enqueue() queues
+// a step's work and the asynchronous copy of its reductions; once the stream
+// has reached that point (the caller synchronises it), finish() reads them,
+// takes the step's decisions and returns whether the solve has ended.
+class NagSolve {
+  public:
+    NagSolve(GradFn grad, LossTerms loss, float *x3, Dims3 d, int max_iters, float lipschitz, float tol, float xtol,
+             int max_inner, cudaStream_t s);
+    void enqueue();
+    bool finish();
+    bool done() const { return done_; }
+    int iterations() const { return it_; }
+    cudaStream_t stream() const { return s_; }
+
+  private:
+    GradFn grad_;
+    LossTerms loss_;
+    float *x_;
+    Dims3 d_;
+    int max_iters_, max_inner_;
+    float tol_, xtol_;
+    cudaStream_t s_;
+    DevBuf<float> xold_, y_, g_;
+    Reducer red_;
+    double t_ = 1, tnew_ = 1, xerr_ = 1e300;
+    float step_, step_prev_;
+    int it_ = 0, inner_ = 0;
+    bool done_ = false;
+};
 
 // power iteration for ||A|| (src/lipschitz.cpp:31-53, made to work: seeded start, FP64 norms)
 double lipschitz(const OpFn &A, Dims3 d, int max_iters, double tol, unsigned long long seed, cudaStream_t s);

@@ -1,9 +1,10 @@
-"""The served form at the sizes it serves, against the FP64 oracle.
+"""The served and batched forms at the sizes they serve, against the FP64 oracle.
 
 The two smallest requests of the batched / served mix (NAG + qGGMRF, recon
 thickness 8 and 16 x lateral 64, two datasets of 60 angles at gamma 0 and a
 tilt, 64 x 64 projections) run through the continuous-batching server
-(lamino_server_*) and as direct MBIR3 calls, and both are compared with the
+(lamino_server_*), the batched form (lamino_mbir3_batch) and as direct MBIR3
+calls, and all three are compared with the
 oracle's double-precision MBIR3 (src/mbir3.cpp:47-135) in its Toeplitz form
 (oracle.MBIR3_toeplitz, pinned to the reference's own MBIR3 on the CPU).  The
 Lipschitz constant is the oracle's 30-step power iteration, passed to both as
@@ -48,7 +49,11 @@ def test_served_and_direct_mbir3_vs_fp64_oracle(L, O, thickness, seed):
     with L.ReconServer(budget_bytes=8 << 30, slots=2) as srv:
         rid = srv.submit(3, data, recon, p)
         served, _ = srv.wait(rid)
-    e_direct, e_served = rel(direct, want), rel(served, want)
-    print(f"thickness {thickness}: direct {e_direct:.2e}, served {e_served:.2e} vs FP64 oracle (L = {lip:.4g})")
+    (batched,), info = L.mbir3_batch([(data, recon, p)], budget_bytes=8 << 30, threads=1)
+    e_direct, e_served, e_batched = rel(direct, want), rel(served, want), rel(batched, want)
+    print(f"thickness {thickness}: direct {e_direct:.2e}, served {e_served:.2e}, batched {e_batched:.2e} "
+          f"vs FP64 oracle (L = {lip:.4g})")
     assert e_direct < TOL_VOLUME
     assert e_served < TOL_VOLUME
+    assert e_batched < TOL_VOLUME
+    assert info["iterations"] == [ITERS]

@@ -105,6 +105,14 @@ def test_lipschitz_vs_oracle(L, O):
     Lo = O.lipschitz(A_o, (3,) + dims, max_iters=60, tol=1e-9)
     Lg = L.opt.lipschitz(L.ToeplitzNormal(pgs, dims), dims, max_iters=60, tol=1e-9)
     assert Lg == pytest.approx(Lo, rel=1e-3)
+    # without an early stop (tol 0, as MBIR3 calls it) the iteration runs on the
+    # device with one host read at the end: the same arithmetic as the loop with a
+    # read per step, which tol = -1 (a stop that never triggers) still takes
+    T = L.ToeplitzNormal(pgs, dims)
+    a = L.opt.lipschitz(T, dims, max_iters=30, tol=0.0)
+    b = L.opt.lipschitz(T, dims, max_iters=30, tol=-1.0)
+    assert a == b
+    assert a == pytest.approx(O.lipschitz(A_o, (3,) + dims, max_iters=30, tol=0.0), rel=1e-3)
 
 
 def _datasets(L, O, recon=(8, 5, 9), nproj=(6, 5), det=(9, 11), gammas=(0.0, 0.8), seed=3):

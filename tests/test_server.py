@@ -151,6 +151,24 @@ def test_server_bad_arguments(LB):
             srv.submit(1, [(np.zeros((4, 8, 8), np.float32), np.zeros(3, np.float32), 0.0)], (8, 8, 8))
 
 
+def test_batch_checks_before_device_work(LB):
+    """lamino_mbir3_batch validates every request (and its footprint against the
+    budget) before it touches a device, so these run without a GPU."""
+    out, info = LB.mbir3_batch([])
+    assert out == [] and info["steps"] == 0
+    req = (_req(nproj=4, det=(16, 16)), (16, 8, 16), LB.ReconParams())
+    fp = LB.mbir_footprint(3, [(4, 16, 16)], (16, 8, 16), LB.ReconParams())
+    with pytest.raises(LB.LaminoError) as e:  # larger than the budget
+        LB.mbir3_batch([req, req], budget_bytes=fp - 1)
+    assert e.value.args[0].startswith("lamino error 2")
+    with pytest.raises(LB.LaminoError):
+        LB.mbir3_batch([req], budget_bytes=0)
+    with pytest.raises(LB.LaminoError):
+        LB.mbir3_batch([req], threads=0)
+    with pytest.raises(ValueError):
+        LB.mbir3_batch([([], (16, 8, 16), None)])
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
