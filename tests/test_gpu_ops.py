@@ -256,7 +256,7 @@ def test_full_size_toeplitz_properties(L):
     assert (torch.linalg.norm(ys - yn) / torch.linalg.norm(yn)).item() < 1e-4
 
 
-@pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721)])
+@pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721), (721, 71, 9)])
 def test_toeplitz_compiled_fft_lengths(L, O, dims):
     """Thin volumes whose FFT lengths hit the compile-time schedules (n1 = 721 ->
     1458, n2 = 71 -> 144, n3 = 721 -> packed 729) against the oracle.  The
