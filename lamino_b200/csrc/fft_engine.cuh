@@ -386,26 +386,50 @@ __device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const F
 
 // ---- compile-time schedules for the lengths of the common problem sizes ----
 // (729 = packed n3 transform and 1458 = n1 transform of a 721-voxel axis; 144 =
-// n2 transform of a 71-voxel axis).  Other lengths use the runtime path above.
+// n2 transform of a 71-voxel axis; 180, 360, 540, 750 = n1 transforms of the
+// 90-, 180-, 270- and 362-voxel lateral axes of 64- to 256-wide reconstructions).
+// Each equals the runtime schedule fft_schedule(N, true), so the DIF output
+// positions are the same either way.  Other lengths use the runtime path above.
+constexpr int CT_MAX_STAGES = 6;
 template <int N>
 struct CtSched {
     static constexpr int ns = 0;
-    static constexpr int r[4] = {0, 0, 0, 0};
+    static constexpr int r[CT_MAX_STAGES] = {0, 0, 0, 0, 0, 0};
 };
 template <>
 struct CtSched<729> {
     static constexpr int ns = 3;
-    static constexpr int r[4] = {9, 9, 9, 0};
+    static constexpr int r[CT_MAX_STAGES] = {9, 9, 9, 0, 0, 0};
 };
 template <>
 struct CtSched<1458> {
     static constexpr int ns = 4;
-    static constexpr int r[4] = {2, 9, 9, 9};
+    static constexpr int r[CT_MAX_STAGES] = {2, 9, 9, 9, 0, 0};
 };
 template <>
 struct CtSched<144> {
     static constexpr int ns = 3;
-    static constexpr int r[4] = {2, 8, 9, 0};
+    static constexpr int r[CT_MAX_STAGES] = {2, 8, 9, 0, 0, 0};
+};
+template <>
+struct CtSched<180> {
+    static constexpr int ns = 4;
+    static constexpr int r[CT_MAX_STAGES] = {2, 2, 9, 5, 0, 0};
+};
+template <>
+struct CtSched<360> {
+    static constexpr int ns = 4;
+    static constexpr int r[CT_MAX_STAGES] = {2, 4, 9, 5, 0, 0};
+};
+template <>
+struct CtSched<540> {
+    static constexpr int ns = 5;
+    static constexpr int r[CT_MAX_STAGES] = {2, 2, 9, 5, 3, 0};
+};
+template <>
+struct CtSched<750> {
+    static constexpr int ns = 5;
+    static constexpr int r[CT_MAX_STAGES] = {2, 5, 5, 5, 3, 0};
 };
 
 template <int N>

@@ -904,6 +904,10 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(
     }
     if constexpr (N1 == 1458) {
         p1458_forward(PencilRows{pv, cs, n1}, tw1, sm);
+    } else if constexpr (N1 != 0) {  // compile-time schedule: lead stages in registers, the rest fixed
+        fftlead_load<CtSched<N1>::r[1]>(PencilRows{pv, cs, n1}, tw1, sm, N1, N1, threadIdx.x, blockDim.x);
+        __syncthreads();
+        ct_forward<N1, 2>(sm, 3, N1, tw1, threadIdx.x, blockDim.x);
     } else if (F1.ns >= 2) {  // runtime length: the outer stages in registers as well
         fftlead_any<false>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -977,6 +981,9 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(
     __syncthreads();
     if constexpr (N1 == 1458) {
         p1458_inverse(PencilRows{pv, cs, n1}, tw1, sm);
+    } else if constexpr (N1 != 0) {
+        ct_inverse<N1, CtSched<N1>::ns - 1, 2>(sm, 3, N1, tw1, threadIdx.x, blockDim.x);
+        fftlead_store<CtSched<N1>::r[1]>(PencilRows{pv, cs, n1}, tw1, sm, N1, N1, threadIdx.x, blockDim.x);
     } else if (F1.ns >= 2) {
         fft_inverse(sm, 3, L1, F1, 2, threadIdx.x, blockDim.x);
         fftlead_any<true>(PencilRows{pv, cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
@@ -1011,6 +1018,11 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256) k_pencil_qua
     const float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
         p1458_forward(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm);  // reads only
+    } else if constexpr (N1 != 0) {
+        fftlead_load<CtSched<N1>::r[1]>(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm, N1, N1,
+                                        threadIdx.x, blockDim.x);
+        __syncthreads();
+        ct_forward<N1, 2>(sm, 3, N1, tw1, threadIdx.x, blockDim.x);
     } else if (F1.ns >= 2) {
         fftlead_any<false>(PencilRows{const_cast<float2 *>(pv), cs, n1}, F1, sm, L1, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -1276,6 +1288,25 @@ static int64_t embed_len(int64_t n) {
     return next_smooth_even(2 * n);
 }
 
+// whether the n1 length has a compile-time pencil schedule equal to the runtime
+// one r (the spectra are stored in the runtime schedule's DIF positions)
+template <int N>
+static bool ct_equal(const std::vector<int> &r) {
+    if ((int)r.size() != CtSched<N>::ns) return false;
+    for (int i = 0; i < CtSched<N>::ns; ++i)
+        if (r[i] != CtSched<N>::r[i]) return false;
+    return true;
+}
+static bool ct_schedule_matches(int L, const std::vector<int> &r) {
+    switch (L) {
+        case 750: return ct_equal<750>(r);
+        case 540: return ct_equal<540>(r);
+        case 360: return ct_equal<360>(r);
+        case 180: return ct_equal<180>(r);
+        default: return false;
+    }
+}
+
 void Toeplitz::init_tables(Dims3 d, int prec) {
     if (d.n1 <= 0 || d.n2 <= 0 || d.n3 <= 0) throw Error(ERR_ARG, "volume dims must be positive");
     if (prec != PREC_FP32 && prec != PREC_FP16 && prec != PREC_MIXED)
@@ -1425,7 +1456,7 @@ void Toeplitz::finish(cudaStream_t s) {
     while (kb2 > 1 && d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 160 * 1024) kb2 /= 2;
     if (d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
         throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
-    ct1 = L1 == 1458 ? 1458 : 0;
+    ct1 = (L1 == 1458 || ct_schedule_matches((int)L1, r1_)) ? (int)L1 : 0;
     ct2 = L2 == 144 ? 144 : 0;
     ct3 = M3 == 729 ? 729 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
@@ -1446,6 +1477,13 @@ void Toeplitz::finish(cudaStream_t s) {
     attr((const void *)k_pencil<true, 1458>, smem_pen);
     attr((const void *)k_pencil_quad<0>, smem_pen);
     attr((const void *)k_pencil_quad<1458>, smem_pen);
+    for (const void *f : {(const void *)k_pencil<false, 750>, (const void *)k_pencil<true, 750>,
+                          (const void *)k_pencil_quad<750>, (const void *)k_pencil<false, 540>,
+                          (const void *)k_pencil<true, 540>, (const void *)k_pencil_quad<540>,
+                          (const void *)k_pencil<false, 360>, (const void *)k_pencil<true, 360>,
+                          (const void *)k_pencil_quad<360>, (const void *)k_pencil<false, 180>,
+                          (const void *)k_pencil<true, 180>, (const void *)k_pencil_quad<180>})
+        attr(f, smem_pen);
 }
 
 Toeplitz::~Toeplitz() {
@@ -1498,6 +1536,29 @@ void Toeplitz::stage_bytes(int64_t *b) const {
     b[4] = Z + 3 * V * 4;                               // read z1, write y
 }
 
+// the pencil kernel of the operator's n1 length: compile-time schedules for the
+// lengths in CtSched (ct1), the runtime one otherwise (ct1 = 0)
+template <bool HALF>
+static void launch_pencil(int ct1, unsigned grid, int smem, cudaStream_t s, float2 *xa, int n1, int np1, int l2,
+                          int l3h, const FftLen &f1, const float2 *tw1, const float *K, const __half *Kh,
+                          const float *ksc) {
+    switch (ct1) {
+#define LAMINO_PENCIL(N)                                                                                       \
+    case N:                                                                                                    \
+        k_pencil<HALF, N><<<grid, N == 1458 ? P1458_THREADS : 256, smem, s>>>(xa, n1, np1, l2, l3h, f1, tw1, K, \
+                                                                              Kh, ksc);                        \
+        break;
+        LAMINO_PENCIL(1458)
+        LAMINO_PENCIL(750)
+        LAMINO_PENCIL(540)
+        LAMINO_PENCIL(360)
+        LAMINO_PENCIL(180)
+        LAMINO_PENCIL(0)
+#undef LAMINO_PENCIL
+        default: throw Error(ERR_STATE, "no pencil kernel for this length");
+    }
+}
+
 void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     if (!z1.p || !xa.p) throw Error(ERR_STATE, "Toeplitz operator has no work buffers");
     const bool prof = profiling && (size_t)(nprof + 1) * (NSTAGE + 1) <= ev.size();
@@ -1520,14 +1581,8 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
     const bool h = precision == PREC_FP16 || (precision == PREC_MIXED && low);
-    if (ct1 && h)
-        k_pencil<true, 1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
-    else if (ct1)
-        k_pencil<false, 1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
-    else if (h)
-        k_pencil<true, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
-    else
-        k_pencil<false, 0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
+    if (h) launch_pencil<true>(ct1, gpen, smem_pen, s, xa.p, n1, np1, l2, l3h, f1, tw1.p, nullptr, Kh.p, Kscale.p);
+    else launch_pencil<false>(ct1, gpen, smem_pen, s, xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
     LAMINO_LAUNCH("k_pencil");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[3], s));
     if (ct2) k_dim2_inv<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
@@ -1570,10 +1625,21 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
         QuadSets qs{};
         const int ng = (int)std::min<size_t>(kMaxQuadSets, parts.size() - g0);
         for (int g = 0; g < ng; ++g) qs.K[g] = parts[g0 + g]->K.p;
-        if (ct1)
-            k_pencil_quad<1458><<<gpen, P1458_THREADS, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
-        else
-            k_pencil_quad<0><<<gpen, 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1, tw1.p, qs, ng, acc + 3 * g0);
+        switch (ct1) {
+#define LAMINO_QUAD(N)                                                                                          \
+    case N:                                                                                                     \
+        k_pencil_quad<N><<<gpen, N == 1458 ? P1458_THREADS : 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1,    \
+                                                                              tw1.p, qs, ng, acc + 3 * g0); \
+        break;
+            LAMINO_QUAD(1458)
+            LAMINO_QUAD(750)
+            LAMINO_QUAD(540)
+            LAMINO_QUAD(360)
+            LAMINO_QUAD(180)
+            LAMINO_QUAD(0)
+#undef LAMINO_QUAD
+            default: throw Error(ERR_STATE, "no pencil kernel for this length");
+        }
         LAMINO_LAUNCH("k_pencil_quad");
     }
 }

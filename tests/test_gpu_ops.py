@@ -256,10 +256,13 @@ def test_full_size_toeplitz_properties(L):
     assert (torch.linalg.norm(ys - yn) / torch.linalg.norm(yn)).item() < 1e-4
 
 
-@pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721), (721, 71, 9)])
+@pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721), (721, 71, 9), (90, 3, 8), (180, 3, 8),
+                                  (270, 3, 8), (362, 3, 8)])
 def test_toeplitz_compiled_fft_lengths(L, O, dims):
     """Thin volumes whose FFT lengths hit the compile-time schedules (n1 = 721 ->
-    1458, n2 = 71 -> 144, n3 = 721 -> packed 729) against the oracle.  The
+    1458, n2 = 71 -> 144, n3 = 721 -> packed 729; n1 = 90 / 180 / 270 / 362 ->
+    180 / 360 / 540 / 750, the lateral lengths of the batched mix) against the
+    oracle.  The
     Toeplitz form evaluates the exact lattice, so the oracle here uses FP64
     points (the reference's double path): with white input on a 721-long axis
     the float32 points of the float path move the highest modes' phases by about
