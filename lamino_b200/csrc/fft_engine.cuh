@@ -387,7 +387,8 @@ __device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const F
 // ---- compile-time schedules for the lengths of the common problem sizes ----
 // (729 = packed n3 transform and 1458 = n1 transform of a 721-voxel axis; 144 =
 // n2 transform of a 71-voxel axis; 180, 360, 540, 750 = n1 transforms of the
-// 90-, 180-, 270- and 362-voxel lateral axes of 64- to 256-wide reconstructions).
+// 90-, 180-, 270- and 362-voxel lateral axes of 64- to 256-wide reconstructions;
+// 20, 48, 64, 90 = n2 transforms of their 10- to 44-voxel thickness axes).
 // Each equals the runtime schedule fft_schedule(N, true), so the DIF output
 // positions are the same either way.  Other lengths use the runtime path above.
 constexpr int CT_MAX_STAGES = 6;
@@ -431,11 +432,62 @@ struct CtSched<750> {
     static constexpr int ns = 5;
     static constexpr int r[CT_MAX_STAGES] = {2, 5, 5, 5, 3, 0};
 };
+// n2 transforms of the 10-, 22-, 32- and 44-voxel thickness axes
+template <>
+struct CtSched<20> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {2, 2, 5, 0, 0, 0};
+};
+template <>
+struct CtSched<48> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {2, 8, 3, 0, 0, 0};
+};
+template <>
+struct CtSched<64> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {2, 4, 8, 0, 0, 0};
+};
+template <>
+struct CtSched<90> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {2, 9, 5, 0, 0, 0};
+};
 
+// Schedules of the packed row transforms (no zero-padded lead stage): the
+// packed half lengths 90, 180, 270, 375 of the 180- to 750-long n3 embeddings.
+// Each equals fft_schedule(N, false).
 template <int N>
+struct CtRowSched {
+    static constexpr int ns = 0;
+    static constexpr int r[CT_MAX_STAGES] = {0, 0, 0, 0, 0, 0};
+};
+template <>
+struct CtRowSched<90> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {2, 9, 5, 0, 0, 0};
+};
+template <>
+struct CtRowSched<180> {
+    static constexpr int ns = 3;
+    static constexpr int r[CT_MAX_STAGES] = {4, 9, 5, 0, 0, 0};
+};
+template <>
+struct CtRowSched<270> {
+    static constexpr int ns = 4;
+    static constexpr int r[CT_MAX_STAGES] = {2, 9, 5, 3, 0, 0};
+};
+template <>
+struct CtRowSched<375> {
+    static constexpr int ns = 4;
+    static constexpr int r[CT_MAX_STAGES] = {5, 5, 5, 3, 0, 0};
+};
+
+// block size before stage s of schedule SC (length N)
+template <int N, class SC>
 __host__ __device__ constexpr int ct_block(int s) {
     int b = N;
-    for (int i = 0; i < s; ++i) b /= CtSched<N>::r[i];
+    for (int i = 0; i < s; ++i) b /= SC::r[i];
     return b;
 }
 
@@ -493,22 +545,23 @@ __device__ __forceinline__ void fft_stage_fixed(float2 *__restrict__ data, int P
     }
 }
 
-template <int N, int S>
+// stages S .. SC::ns - 1 of schedule SC, each followed by a barrier
+template <int N, int S, class SC = CtSched<N>>
 __device__ __forceinline__ void ct_forward(float2 *data, int P, int ps, const float2 *tw, int tid, int nth) {
-    if constexpr (S < CtSched<N>::ns) {
-        fft_stage_fixed<CtSched<N>::r[S], N, ct_block<N>(S), false>(data, P, ps, tw, tid, nth);
+    if constexpr (S < SC::ns) {
+        fft_stage_fixed<SC::r[S], N, ct_block<N, SC>(S), false>(data, P, ps, tw, tid, nth);
         __syncthreads();
-        ct_forward<N, S + 1>(data, P, ps, tw, tid, nth);
+        ct_forward<N, S + 1, SC>(data, P, ps, tw, tid, nth);
     }
 }
 
 // undo stages S, S-1, ..., S_END
-template <int N, int S, int S_END>
+template <int N, int S, int S_END, class SC = CtSched<N>>
 __device__ __forceinline__ void ct_inverse(float2 *data, int P, int ps, const float2 *tw, int tid, int nth) {
     if constexpr (S >= S_END) {
-        fft_stage_fixed<CtSched<N>::r[S], N, ct_block<N>(S), true>(data, P, ps, tw, tid, nth);
+        fft_stage_fixed<SC::r[S], N, ct_block<N, SC>(S), true>(data, P, ps, tw, tid, nth);
         __syncthreads();
-        ct_inverse<N, S - 1, S_END>(data, P, ps, tw, tid, nth);
+        ct_inverse<N, S - 1, S_END, SC>(data, P, ps, tw, tid, nth);
     }
 }
 

@@ -390,6 +390,10 @@ __global__ void __launch_bounds__(256, N3 == 729 ? 3 : 4) k_r2c_rows(const float
     if constexpr (N3 == 729) {
         rows27_load(x + row0 * n3, nr, n3, F3.tw, sm, ps);
         rows27_mid<false>(sm, nr, ps);
+    } else if constexpr (N3 != 0) {  // compile-time schedule: the first stage in registers
+        rowslead_load<CtRowSched<N3>::r[0]>(x + row0 * n3, nr, n3, N3, F3.tw, sm, ps, threadIdx.x, blockDim.x);
+        __syncthreads();
+        ct_forward<N3, 1, CtRowSched<N3>>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
     } else if (F3.ns >= 1) {  // runtime length: the first stage in registers as well
         rowslead_any<false>(F3, x + row0 * n3, nullptr, sm, nullptr, nr, n3, ps, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -705,6 +709,11 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         dim2_144_load(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm, threadIdx.x, blockDim.x);
         __syncthreads();
         dim2_144_tail_store(sm, L3h, n1p, c, i1b, k3b, nk, KB, xa, threadIdx.x, blockDim.x);
+    } else if constexpr (N2 != 0) {  // compile-time schedule: the lead stages in registers, the rest fixed
+        dim2lead_load<CtSched<N2>::r[1]>(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, N2, tw2, sm, (int)threadIdx.x,
+                                         (int)blockDim.x);
+        __syncthreads();
+        ct_forward<N2, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
     } else if (F2.ns >= 2) {  // runtime length: the outer stages in registers as well
         LAMINO_DIM2_LEAD(dim2lead_load, F2.radix[1], z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, sm,
                          (int)threadIdx.x, (int)blockDim.x)
@@ -1123,6 +1132,12 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
         }
     }
     __syncthreads();
+    if constexpr (N2 != 0) {
+        ct_inverse<N2, CtSched<N2>::ns - 1, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+        dim2lead_store<CtSched<N2>::r[1]>(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, N2, tw2, z1, (int)threadIdx.x,
+                                          (int)blockDim.x);
+        return;
+    }
     if (F2.ns >= 2) {
         fft_inverse(sm, D2_IB * KB, ps, F2, 2, threadIdx.x, blockDim.x);
         LAMINO_DIM2_LEAD(dim2lead_store, F2.radix[1], sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, z1,
@@ -1184,6 +1199,10 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
     if constexpr (N3 == 729) {
         rows27_mid<true>(sm, nr, ps);
         rows27_store(sm, nr, ps, n3, F3.tw, y + row0 * n3);
+        return;
+    } else if constexpr (N3 != 0) {
+        ct_inverse<N3, CtRowSched<N3>::ns - 1, 1, CtRowSched<N3>>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
+        rowslead_store<CtRowSched<N3>::r[0]>(sm, nr, ps, n3, N3, F3.tw, y + row0 * n3, threadIdx.x, blockDim.x);
         return;
     }
     if (F3.ns >= 1) {
@@ -1288,6 +1307,9 @@ static int64_t embed_len(int64_t n) {
     return next_smooth_even(2 * n);
 }
 
+static void raise_rows_smem(int bytes);
+static void raise_d2_smem(int bytes);
+
 // whether the n1 length has a compile-time pencil schedule equal to the runtime
 // one r (the spectra are stored in the runtime schedule's DIF positions)
 template <int N>
@@ -1297,12 +1319,37 @@ static bool ct_equal(const std::vector<int> &r) {
         if (r[i] != CtSched<N>::r[i]) return false;
     return true;
 }
-static bool ct_schedule_matches(int L, const std::vector<int> &r) {
+template <int N>
+static bool ct_row_equal(const std::vector<int> &r) {
+    if ((int)r.size() != CtRowSched<N>::ns) return false;
+    for (int i = 0; i < CtRowSched<N>::ns; ++i)
+        if (r[i] != CtRowSched<N>::r[i]) return false;
+    return true;
+}
+static bool ct_row_matches(int M, const std::vector<int> &r) {
+    switch (M) {
+        case 375: return ct_row_equal<375>(r);
+        case 270: return ct_row_equal<270>(r);
+        case 180: return ct_row_equal<180>(r);
+        case 90: return ct_row_equal<90>(r);
+        default: return false;
+    }
+}
+static bool ct_schedule_matches(int L, const std::vector<int> &r) {  // n1 (pencil) lengths
     switch (L) {
         case 750: return ct_equal<750>(r);
         case 540: return ct_equal<540>(r);
         case 360: return ct_equal<360>(r);
         case 180: return ct_equal<180>(r);
+        default: return false;
+    }
+}
+static bool ct_dim2_matches(int L, const std::vector<int> &r) {  // n2 lengths
+    switch (L) {
+        case 90: return ct_equal<90>(r);
+        case 64: return ct_equal<64>(r);
+        case 48: return ct_equal<48>(r);
+        case 20: return ct_equal<20>(r);
         default: return false;
     }
 }
@@ -1457,20 +1504,14 @@ void Toeplitz::finish(cudaStream_t s) {
     if (d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
         throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
     ct1 = (L1 == 1458 || ct_schedule_matches((int)L1, r1_)) ? (int)L1 : 0;
-    ct2 = L2 == 144 ? 144 : 0;
-    ct3 = M3 == 729 ? 729 : 0;
+    ct2 = (L2 == 144 || ct_dim2_matches((int)L2, r2_)) ? (int)L2 : 0;
+    ct3 = M3 == 729 ? 729 : (ct_row_matches((int)M3, fft_schedule((int)M3, false)) ? (int)M3 : 0);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
     const int smem_d2 = d2_smem_values((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
     auto attr = [](const void *f, int bytes) { raise_smem_limit(f, bytes); };
-    attr((const void *)k_r2c_rows<0>, smem_rows);
-    attr((const void *)k_r2c_rows<729>, smem_rows);
-    attr((const void *)k_c2r_rows<0>, smem_rows);
-    attr((const void *)k_c2r_rows<729>, smem_rows);
-    attr((const void *)k_dim2_fwd<0>, smem_d2);
-    attr((const void *)k_dim2_fwd<144>, smem_d2);
-    attr((const void *)k_dim2_inv<0>, smem_d2);
-    attr((const void *)k_dim2_inv<144>, smem_d2);
+    raise_rows_smem(smem_rows);
+    raise_d2_smem(smem_d2);
     attr((const void *)k_pencil<false, 0>, smem_pen);
     attr((const void *)k_pencil<true, 0>, smem_pen);
     attr((const void *)k_pencil<false, 1458>, smem_pen);
@@ -1559,6 +1600,78 @@ static void launch_pencil(int ct1, unsigned grid, int smem, cudaStream_t s, floa
     }
 }
 
+// the n2-pass kernels of the operator's n2 length (ct2: a compile-time length, 0
+// = runtime schedule)
+#define LAMINO_D2_LENGTHS(X) X(144) X(90) X(64) X(48) X(20) X(0)
+static void launch_dim2_fwd(int ct2, dim3 grid, int kb, int smem, cudaStream_t s, const float2 *z1, int n1, int n2,
+                            int l3h, int np1, const FftLen &f2, const float2 *tw2, float2 *xa) {
+    switch (ct2) {
+#define LAMINO_D2F(N)                                                                                           \
+    case N:                                                                                                     \
+        k_dim2_fwd<N><<<grid, N == 0 ? 256 : d2_threads(N, kb), smem, s>>>(z1, n1, n2, l3h, np1, f2, tw2, kb, xa); \
+        break;
+        LAMINO_D2_LENGTHS(LAMINO_D2F)
+#undef LAMINO_D2F
+        default: throw Error(ERR_STATE, "no n2-pass kernel for this length");
+    }
+}
+static void launch_dim2_inv(int ct2, dim3 grid, int kb, int smem, cudaStream_t s, const float2 *xa, int n1, int n2,
+                            int l3h, int np1, const FftLen &f2, const float2 *tw2, float2 *z1) {
+    switch (ct2) {
+#define LAMINO_D2I(N)                                                                                           \
+    case N:                                                                                                     \
+        k_dim2_inv<N><<<grid, N == 0 ? 256 : d2_threads(N, kb), smem, s>>>(xa, n1, n2, l3h, np1, f2, tw2, kb, z1); \
+        break;
+        LAMINO_D2_LENGTHS(LAMINO_D2I)
+#undef LAMINO_D2I
+        default: throw Error(ERR_STATE, "no n2-pass kernel for this length");
+    }
+}
+static void raise_d2_smem(int bytes) {
+#define LAMINO_D2_ATTR(N)                                           \
+    raise_smem_limit((const void *)k_dim2_fwd<N>, bytes);           \
+    raise_smem_limit((const void *)k_dim2_inv<N>, bytes);
+    LAMINO_D2_LENGTHS(LAMINO_D2_ATTR)
+#undef LAMINO_D2_ATTR
+}
+
+// the row kernels of the operator's packed n3 length (ct3: compile-time 729 or
+// a CtRowSched length, 0 = runtime schedule)
+#define LAMINO_ROW_LENGTHS(X) X(729) X(375) X(270) X(180) X(90) X(0)
+static void launch_r2c(int ct3, unsigned grid, int rows, int smem, cudaStream_t s, const float *x, int64_t nrows,
+                       int n3, const FftLen &f3, const int *pos3, const float2 *twh3, float2 *z1) {
+    switch (ct3) {
+#define LAMINO_R2C(N)                                                                                         \
+    case N:                                                                                                   \
+        k_r2c_rows<N><<<grid, rows_threads(N == 0 ? 1 : N, rows), smem, s>>>(x, nrows, n3, f3, pos3, twh3, rows, \
+                                                                             z1);                             \
+        break;
+        LAMINO_ROW_LENGTHS(LAMINO_R2C)
+#undef LAMINO_R2C
+        default: throw Error(ERR_STATE, "no row kernel for this length");
+    }
+}
+static void launch_c2r(int ct3, unsigned grid, int rows, int smem, cudaStream_t s, const float2 *z1, int64_t nrows,
+                       int n3, const FftLen &f3, const int *pos3, const float2 *twh3, float *y) {
+    switch (ct3) {
+#define LAMINO_C2R(N)                                                                                         \
+    case N:                                                                                                   \
+        k_c2r_rows<N><<<grid, rows_threads(N == 0 ? 1 : N, rows), smem, s>>>(z1, nrows, n3, f3, pos3, twh3, rows, \
+                                                                             y);                              \
+        break;
+        LAMINO_ROW_LENGTHS(LAMINO_C2R)
+#undef LAMINO_C2R
+        default: throw Error(ERR_STATE, "no row kernel for this length");
+    }
+}
+static void raise_rows_smem(int bytes) {
+#define LAMINO_ROWS_ATTR(N)                                           \
+    raise_smem_limit((const void *)k_r2c_rows<N>, bytes);             \
+    raise_smem_limit((const void *)k_c2r_rows<N>, bytes);
+    LAMINO_ROW_LENGTHS(LAMINO_ROWS_ATTR)
+#undef LAMINO_ROWS_ATTR
+}
+
 void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     if (!z1.p || !xa.p) throw Error(ERR_STATE, "Toeplitz operator has no work buffers");
     const bool prof = profiling && (size_t)(nprof + 1) * (NSTAGE + 1) <= ev.size();
@@ -1572,12 +1685,10 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
     const unsigned gpen = (unsigned)(L2 * L3h);
     if (prof) LAMINO_CUDA(cudaEventRecord(E[0], s));
-    if (ct3) k_r2c_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
-    else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    launch_r2c(ct3, grows, rows1, smem_rows, s, x3, nrows, n3, f3, pos3.p, twh3.p, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[1], s));
-    if (ct2) k_dim2_fwd<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
-    else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    launch_dim2_fwd(ct2, gd2, kb2, smem_d2, s, z1.p, n1, n2, l3h, np1, f2, tw2.p, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[2], s));
     const bool h = precision == PREC_FP16 || (precision == PREC_MIXED && low);
@@ -1585,12 +1696,10 @@ void Toeplitz::apply(const float *x3, float *y3, cudaStream_t s, bool low) {
     else launch_pencil<false>(ct1, gpen, smem_pen, s, xa.p, n1, np1, l2, l3h, f1, tw1.p, K.p, nullptr, nullptr);
     LAMINO_LAUNCH("k_pencil");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[3], s));
-    if (ct2) k_dim2_inv<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
-    else k_dim2_inv<0><<<gd2, 256, smem_d2, s>>>(xa.p, n1, n2, l3h, np1, f2, tw2.p, kb2, z1.p);
+    launch_dim2_inv(ct2, gd2, kb2, smem_d2, s, xa.p, n1, n2, l3h, np1, f2, tw2.p, z1.p);
     LAMINO_LAUNCH("k_dim2_inv");
     if (prof) LAMINO_CUDA(cudaEventRecord(E[4], s));
-    if (ct3) k_c2r_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
-    else k_c2r_rows<0><<<grows, 256, smem_rows, s>>>(z1.p, nrows, n3, f3, pos3.p, twh3.p, rows1, y3);
+    launch_c2r(ct3, grows, rows1, smem_rows, s, z1.p, nrows, n3, f3, pos3.p, twh3.p, y3);
     LAMINO_LAUNCH("k_c2r_rows");
     if (prof) {
         LAMINO_CUDA(cudaEventRecord(E[5], s));
@@ -1615,11 +1724,9 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
     const dim3 gd2((unsigned)((vol.n1 + D2_IB - 1) / D2_IB), (unsigned)((L3h + kb2 - 1) / kb2), 3);
     const int n1 = (int)vol.n1, n2 = (int)vol.n2, n3 = (int)vol.n3, l2 = (int)L2, l3h = (int)L3h, np1 = (int)n1p;
     const unsigned gpen = (unsigned)(L2 * L3h);
-    if (ct3) k_r2c_rows<729><<<grows, rows_threads(729, rows1), smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
-    else k_r2c_rows<0><<<grows, 256, smem_rows, s>>>(x3, nrows, n3, f3, pos3.p, twh3.p, rows1, z1.p);
+    launch_r2c(ct3, grows, rows1, smem_rows, s, x3, nrows, n3, f3, pos3.p, twh3.p, z1.p);
     LAMINO_LAUNCH("k_r2c_rows");
-    if (ct2) k_dim2_fwd<144><<<gd2, d2_threads(l2, kb2), smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
-    else k_dim2_fwd<0><<<gd2, 256, smem_d2, s>>>(z1.p, n1, n2, l3h, np1, f2, tw2.p, kb2, xa.p);
+    launch_dim2_fwd(ct2, gd2, kb2, smem_d2, s, z1.p, n1, n2, l3h, np1, f2, tw2.p, xa.p);
     LAMINO_LAUNCH("k_dim2_fwd");
     for (size_t g0 = 0; g0 < parts.size(); g0 += kMaxQuadSets) {
         QuadSets qs{};
@@ -1646,20 +1753,14 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
 
 void Toeplitz::set_shape(int rows, int kb) {
     if (rows < 1 || kb < 1) throw Error(ERR_ARG, "launch shape values must be positive");
-    if (ct3 && rows > 8) throw Error(ERR_ARG, "rows of 729 run one warp per row, at most 8 per CTA");
+    if (ct3 == 729 && rows > 8) throw Error(ERR_ARG, "rows of 729 run one warp per row, at most 8 per CTA");
     const int64_t smem_rows = (int64_t)rows * L3h * (int64_t)sizeof(float2);
     const int64_t smem_d2 = (int64_t)d2_smem_values((int)L2, kb) * (int64_t)sizeof(float2);
     if (smem_rows > 200 * 1024 || smem_d2 > 200 * 1024) throw Error(ERR_ARG, "launch shape exceeds shared memory");
     rows1 = rows;
     kb2 = kb;
-    raise_smem_limit((const void *)k_r2c_rows<0>, (int)smem_rows);
-    raise_smem_limit((const void *)k_r2c_rows<729>, (int)smem_rows);
-    raise_smem_limit((const void *)k_c2r_rows<0>, (int)smem_rows);
-    raise_smem_limit((const void *)k_c2r_rows<729>, (int)smem_rows);
-    raise_smem_limit((const void *)k_dim2_fwd<0>, (int)smem_d2);
-    raise_smem_limit((const void *)k_dim2_fwd<144>, (int)smem_d2);
-    raise_smem_limit((const void *)k_dim2_inv<0>, (int)smem_d2);
-    raise_smem_limit((const void *)k_dim2_inv<144>, (int)smem_d2);
+    raise_rows_smem((int)smem_rows);
+    raise_d2_smem((int)smem_d2);
 }
 
 namespace {

@@ -257,12 +257,14 @@ def test_full_size_toeplitz_properties(L):
 
 
 @pytest.mark.parametrize("dims", [(721, 3, 8), (5, 71, 9), (4, 3, 721), (721, 71, 9), (90, 3, 8), (180, 3, 8),
-                                  (270, 3, 8), (362, 3, 8)])
+                                  (270, 3, 8), (362, 3, 8), (4, 10, 90), (4, 22, 180), (4, 32, 270),
+                                  (4, 44, 362)])
 def test_toeplitz_compiled_fft_lengths(L, O, dims):
     """Thin volumes whose FFT lengths hit the compile-time schedules (n1 = 721 ->
     1458, n2 = 71 -> 144, n3 = 721 -> packed 729; n1 = 90 / 180 / 270 / 362 ->
-    180 / 360 / 540 / 750, the lateral lengths of the batched mix) against the
-    oracle.  The
+    180 / 360 / 540 / 750, n2 = 10 / 22 / 32 / 44 -> 20 / 48 / 64 / 90 and n3 =
+    90 / 180 / 270 / 362 -> packed 90 / 180 / 270 / 375, the lengths of the
+    batched mix) against the oracle.  The
     Toeplitz form evaluates the exact lattice, so the oracle here uses FP64
     points (the reference's double path): with white input on a 721-long axis
     the float32 points of the float path move the highest modes' phases by about
