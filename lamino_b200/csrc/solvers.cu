@@ -223,6 +223,99 @@ __global__ void __launch_bounds__(kVoxX) k_qggmrf(float *__restrict__ g, const f
     }
 }
 
+// The same sums with each neighbour pair's derivative evaluated once.
+// rho'(-delta) = -rho'(delta) exactly in float for delta != 0 (the sign only
+// flips a product), and both sides take rho'(0) = q / (sigma^q C) at delta = 0,
+// so the 13 "forward" directions (dx = +1, and dx = 0 with (dy, dz) after
+// (0, 0)) give every pair: the owner c keeps rho'(x[c+d] - x[c]) for its own
+// sum and leaves the other side's term in shared memory.  A CTA owns a tile of
+// QG_TJ x QG_TK columns (j, k) and marches through a run of planes i; its
+// threads cover the tile plus a one-column halo, whose pairs reach into the
+// tile.  The 26 terms of every voxel are added in the direct kernel's order
+// (dx, dy, dz from -1 to 1), so the sums are the same.
+constexpr int QG_TJ = 12, QG_TK = 32;  // 476 threads, 42 KB of shared memory
+constexpr int QG_HJ = QG_TJ + 2, QG_HK = QG_TK + 2, QG_THREADS = QG_HJ * QG_HK;
+
+__global__ void __launch_bounds__(QG_THREADS) k_qggmrf_pairs(float *__restrict__ g, const float *__restrict__ x,
+                                                             int n1, int n2, int n3, QgConst kq) {
+    __shared__ float q9[2][9][QG_THREADS];  // other-side terms of the dx = +1 pairs, planes i - 1 and i
+    __shared__ float q4[4][QG_THREADS];     // other-side terms of the dx = 0 forward pairs, plane i
+    const int t = threadIdx.x;
+    const int tx = t % QG_HK, ty = t / QG_HK;
+    const int k = blockIdx.x * QG_TK - 1 + tx, j = blockIdx.y * QG_TJ - 1 + ty;
+    const bool col = j >= 0 && j < n2 && k >= 0 && k < n3;
+    const bool fin = tx >= 1 && tx <= QG_TK && ty >= 1 && ty <= QG_TJ && j >= 1 && j <= n2 - 2 && k >= 1 &&
+                     k <= n3 - 2;
+    const int64_t sj = n3, si = (int64_t)n2 * n3;
+    const PlaneRun pr(n1);
+    float p9[9], p4[4];
+    // own derivatives of plane i's forward pairs; other sides into shared memory
+    auto pairs = [&](int i, int buf, bool with4) {
+        if (!col || i < 0 || i >= n1) return;
+        const int64_t c = i * si + j * sj + k;
+        const float u = x[c];
+        if (i + 1 < n1) {
+#pragma unroll
+            for (int dy = -1; dy < 2; ++dy)
+#pragma unroll
+                for (int dz = -1; dz < 2; ++dz) {
+                    const int e = (dy + 1) * 3 + (dz + 1);
+                    if (j + dy < 0 || j + dy >= n2 || k + dz < 0 || k + dz >= n3) continue;
+                    const float delta = x[c + si + dy * sj + dz] - u;
+                    const float pv = d_potential(delta, kq);
+                    p9[e] = pv;
+                    q9[buf][e][t] = !(fabsf(delta) > 0.f) ? kq.at_zero : -pv;
+                }
+        }
+        if (with4) {
+            const int dys[4] = {0, 1, 1, 1}, dzs[4] = {1, -1, 0, 1};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int dy = dys[e], dz = dzs[e];
+                if (j + dy >= n2 || k + dz < 0 || k + dz >= n3) continue;
+                const float delta = x[c + dy * sj + dz] - u;
+                const float pv = d_potential(delta, kq);
+                p4[e] = pv;
+                q4[e][t] = !(fabsf(delta) > 0.f) ? kq.at_zero : -pv;
+            }
+        }
+    };
+    int buf = 0;
+    pairs(pr.z0 - 1, buf, false);  // plane z0 - 1's dx = +1 pairs feed plane z0
+    for (int i = pr.z0; i < pr.z1; ++i) {
+        buf ^= 1;
+        pairs(i, buf, true);
+        __syncthreads();
+        if (fin && i >= 1 && i <= n1 - 2) {
+            const int pb = buf ^ 1;
+            float sum = 0.f;
+            // dx = -1: pairs owned by plane i - 1, at column (j + dy, k + dz), direction (1, -dy, -dz)
+#pragma unroll
+            for (int dy = -1; dy < 2; ++dy)
+#pragma unroll
+                for (int dz = -1; dz < 2; ++dz)
+                    sum += c_qggmrf_w[(dy + 1) * 3 + (dz + 1)] *
+                           q9[pb][(1 - dy) * 3 + (1 - dz)][t + dy * QG_HK + dz];
+            // dx = 0, dy = -1: owned by (j - 1, k + dz), direction (0, 1, -dz)
+            sum += c_qggmrf_w[9] * q4[3][t - QG_HK - 1];
+            sum += c_qggmrf_w[10] * q4[2][t - QG_HK];
+            sum += c_qggmrf_w[11] * q4[1][t - QG_HK + 1];
+            // dx = 0, dy = 0: (0, 0, -1) owned by (j, k - 1); (0, 0, 1) own
+            sum += c_qggmrf_w[12] * q4[0][t - 1];
+            sum += c_qggmrf_w[14] * p4[0];
+            // dx = 0, dy = 1: own
+            sum += c_qggmrf_w[15] * p4[1];
+            sum += c_qggmrf_w[16] * p4[2];
+            sum += c_qggmrf_w[17] * p4[3];
+            // dx = +1: own
+#pragma unroll
+            for (int e = 0; e < 9; ++e) sum += c_qggmrf_w[18 + e] * p9[e];
+            g[i * si + j * sj + k] += sum;
+        }
+        __syncthreads();
+    }
+}
+
 void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStream_t s) {
     if (d.n1 < 3 || d.n2 < 3 || d.n3 < 3) return;  // no interior voxels
     float sigma_q = std::pow(sigma, 2.0f);
@@ -232,8 +325,12 @@ void qggmrf_add(float *g, const float *x, Dims3 d, float sigma, float p, cudaStr
     kq.inv_sqp = (float)(1.0 / (double)sigma_qp);
     kq.inv_sq = (float)(1.0 / (double)sigma_q);
     kq.at_zero = (float)(2.0 / ((double)sigma_q * 0.001));
-    k_qggmrf<<<vox_grid(d, 1), kVoxX, 0, s>>>(g, x, (int)d.n1, (int)d.n2, (int)d.n3, kq);
-    LAMINO_LAUNCH("k_qggmrf");
+    if (d.n2 > (int64_t)65535 * QG_TJ) throw Error(ERR_ARG, "n2 too large for the qGGMRF kernel");
+    const int64_t gx = (d.n3 + QG_TK - 1) / QG_TK, gy = (d.n2 + QG_TJ - 1) / QG_TJ;
+    const int64_t gz = std::max<int64_t>(1, std::min<int64_t>({d.n1, 65535, 148LL * 6 / (gx * gy) + 1}));
+    k_qggmrf_pairs<<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), QG_THREADS, 0, s>>>(g, x, (int)d.n1, (int)d.n2,
+                                                                                        (int)d.n3, kq);
+    LAMINO_LAUNCH("k_qggmrf_pairs");
 }
 
 // ---------------------------------------------------------------------------
