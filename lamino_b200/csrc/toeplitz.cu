@@ -1790,7 +1790,7 @@ double Toeplitz::autotune(cudaStream_t s) {
     const bool was_prof = profiling;
     profiling = false;
     for (int rows : {2, 4, 8}) {
-        for (int kb : {2, 4}) {
+        for (int kb : {2, 4, 8}) {
             try {
                 set_shape(rows, kb);
             } catch (const Error &) {
