@@ -14,50 +14,20 @@ def test_qggmrf_vs_reference(L, gold_ref):
     assert rel(g, gold_ref["qg_g"]) < 1e-6
 
 
-def _qggmrf_f32(x, sigma, p):
-    """The direct 26-neighbour sum in float32 (src/qggmrf.cpp:60-95 with the
-    derivative of src/qggmrf.cpp:42-57 in float), interior voxels only."""
-    w = np.array([0.0302, 0.037, 0.0302, 0.037, 0.0523, 0.037, 0.0302, 0.037, 0.0302,
-                  0.037, 0.0523, 0.037, 0.0532, 0.0, 0.0523, 0.037, 0.0523, 0.037,
-                  0.0302, 0.037, 0.0302, 0.037, 0.0523, 0.037, 0.0302, 0.037, 0.0302], np.float32)
-    f = np.float32
-    qmp = f(2.0) - f(p)
-    inv_sqp = f(1.0 / float(f(sigma) ** qmp))
-    inv_sq = f(1.0 / float(f(sigma) ** f(2.0)))
-    at_zero = f(2.0 / (float(f(sigma) ** f(2.0)) * 0.001))
-    u = x[1:-1, 1:-1, 1:-1]
-    out = np.zeros_like(u)
-    for dx in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dz in (-1, 0, 1):
-                if dx == dy == dz == 0:
-                    continue
-                v = x[1 + dx:x.shape[0] - 1 + dx, 1 + dy:x.shape[1] - 1 + dy, 1 + dz:x.shape[2] - 1 + dz]
-                d = (v - u).astype(np.float32)
-                ad = np.abs(d)
-                with np.errstate(divide="ignore", invalid="ignore"):
-                    t1 = np.power(ad, qmp, dtype=np.float32) * inv_sqp
-                    r = f(1.0) / (f(0.001) + t1)
-                    a = d * r * inv_sq
-                    dp = np.where(ad > 0, a * (f(2.0) - qmp * t1 * r), at_zero).astype(np.float32)
-                out += w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)] * dp
-    return out
-
-
 @pytest.mark.parametrize("dims", [(37, 29, 70), (300, 40, 100)])
-def test_qggmrf_tiles_and_plane_runs(L, dims):
+def test_qggmrf_tiles_and_plane_runs(L, O, dims):
     """qGGMRF at sizes with several CTA tiles (12 x 32 columns plus halo) and
-    runs of planes per CTA, against the direct float32 sum; includes equal
-    neighbours (delta = 0, where both sides of a pair take rho'(0))."""
+    runs of planes per CTA, against the oracle (src/qggmrf.cpp:60-95, pinned to
+    the reference's compiled code); includes equal neighbours (delta = 0, where
+    both sides of a pair take rho'(0))."""
     rng = np.random.default_rng(7)
     x = rng.standard_normal(dims).astype(np.float32)
     x[5:9, 3:6, 10:20] = 0.25  # a flat patch: delta = 0 pairs
-    g = rng.standard_normal(dims).astype(np.float32)
-    want = g.copy()
-    want[1:-1, 1:-1, 1:-1] += _qggmrf_f32(x, 1000.0, 1.2)
+    g = np.zeros(dims, np.float32)  # the increments alone (they are small beside O(1) values)
+    want = O.qggmrf(g, x, 1000.0, 1.2)
     L.opt.qggmrf(g, x, 1000.0, 1.2)
     assert rel(g, want) < 1e-6
-    assert np.array_equal(g[0], want[0]) and np.array_equal(g[:, :, -1], want[:, :, -1])  # borders untouched
+    assert not g[0].any() and not g[:, :, -1].any()  # borders untouched
 
 
 def test_laplacian_plane_runs(L, O):
