@@ -891,12 +891,248 @@ __device__ __forceinline__ void p1458_inverse(const PencilRows &rows, const floa
     }
 }
 
+// ---- n1 transforms of L = 2 A B in two register stages (the 270- and 362-voxel axes) ----
+// cos / sin of 2 pi m / R for the composite register DFTs (R = 15, 18, 25)
+__host__ __device__ constexpr float wr_c(int R, int m) {
+    if (R == 18) {
+        constexpr float t[18] = {
+        1.0f, 0.9396926207859084f, 0.766044443118978f, 0.5000000000000001f, 0.17364817766693041f,
+        -0.1736481776669303f, -0.4999999999999998f, -0.7660444431189779f, -0.9396926207859083f, -1.0f,
+        -0.9396926207859084f, -0.7660444431189783f, -0.5000000000000004f, -0.17364817766693033f,
+        0.17364817766692997f, 0.49999999999999933f, 0.7660444431189778f, 0.9396926207859084f};
+        return t[m];
+    }
+    if (R == 15) {
+        constexpr float t[15] = {
+        1.0f, 0.9135454576426009f, 0.6691306063588582f, 0.30901699437494745f, -0.10452846326765333f,
+        -0.4999999999999998f, -0.8090169943749473f, -0.9781476007338057f, -0.9781476007338057f,
+        -0.8090169943749476f, -0.5000000000000004f, -0.10452846326765423f, 0.30901699437494723f,
+        0.6691306063588585f, 0.913545457642601f};
+        return t[m];
+    }
+    if (R == 25) {
+        constexpr float t[25] = {
+        1.0f, 0.9685831611286311f, 0.8763066800438636f, 0.7289686274214116f, 0.5358267949789965f,
+        0.30901699437494745f, 0.06279051952931353f, -0.1873813145857246f, -0.4257792915650727f,
+        -0.6374239897486897f, -0.8090169943749473f, -0.9297764858882513f, -0.9921147013144778f,
+        -0.9921147013144779f, -0.9297764858882515f, -0.8090169943749478f, -0.6374239897486895f,
+        -0.42577929156507216f, -0.18738131458572463f, 0.06279051952931283f, 0.30901699437494723f,
+        0.5358267949789968f, 0.7289686274214112f, 0.8763066800438631f, 0.968583161128631f};
+        return t[m];
+    }
+    return 1.f;
+}
+__host__ __device__ constexpr float wr_s(int R, int m) {
+    if (R == 18) {
+        constexpr float t[18] = {
+        0.0f, 0.3420201433256687f, 0.6427876096865393f, 0.8660254037844386f, 0.984807753012208f,
+        0.984807753012208f, 0.8660254037844387f, 0.6427876096865395f, 0.3420201433256689f, 0.0f,
+        -0.34202014332566866f, -0.6427876096865389f, -0.8660254037844384f, -0.984807753012208f,
+        -0.9848077530122081f, -0.866025403784439f, -0.6427876096865396f, -0.3420201433256686f};
+        return t[m];
+    }
+    if (R == 15) {
+        constexpr float t[15] = {
+        0.0f, 0.40673664307580015f, 0.7431448254773941f, 0.9510565162951535f, 0.9945218953682734f,
+        0.8660254037844387f, 0.5877852522924732f, 0.20791169081775931f, -0.20791169081775907f, -0.587785252292473f,
+        -0.8660254037844384f, -0.9945218953682733f, -0.9510565162951536f, -0.743144825477394f, -0.40673664307580015f};
+        return t[m];
+    }
+    if (R == 25) {
+        constexpr float t[25] = {
+        0.0f, 0.2486898871648548f, 0.4817536741017153f, 0.6845471059286886f, 0.8443279255020151f,
+        0.9510565162951535f, 0.9980267284282716f, 0.9822872507286887f, 0.9048270524660195f, 0.7705132427757893f,
+        0.5877852522924732f, 0.36812455268467814f, 0.12533323356430454f, -0.12533323356430429f,
+        -0.3681245526846779f, -0.5877852522924727f, -0.7705132427757894f, -0.9048270524660198f,
+        -0.9822872507286887f, -0.9980267284282716f, -0.9510565162951536f, -0.844327925502015f, -0.684547105928689f,
+        -0.4817536741017161f, -0.24868988716485535f};
+        return t[m];
+    }
+    return 0.f;
+}
+
+// Composite register DFT of R1 R2 points (Cooley-Tukey, input i = R2 i1 + i2,
+// output k = k1 + R1 k2, twiddles W_R^(i2 k1) as constants).
+template <int R1, int R2, bool INV>
+__device__ __forceinline__ void dft_cs(float2 (&v)[R1 * R2]) {
+    constexpr int R = R1 * R2;
+    float2 a[R];
+#pragma unroll
+    for (int i2 = 0; i2 < R2; ++i2) {
+        float2 x[R1];
+#pragma unroll
+        for (int i1 = 0; i1 < R1; ++i1) x[i1] = v[R2 * i1 + i2];
+        dft_small<R1, INV>(x);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            const int m = (i2 * k1) % R;
+            a[i2 * R1 + k1] = m == 0 ? x[k1] : c_mul_k(x[k1], wr_c(R, m), INV ? wr_s(R, m) : -wr_s(R, m));
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        float2 y[R2];
+#pragma unroll
+        for (int i2 = 0; i2 < R2; ++i2) y[i2] = a[i2 * R1 + k1];
+        dft_small<R2, INV>(y);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = y[k2];
+    }
+}
+
+// register DFT of R points
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&v)[R]) {
+    if constexpr (R == 27) dft27<INV>(v);
+    else if constexpr (R == 25) dft_cs<5, 5, INV>(v);
+    else if constexpr (R == 15) dft_cs<3, 5, INV>(v);
+    else if constexpr (R == 18) dft_cs<2, 9, INV>(v);
+    else dft_small<R, INV>(v);
+}
+
+// v[k] *= (b w^(e k)) (INV: its conjugate), k < A, w = tw[1]: two table loads
+// (w^e, w^5e) and at most four products per value.
+template <int A, bool INV>
+__device__ __forceinline__ void twiddle_lin(const float2 *__restrict__ tw, int e, int L, float2 b, float2 (&v)[A]) {
+    constexpr int R0 = 5, R1 = (A + R0 - 1) / R0;
+    const float2 z = __ldg(tw + e % L), z5 = __ldg(tw + (5 * e) % L);
+    float2 p0[R0];
+    p0[0] = b;
+#pragma unroll
+    for (int k0 = 1; k0 < R0; ++k0) p0[k0] = c_mul(p0[k0 - 1], z);
+    float2 q = z5;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+#pragma unroll
+        for (int k0 = 0; k0 < R0; ++k0) {
+            const int k = k0 + R0 * k1;
+            if (k < A) {
+                const float2 t = k1 == 0 ? p0[k0] : c_mul(p0[k0], q);
+                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
+            }
+        }
+        if (k1 > 0) q = c_mul(q, z5);
+    }
+}
+
+// Forward n1 transform of L = 2 A B (the 1458 scheme of p1458_forward with A-
+// and B-point stages): six warps per pencil, warp (c, h); lane n < B takes
+// y_h[n + B j] = w^{h n} x_{n+B j} W_{2A}^{h j} (W_{2A} = w^B, from the table),
+// forms its A-point DFT, multiplies output k by w^{n (2k + h)} and stores it at
+// position A B h + n + B k; lane m < A then runs the B-point DFT of block m in
+// place.  DIF positions: fft_positions(L, {2, A, B}).
+template <int A, int B>
+__device__ __forceinline__ void p2s_forward(const PencilRows &rows, const float2 *__restrict__ tw,
+                                            float2 *__restrict__ sm) {
+    constexpr int M = A * B, L = 2 * M;
+    const int w = threadIdx.x >> 5, n = threadIdx.x & 31;
+    const int c = w >> 1, h = w & 1;
+    float2 *half = sm + c * L + h * M;
+    if (n < B) {
+        float2 v[A];
+#pragma unroll
+        for (int j = 0; j < A; ++j) v[j] = rows.get(c, n + B * j);
+        if (h) {
+#pragma unroll
+            for (int j = 1; j < A; ++j) v[j] = c_mul(v[j], __ldg(tw + B * j));
+        }
+        dft_reg<A, false>(v);
+        twiddle_lin<A, false>(tw, 2 * n, L, h ? __ldg(tw + n) : make_float2(1.f, 0.f), v);
+#pragma unroll
+        for (int k = 0; k < A; ++k) half[n + B * k] = v[k];
+    }
+    __syncthreads();
+    if (n < A) {
+        float2 *row = half + B * n;
+        float2 v[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) v[j] = row[j];
+        dft_reg<B, false>(v);
+#pragma unroll
+        for (int k = 0; k < B; ++k) row[k] = v[k];
+    }
+    __syncthreads();
+}
+
+// Its inverse and the pruned store of the first n1 values (the caller
+// synchronises after writing the spectrum).
+template <int A, int B>
+__device__ __forceinline__ void p2s_inverse(const PencilRows &rows, const float2 *__restrict__ tw,
+                                            float2 *__restrict__ sm) {
+    constexpr int M = A * B, L = 2 * M;
+    const int w = threadIdx.x >> 5, n = threadIdx.x & 31;
+    const int c = w >> 1, h = w & 1;
+    float2 *half = sm + c * L + h * M;
+    if (n < A) {
+        float2 *row = half + B * n;
+        float2 v[B];
+#pragma unroll
+        for (int k = 0; k < B; ++k) v[k] = row[k];
+        dft_reg<B, true>(v);
+#pragma unroll
+        for (int j = 0; j < B; ++j) row[j] = v[j];
+    }
+    __syncthreads();
+    float2 v[A];
+    if (n < B) {
+#pragma unroll
+        for (int k = 0; k < A; ++k) v[k] = half[n + B * k];
+        twiddle_lin<A, true>(tw, 2 * n, L, h ? __ldg(tw + n) : make_float2(1.f, 0.f), v);
+        dft_reg<A, true>(v);
+        if (h) {  // this half times conj(w^i) = conj(w^n) conj(W_{2A}^j); the first factor came with the twiddles
+#pragma unroll
+            for (int j = 0; j < A; ++j) half[n + B * j] = j ? c_mulc(v[j], __ldg(tw + B * j)) : v[j];
+        }
+    }
+    __syncthreads();
+    if (h == 0 && n < B) {
+        const float2 *other = half + M;
+#pragma unroll
+        for (int j = 0; j < A; ++j) {
+            const int i = n + B * j;
+            if (rows.want(i)) rows.put(c, i, c_add(v[j], other[i]));
+        }
+    }
+}
+
+// the n1 lengths run in two register stages, as (A, B); 1458 = 2 x 27 x 27 has its own
+// kernels (p1458_*) with constant W_54 tables
+template <int L>
+struct TwoStage {
+    static constexpr bool on = false;
+    static constexpr int A = 0, B = 0;
+};
+template <>
+struct TwoStage<750> {
+    static constexpr bool on = true;
+    static constexpr int A = 15, B = 25;
+};
+template <>
+struct TwoStage<540> {
+    static constexpr bool on = true;
+    static constexpr int A = 15, B = 18;
+};
+// (360 as 12 x 15 and 180 as 9 x 10 were slower than their compile-time
+// shared-memory schedules: too few lanes busy per warp)
+// threads of a pencil CTA: six warps for the register-stage lengths, 256 otherwise
+__host__ __device__ constexpr int pencil_threads(int L) {
+    return (L == 1458 || L == 750 || L == 540) ? P1458_THREADS : 256;
+}
+// the register-stage schedule (2, A, B) of an n1 length, empty when it has none
+static std::vector<int> two_stage_schedule(int L) {
+    switch (L) {
+        case 750: return {2, TwoStage<750>::A, TwoStage<750>::B};
+        case 540: return {2, TwoStage<540>::A, TwoStage<540>::B};
+        default: return {};
+    }
+}
+
 // B: one (p2, k3) pencil of the 3 components along n1: DIF (zero-padded), 3x3
 // symmetric multiply with the spectra (same position order), undo, first n1 kept.
 // In place on xa.  N1: compile-time L1 or 0.  At L1 = 1458, five CTAs of 256
 // threads per SM (48 registers, 35 KB of shared memory each); four otherwise.
 template <bool HALF, int N1>
-__global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
+__global__ void __launch_bounds__(pencil_threads(N1), 4) k_pencil(float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h, FftLen F1,
                                                 const float2 *__restrict__ tw1, const float *__restrict__ K,
                                                 const __half *__restrict__ Kh, const float *__restrict__ kscale) {
     extern __shared__ float2 sm[];
@@ -913,6 +1149,8 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(
     }
     if constexpr (N1 == 1458) {
         p1458_forward(PencilRows{pv, cs, n1}, tw1, sm);
+    } else if constexpr (TwoStage<N1>::on) {
+        p2s_forward<TwoStage<N1>::A, TwoStage<N1>::B>(PencilRows{pv, cs, n1}, tw1, sm);
     } else if constexpr (N1 != 0) {  // compile-time schedule: lead stages in registers, the rest fixed
         fftlead_load<CtSched<N1>::r[1]>(PencilRows{pv, cs, n1}, tw1, sm, N1, N1, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -990,6 +1228,8 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256, 4) k_pencil(
     __syncthreads();
     if constexpr (N1 == 1458) {
         p1458_inverse(PencilRows{pv, cs, n1}, tw1, sm);
+    } else if constexpr (TwoStage<N1>::on) {
+        p2s_inverse<TwoStage<N1>::A, TwoStage<N1>::B>(PencilRows{pv, cs, n1}, tw1, sm);
     } else if constexpr (N1 != 0) {
         ct_inverse<N1, CtSched<N1>::ns - 1, 2>(sm, 3, N1, tw1, threadIdx.x, blockDim.x);
         fftlead_store<CtSched<N1>::r[1]>(PencilRows{pv, cs, n1}, tw1, sm, N1, N1, threadIdx.x, blockDim.x);
@@ -1015,7 +1255,7 @@ struct QuadSets {
 };
 
 template <int N1>
-__global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256) k_pencil_quad(const float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h,
+__global__ void __launch_bounds__(pencil_threads(N1)) k_pencil_quad(const float2 *__restrict__ xa, int n1, int n1p, int L2, int L3h,
                                                      FftLen F1, const float2 *__restrict__ tw1, QuadSets ks, int ng,
                                                      double *__restrict__ acc) {
     extern __shared__ float2 sm[];
@@ -1027,6 +1267,8 @@ __global__ void __launch_bounds__(N1 == 1458 ? P1458_THREADS : 256) k_pencil_qua
     const float2 *pv = xa + pen * n1p;
     if constexpr (N1 == 1458) {
         p1458_forward(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm);  // reads only
+    } else if constexpr (TwoStage<N1>::on) {
+        p2s_forward<TwoStage<N1>::A, TwoStage<N1>::B>(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm);
     } else if constexpr (N1 != 0) {
         fftlead_load<CtSched<N1>::r[1]>(PencilRows{const_cast<float2 *>(pv), cs, n1}, tw1, sm, N1, N1,
                                         threadIdx.x, blockDim.x);
@@ -1385,7 +1627,10 @@ void Toeplitz::init_tables(Dims3 d, int prec) {
         upload(pos3.p, p3.data(), (size_t)M3);
     }
     // the compile-time n1 transform of 1458 runs the schedule 2, 27, 27 (p1458_forward)
-    r1_ = L1 == 1458 ? std::vector<int>{2, 27, 27} : r1;
+    // the n1 transforms with register stages run the schedules 2, 27, 27 (1458) and
+    // 2, A, B (TwoStage lengths)
+    const std::vector<int> r2s = two_stage_schedule((int)L1);
+    r1_ = L1 == 1458 ? std::vector<int>{2, 27, 27} : (r2s.empty() ? r1 : r2s);
     r2_ = r2;
 }
 
@@ -1503,7 +1748,7 @@ void Toeplitz::finish(cudaStream_t s) {
     while (kb2 > 1 && d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 160 * 1024) kb2 /= 2;
     if (d2_smem_values((int)L2, kb2) * (int64_t)sizeof(float2) > 200 * 1024)
         throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
-    ct1 = (L1 == 1458 || ct_schedule_matches((int)L1, r1_)) ? (int)L1 : 0;
+    ct1 = (L1 == 1458 || !two_stage_schedule((int)L1).empty() || ct_schedule_matches((int)L1, r1_)) ? (int)L1 : 0;
     ct2 = (L2 == 144 || ct_dim2_matches((int)L2, r2_)) ? (int)L2 : 0;
     ct3 = M3 == 729 ? 729 : (ct_row_matches((int)M3, fft_schedule((int)M3, false)) ? (int)M3 : 0);
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
@@ -1586,7 +1831,7 @@ static void launch_pencil(int ct1, unsigned grid, int smem, cudaStream_t s, floa
     switch (ct1) {
 #define LAMINO_PENCIL(N)                                                                                       \
     case N:                                                                                                    \
-        k_pencil<HALF, N><<<grid, N == 1458 ? P1458_THREADS : 256, smem, s>>>(xa, n1, np1, l2, l3h, f1, tw1, K, \
+        k_pencil<HALF, N><<<grid, pencil_threads(N), smem, s>>>(xa, n1, np1, l2, l3h, f1, tw1, K, \
                                                                               Kh, ksc);                        \
         break;
         LAMINO_PENCIL(1458)
@@ -1735,7 +1980,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
         switch (ct1) {
 #define LAMINO_QUAD(N)                                                                                          \
     case N:                                                                                                     \
-        k_pencil_quad<N><<<gpen, N == 1458 ? P1458_THREADS : 256, smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1,    \
+        k_pencil_quad<N><<<gpen, pencil_threads(N), smem_pen, s>>>(xa.p, n1, np1, l2, l3h, f1,    \
                                                                               tw1.p, qs, ng, acc + 3 * g0); \
         break;
             LAMINO_QUAD(1458)
