@@ -224,6 +224,130 @@ __device__ __forceinline__ void rows729_store(const float2 *__restrict__ sm, int
     }
 }
 
+// ---- register DFTs of composite lengths (two-stage row and pencil transforms) ----
+// cos / sin of 2 pi m / R for the composite register DFTs (R = 15, 18, 25)
+__host__ __device__ constexpr float wr_c(int R, int m) {
+    if (R == 18) {
+        constexpr float t[18] = {
+        1.0f, 0.9396926207859084f, 0.766044443118978f, 0.5000000000000001f, 0.17364817766693041f,
+        -0.1736481776669303f, -0.4999999999999998f, -0.7660444431189779f, -0.9396926207859083f, -1.0f,
+        -0.9396926207859084f, -0.7660444431189783f, -0.5000000000000004f, -0.17364817766693033f,
+        0.17364817766692997f, 0.49999999999999933f, 0.7660444431189778f, 0.9396926207859084f};
+        return t[m];
+    }
+    if (R == 15) {
+        constexpr float t[15] = {
+        1.0f, 0.9135454576426009f, 0.6691306063588582f, 0.30901699437494745f, -0.10452846326765333f,
+        -0.4999999999999998f, -0.8090169943749473f, -0.9781476007338057f, -0.9781476007338057f,
+        -0.8090169943749476f, -0.5000000000000004f, -0.10452846326765423f, 0.30901699437494723f,
+        0.6691306063588585f, 0.913545457642601f};
+        return t[m];
+    }
+    if (R == 25) {
+        constexpr float t[25] = {
+        1.0f, 0.9685831611286311f, 0.8763066800438636f, 0.7289686274214116f, 0.5358267949789965f,
+        0.30901699437494745f, 0.06279051952931353f, -0.1873813145857246f, -0.4257792915650727f,
+        -0.6374239897486897f, -0.8090169943749473f, -0.9297764858882513f, -0.9921147013144778f,
+        -0.9921147013144779f, -0.9297764858882515f, -0.8090169943749478f, -0.6374239897486895f,
+        -0.42577929156507216f, -0.18738131458572463f, 0.06279051952931283f, 0.30901699437494723f,
+        0.5358267949789968f, 0.7289686274214112f, 0.8763066800438631f, 0.968583161128631f};
+        return t[m];
+    }
+    return 1.f;
+}
+__host__ __device__ constexpr float wr_s(int R, int m) {
+    if (R == 18) {
+        constexpr float t[18] = {
+        0.0f, 0.3420201433256687f, 0.6427876096865393f, 0.8660254037844386f, 0.984807753012208f,
+        0.984807753012208f, 0.8660254037844387f, 0.6427876096865395f, 0.3420201433256689f, 0.0f,
+        -0.34202014332566866f, -0.6427876096865389f, -0.8660254037844384f, -0.984807753012208f,
+        -0.9848077530122081f, -0.866025403784439f, -0.6427876096865396f, -0.3420201433256686f};
+        return t[m];
+    }
+    if (R == 15) {
+        constexpr float t[15] = {
+        0.0f, 0.40673664307580015f, 0.7431448254773941f, 0.9510565162951535f, 0.9945218953682734f,
+        0.8660254037844387f, 0.5877852522924732f, 0.20791169081775931f, -0.20791169081775907f, -0.587785252292473f,
+        -0.8660254037844384f, -0.9945218953682733f, -0.9510565162951536f, -0.743144825477394f, -0.40673664307580015f};
+        return t[m];
+    }
+    if (R == 25) {
+        constexpr float t[25] = {
+        0.0f, 0.2486898871648548f, 0.4817536741017153f, 0.6845471059286886f, 0.8443279255020151f,
+        0.9510565162951535f, 0.9980267284282716f, 0.9822872507286887f, 0.9048270524660195f, 0.7705132427757893f,
+        0.5877852522924732f, 0.36812455268467814f, 0.12533323356430454f, -0.12533323356430429f,
+        -0.3681245526846779f, -0.5877852522924727f, -0.7705132427757894f, -0.9048270524660198f,
+        -0.9822872507286887f, -0.9980267284282716f, -0.9510565162951536f, -0.844327925502015f, -0.684547105928689f,
+        -0.4817536741017161f, -0.24868988716485535f};
+        return t[m];
+    }
+    return 0.f;
+}
+
+// Composite register DFT of R1 R2 points (Cooley-Tukey, input i = R2 i1 + i2,
+// output k = k1 + R1 k2, twiddles W_R^(i2 k1) as constants).
+template <int R1, int R2, bool INV>
+__device__ __forceinline__ void dft_cs(float2 (&v)[R1 * R2]) {
+    constexpr int R = R1 * R2;
+    float2 a[R];
+#pragma unroll
+    for (int i2 = 0; i2 < R2; ++i2) {
+        float2 x[R1];
+#pragma unroll
+        for (int i1 = 0; i1 < R1; ++i1) x[i1] = v[R2 * i1 + i2];
+        dft_small<R1, INV>(x);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            const int m = (i2 * k1) % R;
+            a[i2 * R1 + k1] = m == 0 ? x[k1] : c_mul_k(x[k1], wr_c(R, m), INV ? wr_s(R, m) : -wr_s(R, m));
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        float2 y[R2];
+#pragma unroll
+        for (int i2 = 0; i2 < R2; ++i2) y[i2] = a[i2 * R1 + k1];
+        dft_small<R2, INV>(y);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = y[k2];
+    }
+}
+
+// register DFT of R points
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2 (&v)[R]) {
+    if constexpr (R == 27) dft27<INV>(v);
+    else if constexpr (R == 25) dft_cs<5, 5, INV>(v);
+    else if constexpr (R == 15) dft_cs<3, 5, INV>(v);
+    else if constexpr (R == 18) dft_cs<2, 9, INV>(v);
+    else dft_small<R, INV>(v);
+}
+
+// v[k] *= (b w^(e k)) (INV: its conjugate), k < A, w = tw[1]: two table loads
+// (w^e, w^5e) and at most four products per value.
+template <int A, bool INV>
+__device__ __forceinline__ void twiddle_lin(const float2 *__restrict__ tw, int e, int L, float2 b, float2 (&v)[A]) {
+    constexpr int R0 = 5, R1 = (A + R0 - 1) / R0;
+    const float2 z = __ldg(tw + e % L), z5 = __ldg(tw + (5 * e) % L);
+    float2 p0[R0];
+    p0[0] = b;
+#pragma unroll
+    for (int k0 = 1; k0 < R0; ++k0) p0[k0] = c_mul(p0[k0 - 1], z);
+    float2 q = z5;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+#pragma unroll
+        for (int k0 = 0; k0 < R0; ++k0) {
+            const int k = k0 + R0 * k1;
+            if (k < A) {
+                const float2 t = k1 == 0 ? p0[k0] : c_mul(p0[k0], q);
+                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
+            }
+        }
+        if (k1 > 0) q = c_mul(q, z5);
+    }
+}
+
 // Rows of M3 = 729 as 27 x 27 (schedule 27, 27; positions
 // fft_positions(729, {27, 27})): one warp per row, lanes 0..26 busy.  The first
 // stage (27-point DFTs over the packed values n + 27 j, twiddles w729^{n k})
@@ -287,16 +411,96 @@ __device__ __forceinline__ void rows27_store(const float2 *__restrict__ sm, int 
     }
 }
 
+// Rows of M3 = A B in the same two register stages (schedule A, B; positions
+// fft_positions(M3, {A, B})): one warp per row; lane n < B takes the packed
+// values n + B j (j < A), lane b < A the B-point block b.
+template <int M3>
+struct RowTwo {
+    static constexpr bool on = false;
+    static constexpr int A = 0, B = 0;
+};
+template <>
+struct RowTwo<375> {
+    static constexpr bool on = true;
+    static constexpr int A = 15, B = 25;
+};
+template <>
+struct RowTwo<270> {
+    static constexpr bool on = true;
+    static constexpr int A = 15, B = 18;
+};
+
+template <int A, int B>
+__device__ __forceinline__ void rows2s_load(const float *__restrict__ xb, int nr, int n3,
+                                            const float2 *__restrict__ tw3, float2 *__restrict__ sm, int ps) {
+    const int r = threadIdx.x >> 5, n = threadIdx.x & 31;
+    if (r < nr && n < B) {
+        const float *xr = xb + (int64_t)r * n3;
+        float2 v[A];
+#pragma unroll
+        for (int j = 0; j < A; ++j) {
+            const int i = 2 * (n + B * j);
+            v[j].x = i < n3 ? xr[i] : 0.f;
+            v[j].y = i + 1 < n3 ? xr[i + 1] : 0.f;
+        }
+        dft_reg<A, false>(v);
+        twiddle_lin<A, false>(tw3, n, A * B, make_float2(1.f, 0.f), v);
+        float2 *sp = sm + r * ps + n;
+#pragma unroll
+        for (int k = 0; k < A; ++k) sp[B * k] = v[k];
+    }
+    __syncthreads();
+}
+
+template <int A, int B, bool INV>
+__device__ __forceinline__ void rows2s_mid(float2 *__restrict__ sm, int nr, int ps) {
+    const int r = threadIdx.x >> 5, b = threadIdx.x & 31;
+    if (r < nr && b < A) {
+        float2 *row = sm + r * ps + B * b;
+        float2 v[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) v[j] = row[j];
+        dft_reg<B, INV>(v);
+#pragma unroll
+        for (int k = 0; k < B; ++k) row[k] = v[k];
+    }
+    __syncthreads();
+}
+
+template <int A, int B>
+__device__ __forceinline__ void rows2s_store(const float2 *__restrict__ sm, int nr, int ps, int n3,
+                                             const float2 *__restrict__ tw3, float *__restrict__ yb) {
+    const int r = threadIdx.x >> 5, n = threadIdx.x & 31;
+    if (r < nr && n < B) {
+        const float2 *sp = sm + r * ps + n;
+        float2 v[A];
+#pragma unroll
+        for (int k = 0; k < A; ++k) v[k] = sp[B * k];
+        twiddle_lin<A, true>(tw3, n, A * B, make_float2(1.f, 0.f), v);
+        dft_reg<A, true>(v);
+        float *yr = yb + (int64_t)r * n3;
+#pragma unroll
+        for (int j = 0; j < A; ++j) {
+            const int i = 2 * (n + B * j);
+            if (i < n3) yr[i] = v[j].x;
+            if (i + 1 < n3) yr[i + 1] = v[j].y;
+        }
+    }
+}
+
 // DIF position of packed frequency k: digit reversal of k = k0 + 27 k1 for the
 // 27 x 27 schedule of 729, the table otherwise
 template <int N3>
 __device__ __forceinline__ int row_pos(const int *__restrict__ pos3, int k) {
     if constexpr (N3 == 729) return 27 * (k % 27) + k / 27;
+    else if constexpr (RowTwo<N3>::on) return RowTwo<N3>::B * (k % RowTwo<N3>::A) + k / RowTwo<N3>::A;
     else return __ldg(pos3 + k);
 }
 
-// threads of a rows CTA of R rows: one warp per row for M3 = 729
-__host__ __device__ constexpr int rows_threads(int M3, int R) { return M3 == 729 && R <= 8 ? 32 * R : 256; }
+// rows with a warp per row: 729 and the two-register-stage lengths
+__host__ __device__ constexpr bool warp_rows(int M3) { return M3 == 729 || M3 == 375 || M3 == 270; }
+// threads of a rows CTA of R rows: one warp per row where the lengths run in registers
+__host__ __device__ constexpr int rows_threads(int M3, int R) { return warp_rows(M3) && R <= 8 ? 32 * R : 256; }
 
 // The first stage of a runtime-length row transform (radix R0 over the whole
 // packed row of M3, m0 = M3 / R0 offsets) in registers on the way in and its
@@ -379,7 +583,7 @@ __device__ __forceinline__ void rowslead_any(const FftLen &F3, const float *xb, 
 // A1: real rows along n3 (zero-padded to L3) -> half spectrum k3 in [0, M3], via the
 // packed-complex M3-point DIF and the even/odd split.  N3: compile-time M3 or 0.
 template <int N3>
-__global__ void __launch_bounds__(256, N3 == 729 ? 3 : 4) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
+__global__ void __launch_bounds__(256, warp_rows(N3) ? 3 : 4) k_r2c_rows(const float *__restrict__ x, int64_t nrows, int n3, FftLen F3,
                                                   const int *__restrict__ pos3, const float2 *__restrict__ twh,
                                                   int R, float2 *__restrict__ z1) {
     extern __shared__ float2 sm[];
@@ -390,6 +594,9 @@ __global__ void __launch_bounds__(256, N3 == 729 ? 3 : 4) k_r2c_rows(const float
     if constexpr (N3 == 729) {
         rows27_load(x + row0 * n3, nr, n3, F3.tw, sm, ps);
         rows27_mid<false>(sm, nr, ps);
+    } else if constexpr (RowTwo<N3>::on) {
+        rows2s_load<RowTwo<N3>::A, RowTwo<N3>::B>(x + row0 * n3, nr, n3, F3.tw, sm, ps);
+        rows2s_mid<RowTwo<N3>::A, RowTwo<N3>::B, false>(sm, nr, ps);
     } else if constexpr (N3 != 0) {  // compile-time schedule: the first stage in registers
         rowslead_load<CtRowSched<N3>::r[0]>(x + row0 * n3, nr, n3, N3, F3.tw, sm, ps, threadIdx.x, blockDim.x);
         __syncthreads();
@@ -891,130 +1098,6 @@ __device__ __forceinline__ void p1458_inverse(const PencilRows &rows, const floa
     }
 }
 
-// ---- n1 transforms of L = 2 A B in two register stages (the 270- and 362-voxel axes) ----
-// cos / sin of 2 pi m / R for the composite register DFTs (R = 15, 18, 25)
-__host__ __device__ constexpr float wr_c(int R, int m) {
-    if (R == 18) {
-        constexpr float t[18] = {
-        1.0f, 0.9396926207859084f, 0.766044443118978f, 0.5000000000000001f, 0.17364817766693041f,
-        -0.1736481776669303f, -0.4999999999999998f, -0.7660444431189779f, -0.9396926207859083f, -1.0f,
-        -0.9396926207859084f, -0.7660444431189783f, -0.5000000000000004f, -0.17364817766693033f,
-        0.17364817766692997f, 0.49999999999999933f, 0.7660444431189778f, 0.9396926207859084f};
-        return t[m];
-    }
-    if (R == 15) {
-        constexpr float t[15] = {
-        1.0f, 0.9135454576426009f, 0.6691306063588582f, 0.30901699437494745f, -0.10452846326765333f,
-        -0.4999999999999998f, -0.8090169943749473f, -0.9781476007338057f, -0.9781476007338057f,
-        -0.8090169943749476f, -0.5000000000000004f, -0.10452846326765423f, 0.30901699437494723f,
-        0.6691306063588585f, 0.913545457642601f};
-        return t[m];
-    }
-    if (R == 25) {
-        constexpr float t[25] = {
-        1.0f, 0.9685831611286311f, 0.8763066800438636f, 0.7289686274214116f, 0.5358267949789965f,
-        0.30901699437494745f, 0.06279051952931353f, -0.1873813145857246f, -0.4257792915650727f,
-        -0.6374239897486897f, -0.8090169943749473f, -0.9297764858882513f, -0.9921147013144778f,
-        -0.9921147013144779f, -0.9297764858882515f, -0.8090169943749478f, -0.6374239897486895f,
-        -0.42577929156507216f, -0.18738131458572463f, 0.06279051952931283f, 0.30901699437494723f,
-        0.5358267949789968f, 0.7289686274214112f, 0.8763066800438631f, 0.968583161128631f};
-        return t[m];
-    }
-    return 1.f;
-}
-__host__ __device__ constexpr float wr_s(int R, int m) {
-    if (R == 18) {
-        constexpr float t[18] = {
-        0.0f, 0.3420201433256687f, 0.6427876096865393f, 0.8660254037844386f, 0.984807753012208f,
-        0.984807753012208f, 0.8660254037844387f, 0.6427876096865395f, 0.3420201433256689f, 0.0f,
-        -0.34202014332566866f, -0.6427876096865389f, -0.8660254037844384f, -0.984807753012208f,
-        -0.9848077530122081f, -0.866025403784439f, -0.6427876096865396f, -0.3420201433256686f};
-        return t[m];
-    }
-    if (R == 15) {
-        constexpr float t[15] = {
-        0.0f, 0.40673664307580015f, 0.7431448254773941f, 0.9510565162951535f, 0.9945218953682734f,
-        0.8660254037844387f, 0.5877852522924732f, 0.20791169081775931f, -0.20791169081775907f, -0.587785252292473f,
-        -0.8660254037844384f, -0.9945218953682733f, -0.9510565162951536f, -0.743144825477394f, -0.40673664307580015f};
-        return t[m];
-    }
-    if (R == 25) {
-        constexpr float t[25] = {
-        0.0f, 0.2486898871648548f, 0.4817536741017153f, 0.6845471059286886f, 0.8443279255020151f,
-        0.9510565162951535f, 0.9980267284282716f, 0.9822872507286887f, 0.9048270524660195f, 0.7705132427757893f,
-        0.5877852522924732f, 0.36812455268467814f, 0.12533323356430454f, -0.12533323356430429f,
-        -0.3681245526846779f, -0.5877852522924727f, -0.7705132427757894f, -0.9048270524660198f,
-        -0.9822872507286887f, -0.9980267284282716f, -0.9510565162951536f, -0.844327925502015f, -0.684547105928689f,
-        -0.4817536741017161f, -0.24868988716485535f};
-        return t[m];
-    }
-    return 0.f;
-}
-
-// Composite register DFT of R1 R2 points (Cooley-Tukey, input i = R2 i1 + i2,
-// output k = k1 + R1 k2, twiddles W_R^(i2 k1) as constants).
-template <int R1, int R2, bool INV>
-__device__ __forceinline__ void dft_cs(float2 (&v)[R1 * R2]) {
-    constexpr int R = R1 * R2;
-    float2 a[R];
-#pragma unroll
-    for (int i2 = 0; i2 < R2; ++i2) {
-        float2 x[R1];
-#pragma unroll
-        for (int i1 = 0; i1 < R1; ++i1) x[i1] = v[R2 * i1 + i2];
-        dft_small<R1, INV>(x);
-#pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) {
-            const int m = (i2 * k1) % R;
-            a[i2 * R1 + k1] = m == 0 ? x[k1] : c_mul_k(x[k1], wr_c(R, m), INV ? wr_s(R, m) : -wr_s(R, m));
-        }
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-        float2 y[R2];
-#pragma unroll
-        for (int i2 = 0; i2 < R2; ++i2) y[i2] = a[i2 * R1 + k1];
-        dft_small<R2, INV>(y);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = y[k2];
-    }
-}
-
-// register DFT of R points
-template <int R, bool INV>
-__device__ __forceinline__ void dft_reg(float2 (&v)[R]) {
-    if constexpr (R == 27) dft27<INV>(v);
-    else if constexpr (R == 25) dft_cs<5, 5, INV>(v);
-    else if constexpr (R == 15) dft_cs<3, 5, INV>(v);
-    else if constexpr (R == 18) dft_cs<2, 9, INV>(v);
-    else dft_small<R, INV>(v);
-}
-
-// v[k] *= (b w^(e k)) (INV: its conjugate), k < A, w = tw[1]: two table loads
-// (w^e, w^5e) and at most four products per value.
-template <int A, bool INV>
-__device__ __forceinline__ void twiddle_lin(const float2 *__restrict__ tw, int e, int L, float2 b, float2 (&v)[A]) {
-    constexpr int R0 = 5, R1 = (A + R0 - 1) / R0;
-    const float2 z = __ldg(tw + e % L), z5 = __ldg(tw + (5 * e) % L);
-    float2 p0[R0];
-    p0[0] = b;
-#pragma unroll
-    for (int k0 = 1; k0 < R0; ++k0) p0[k0] = c_mul(p0[k0 - 1], z);
-    float2 q = z5;
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-#pragma unroll
-        for (int k0 = 0; k0 < R0; ++k0) {
-            const int k = k0 + R0 * k1;
-            if (k < A) {
-                const float2 t = k1 == 0 ? p0[k0] : c_mul(p0[k0], q);
-                v[k] = INV ? c_mulc(v[k], t) : c_mul(v[k], t);
-            }
-        }
-        if (k1 > 0) q = c_mul(q, z5);
-    }
-}
-
 // Forward n1 transform of L = 2 A B (the 1458 scheme of p1458_forward with A-
 // and B-point stages): six warps per pencil, warp (c, h); lane n < B takes
 // y_h[n + B j] = w^{h n} x_{n+B j} W_{2A}^{h j} (W_{2A} = w^B, from the table),
@@ -1442,6 +1525,10 @@ __global__ void __launch_bounds__(256) k_c2r_rows(const float2 *__restrict__ z1,
         rows27_mid<true>(sm, nr, ps);
         rows27_store(sm, nr, ps, n3, F3.tw, y + row0 * n3);
         return;
+    } else if constexpr (RowTwo<N3>::on) {
+        rows2s_mid<RowTwo<N3>::A, RowTwo<N3>::B, true>(sm, nr, ps);
+        rows2s_store<RowTwo<N3>::A, RowTwo<N3>::B>(sm, nr, ps, n3, F3.tw, y + row0 * n3);
+        return;
     } else if constexpr (N3 != 0) {
         ct_inverse<N3, CtRowSched<N3>::ns - 1, 1, CtRowSched<N3>>(sm, nr, ps, F3.tw, threadIdx.x, blockDim.x);
         rowslead_store<CtRowSched<N3>::r[0]>(sm, nr, ps, n3, N3, F3.tw, y + row0 * n3, threadIdx.x, blockDim.x);
@@ -1614,6 +1701,8 @@ void Toeplitz::init_tables(Dims3 d, int prec) {
     f2 = make_len((int)L2, true, tw2, &r2);
     f3 = make_len((int)M3, false, tw3, &r3);
     if (M3 == 729) r3 = {27, 27};  // the compile-time rows (rows27_load / rows27_mid)
+    if (M3 == 375) r3 = {RowTwo<375>::A, RowTwo<375>::B};  // two register stages (rows2s_*)
+    if (M3 == 270) r3 = {RowTwo<270>::A, RowTwo<270>::B};
     {
         std::vector<float2> h(M3 + 1);
         for (int64_t k = 0; k <= M3; ++k) {
@@ -1998,7 +2087,7 @@ void Toeplitz::quadforms(const float *x3, const std::vector<const Toeplitz *> &p
 
 void Toeplitz::set_shape(int rows, int kb) {
     if (rows < 1 || kb < 1) throw Error(ERR_ARG, "launch shape values must be positive");
-    if (ct3 == 729 && rows > 8) throw Error(ERR_ARG, "rows of 729 run one warp per row, at most 8 per CTA");
+    if (warp_rows(ct3) && rows > 8) throw Error(ERR_ARG, "rows of this length run one warp per row, at most 8 per CTA");
     const int64_t smem_rows = (int64_t)rows * L3h * (int64_t)sizeof(float2);
     const int64_t smem_d2 = (int64_t)d2_smem_values((int)L2, kb) * (int64_t)sizeof(float2);
     if (smem_rows > 200 * 1024 || smem_d2 > 200 * 1024) throw Error(ERR_ARG, "launch shape exceeds shared memory");
