@@ -810,6 +810,133 @@ __device__ __forceinline__ void dim2_144_tail_load(const float2 *__restrict__ xa
     }
 }
 
+// n2 passes of the other compile-time lengths L2 = 2 R1 R2 (schedule 2, R1, R2:
+// 20, 48, 64, 90) with the last stage fused into the transposes, as for 144:
+// item (ii, n, kk), kk fastest, holds the values i2 = n + R2 j (j < R1) of tile
+// pencil ii KB + kk (rows ps apart); the zero-padded radix-2 and the radix-R1
+// stage run in registers on the way in (d2f_load), the radix-R2 stage of each
+// block of R2 positions on the way out to xa (d2f_tail_store: item (ii, kk, b),
+// ii fastest, so 8 lanes write one 64-byte i1 run), and their inverses mirror
+// them (d2f_tail_load, d2f_store).
+template <int R1, int R2>
+__device__ __forceinline__ void d2f_load(const float2 *__restrict__ z1, int n1, int n2, int L3h, int c, int i1b,
+                                         int k3b, int nk, int KB, int ps, const float2 *__restrict__ tw2,
+                                         float2 *__restrict__ sm, int tid, int nth) {
+    constexpr int M = R1 * R2;
+    const int total = D2_IB * R2 * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int n = r % R2, ii = r / R2;
+        const int i1 = i1b + ii;
+        const bool live = kk < nk && i1 < n1;
+        float2 x[R1], u[R1];
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int i2 = n + R2 * j;
+            x[j] = (live && i2 < n2) ? z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < R1; ++j) u[j] = c_mul(x[j], __ldg(tw2 + n + R2 * j));
+        dft_small<R1, false>(x);
+        dft_small<R1, false>(u);
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                x[k] = c_mul(x[k], w[k]);
+                u[k] = c_mul(u[k], w[k]);
+            }
+        }
+        float2 *sp = sm + (ii * KB + kk) * ps + n;
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            sp[R2 * k] = x[k];
+            sp[M + R2 * k] = u[k];
+        }
+    }
+}
+
+template <int R1, int R2>
+__device__ __forceinline__ void d2f_tail_store(const float2 *__restrict__ sm, int L3h, int n1p, int c, int i1b,
+                                               int k3b, int nk, int KB, int ps, float2 *__restrict__ xa, int tid,
+                                               int nth) {
+    constexpr int L = 2 * R1 * R2;
+    const int64_t pstride = (int64_t)L3h * n1p;
+    for (int t = tid; t < D2_IB * KB * 2 * R1; t += nth) {
+        const int ii = t % D2_IB, r = t / D2_IB;
+        const int kk = r % KB, b = r / KB;
+        if (kk >= nk) continue;
+        const float2 *sp = sm + (ii * KB + kk) * ps + R2 * b;
+        float2 v[R2];
+#pragma unroll
+        for (int j = 0; j < R2; ++j) v[j] = sp[j];
+        dft_small<R2, false>(v);
+        float2 *dst = xa + (((int64_t)c * L + R2 * b) * L3h + k3b + kk) * n1p + i1b + ii;
+#pragma unroll
+        for (int k = 0; k < R2; ++k) dst[k * pstride] = v[k];
+    }
+}
+
+template <int R1, int R2>
+__device__ __forceinline__ void d2f_tail_load(const float2 *__restrict__ xa, int L3h, int n1p, int c, int i1b,
+                                              int k3b, int nk, int KB, int ps, float2 *__restrict__ sm, int tid,
+                                              int nth) {
+    constexpr int L = 2 * R1 * R2;
+    const int64_t pstride = (int64_t)L3h * n1p;
+    for (int t = tid; t < D2_IB * KB * 2 * R1; t += nth) {
+        const int ii = t % D2_IB, r = t / D2_IB;
+        const int kk = r % KB, b = r / KB;
+        if (kk >= nk) continue;
+        const float2 *src = xa + (((int64_t)c * L + R2 * b) * L3h + k3b + kk) * n1p + i1b + ii;
+        float2 v[R2];
+#pragma unroll
+        for (int k = 0; k < R2; ++k) v[k] = src[k * pstride];
+        dft_small<R2, true>(v);
+        float2 *sp = sm + (ii * KB + kk) * ps + R2 * b;
+#pragma unroll
+        for (int j = 0; j < R2; ++j) sp[j] = v[j];
+    }
+}
+
+template <int R1, int R2>
+__device__ __forceinline__ void d2f_store(const float2 *__restrict__ sm, int n1, int n2, int L3h, int c, int i1b,
+                                          int k3b, int nk, int KB, int ps, const float2 *__restrict__ tw2,
+                                          float2 *__restrict__ z1, int tid, int nth) {
+    constexpr int M = R1 * R2;
+    const int total = D2_IB * R2 * KB;
+    for (int t = tid; t < total; t += nth) {
+        const int kk = t % KB, r = t / KB;
+        const int n = r % R2, ii = r / R2;
+        const int i1 = i1b + ii;
+        if (kk >= nk || i1 >= n1) continue;
+        const float2 *sp = sm + (ii * KB + kk) * ps + n;
+        float2 a[R1], b[R1];
+#pragma unroll
+        for (int k = 0; k < R1; ++k) {
+            a[k] = sp[R2 * k];
+            b[k] = sp[M + R2 * k];
+        }
+        if (n != 0) {
+            float2 w[R1];
+            twiddle_powers<R1>(tw2, 2 * n, w);
+#pragma unroll
+            for (int k = 1; k < R1; ++k) {
+                a[k] = c_mulc(a[k], w[k]);
+                b[k] = c_mulc(b[k], w[k]);
+            }
+        }
+        dft_small<R1, true>(a);
+        dft_small<R1, true>(b);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) {
+            const int i2 = n + R2 * j;
+            if (i2 < n2)
+                z1[(((int64_t)c * n1 + i1) * n2 + i2) * L3h + k3b + kk] = c_add(a[j], c_mulc(b[j], __ldg(tw2 + i2)));
+        }
+    }
+}
+
 // The same register stages for a runtime L2 (schedule 2, R1, ...): item (ii, n, kk),
 // kk fastest, holds the values i2 = n + m1 j of tile pencil ii * KB + kk,
 // m1 = L2 / (2 R1); the stages from 2 on run in shared memory.
@@ -916,11 +1043,13 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         dim2_144_load(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm, threadIdx.x, blockDim.x);
         __syncthreads();
         dim2_144_tail_store(sm, L3h, n1p, c, i1b, k3b, nk, KB, xa, threadIdx.x, blockDim.x);
-    } else if constexpr (N2 != 0) {  // compile-time schedule: the lead stages in registers, the rest fixed
-        dim2lead_load<CtSched<N2>::r[1]>(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, N2, tw2, sm, (int)threadIdx.x,
-                                         (int)blockDim.x);
+    } else if constexpr (N2 != 0) {  // compile-time 2, R1, R2: lead stages in registers, the last fused with the store
+        static_assert(CtSched<N2>::ns == 3, "fused n2 passes take three-stage schedules");
+        d2f_load<CtSched<N2>::r[1], CtSched<N2>::r[2]>(z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, sm,
+                                                        threadIdx.x, blockDim.x);
         __syncthreads();
-        ct_forward<N2, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
+        d2f_tail_store<CtSched<N2>::r[1], CtSched<N2>::r[2]>(sm, L3h, n1p, c, i1b, k3b, nk, KB, ps, xa, threadIdx.x,
+                                                              blockDim.x);
     } else if (F2.ns >= 2) {  // runtime length: the outer stages in registers as well
         LAMINO_DIM2_LEAD(dim2lead_load, F2.radix[1], z1, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, sm,
                          (int)threadIdx.x, (int)blockDim.x)
@@ -960,7 +1089,7 @@ __global__ void __launch_bounds__(288, 4) k_dim2_fwd(const float2 *__restrict__ 
         __syncthreads();
         fft_fwd_any<N2, 1>(sm, D2_IB * KB, ps, F2, threadIdx.x, blockDim.x);
     }
-    if constexpr (N2 != 144) {
+    if constexpr (N2 == 0) {
         // store: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each,
         // so a warp writes 8 runs rather than 32
         for (int t = threadIdx.x; t < L2 * nk * (D2_IB / 2); t += blockDim.x) {
@@ -1429,6 +1558,13 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
         __syncthreads();
         dim2_144_store(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1, threadIdx.x, blockDim.x);
         return;
+    } else if constexpr (N2 != 0) {
+        d2f_tail_load<CtSched<N2>::r[1], CtSched<N2>::r[2]>(xa, L3h, n1p, c, i1b, k3b, nk, KB, ps, sm, threadIdx.x,
+                                                             blockDim.x);
+        __syncthreads();
+        d2f_store<CtSched<N2>::r[1], CtSched<N2>::r[2]>(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, tw2, z1,
+                                                         threadIdx.x, blockDim.x);
+        return;
     }
     // load: four lanes per (p2, kk) run of 8 i1 values (64 B), one float4 each, so a
     // warp reads 8 runs rather than 32; D2_LD runs in flight per thread
@@ -1457,12 +1593,6 @@ __global__ void __launch_bounds__(288, 4) k_dim2_inv(const float2 *__restrict__ 
         }
     }
     __syncthreads();
-    if constexpr (N2 != 0) {
-        ct_inverse<N2, CtSched<N2>::ns - 1, 2>(sm, D2_IB * KB, ps, tw2, threadIdx.x, blockDim.x);
-        dim2lead_store<CtSched<N2>::r[1]>(sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, N2, tw2, z1, (int)threadIdx.x,
-                                          (int)blockDim.x);
-        return;
-    }
     if (F2.ns >= 2) {
         fft_inverse(sm, D2_IB * KB, ps, F2, 2, threadIdx.x, blockDim.x);
         LAMINO_DIM2_LEAD(dim2lead_store, F2.radix[1], sm, n1, n2, L3h, c, i1b, k3b, nk, KB, ps, L2, tw2, z1,
