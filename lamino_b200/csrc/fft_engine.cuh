@@ -386,9 +386,10 @@ __device__ __forceinline__ void fft_inverse(float2 *data, int P, int ps, const F
 
 // ---- compile-time schedules for the lengths of the common problem sizes ----
 // (729 = packed n3 transform and 1458 = n1 transform of a 721-voxel axis; 144 =
-// n2 transform of a 71-voxel axis; 180, 360, 540, 750 = n1 transforms of the
-// 90-, 180-, 270- and 362-voxel lateral axes of 64- to 256-wide reconstructions;
-// 20, 48, 64, 90 = n2 transforms of their 10- to 44-voxel thickness axes).
+// n2 transform of a 71-voxel axis; 180, 360 = n1 transforms of the 90- and
+// 180-voxel lateral axes of 64- and 128-wide reconstructions; 20, 48, 64, 90 =
+// n2 transforms of their 10- to 44-voxel thickness axes; 540 and 750 run in two
+// register stages instead).
 // Each equals the runtime schedule fft_schedule(N, true), so the DIF output
 // positions are the same either way.  Other lengths use the runtime path above.
 constexpr int CT_MAX_STAGES = 6;
@@ -422,16 +423,6 @@ struct CtSched<360> {
     static constexpr int ns = 4;
     static constexpr int r[CT_MAX_STAGES] = {2, 4, 9, 5, 0, 0};
 };
-template <>
-struct CtSched<540> {
-    static constexpr int ns = 5;
-    static constexpr int r[CT_MAX_STAGES] = {2, 2, 9, 5, 3, 0};
-};
-template <>
-struct CtSched<750> {
-    static constexpr int ns = 5;
-    static constexpr int r[CT_MAX_STAGES] = {2, 5, 5, 5, 3, 0};
-};
 // n2 transforms of the 10-, 22-, 32- and 44-voxel thickness axes
 template <>
 struct CtSched<20> {
@@ -455,8 +446,8 @@ struct CtSched<90> {
 };
 
 // Schedules of the packed row transforms (no zero-padded lead stage): the
-// packed half lengths 90, 180, 270, 375 of the 180- to 750-long n3 embeddings.
-// Each equals fft_schedule(N, false).
+// packed half lengths 90 and 180 of the 180- and 360-long n3 embeddings (270
+// and 375 run in two register stages).  Each equals fft_schedule(N, false).
 template <int N>
 struct CtRowSched {
     static constexpr int ns = 0;
@@ -471,16 +462,6 @@ template <>
 struct CtRowSched<180> {
     static constexpr int ns = 3;
     static constexpr int r[CT_MAX_STAGES] = {4, 9, 5, 0, 0, 0};
-};
-template <>
-struct CtRowSched<270> {
-    static constexpr int ns = 4;
-    static constexpr int r[CT_MAX_STAGES] = {2, 9, 5, 3, 0, 0};
-};
-template <>
-struct CtRowSched<375> {
-    static constexpr int ns = 4;
-    static constexpr int r[CT_MAX_STAGES] = {5, 5, 5, 3, 0, 0};
 };
 
 // block size before stage s of schedule SC (length N)

@@ -198,41 +198,17 @@ __device__ __forceinline__ float d_potential(float delta, const QgConst &k) {
     return a * (2.0f - k.qmp * t1 * r);
 }
 
-__global__ void __launch_bounds__(kVoxX) k_qggmrf(float *__restrict__ g, const float *__restrict__ x, int n1, int n2,
-                                                  int n3, QgConst kq) {
-    const int k = blockIdx.x * kVoxX + threadIdx.x, j = blockIdx.y;
-    if (k < 1 || k > n3 - 2 || j < 1 || j > n2 - 2) return;  // interior voxels only
-    const PlaneRun pr(n1);
-    for (int i = pr.z0; i < pr.z1; ++i) {
-        if (i < 1 || i > n1 - 2) continue;
-        const int64_t c = ((int64_t)i * n2 + j) * n3 + k;
-        const float u = x[c];
-        float sum = 0.f;
-#pragma unroll
-        for (int dx = -1; dx < 2; ++dx)
-#pragma unroll
-            for (int dy = -1; dy < 2; ++dy)
-#pragma unroll
-                for (int dz = -1; dz < 2; ++dz) {
-                    if (dx == 0 && dy == 0 && dz == 0) continue;
-                    const float v = x[c + ((int64_t)dx * n2 + dy) * n3 + dz];
-                    const float w = c_qggmrf_w[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
-                    sum += w * d_potential(v - u, kq);
-                }
-        g[c] += sum;
-    }
-}
-
-// The same sums with each neighbour pair's derivative evaluated once.
-// rho'(-delta) = -rho'(delta) exactly in float for delta != 0 (the sign only
+// qGGMRF gradient: g[interior] += sum over the 26 neighbours of w_d rho'(x[c+d] -
+// x[c]) (src/qggmrf.cpp:60-95), with each neighbour pair's derivative evaluated
+// once.  rho'(-delta) = -rho'(delta) exactly in float for delta != 0 (the sign only
 // flips a product), and both sides take rho'(0) = q / (sigma^q C) at delta = 0,
 // so the 13 "forward" directions (dx = +1, and dx = 0 with (dy, dz) after
 // (0, 0)) give every pair: the owner c keeps rho'(x[c+d] - x[c]) for its own
 // sum and leaves the other side's term in shared memory.  A CTA owns a tile of
 // QG_TJ x QG_TK columns (j, k) and marches through a run of planes i; its
 // threads cover the tile plus a one-column halo, whose pairs reach into the
-// tile.  The 26 terms of every voxel are added in the direct kernel's order
-// (dx, dy, dz from -1 to 1), so the sums are the same.
+// tile.  The 26 terms of every voxel are added in the reference's order (dx,
+// dy, dz from -1 to 1), as a direct 26-neighbour loop would add them.
 constexpr int QG_TJ = 12, QG_TK = 32;  // 476 threads, 42 KB of shared memory
 constexpr int QG_HJ = QG_TJ + 2, QG_HK = QG_TK + 2, QG_THREADS = QG_HJ * QG_HK;
 

@@ -1787,8 +1787,6 @@ static bool ct_row_equal(const std::vector<int> &r) {
 }
 static bool ct_row_matches(int M, const std::vector<int> &r) {
     switch (M) {
-        case 375: return ct_row_equal<375>(r);
-        case 270: return ct_row_equal<270>(r);
         case 180: return ct_row_equal<180>(r);
         case 90: return ct_row_equal<90>(r);
         default: return false;
@@ -1796,8 +1794,6 @@ static bool ct_row_matches(int M, const std::vector<int> &r) {
 }
 static bool ct_schedule_matches(int L, const std::vector<int> &r) {  // n1 (pencil) lengths
     switch (L) {
-        case 750: return ct_equal<750>(r);
-        case 540: return ct_equal<540>(r);
         case 360: return ct_equal<360>(r);
         case 180: return ct_equal<180>(r);
         default: return false;
@@ -1969,7 +1965,7 @@ void Toeplitz::finish(cudaStream_t s) {
         throw Error(ERR_ARG, "n2 too large for the n2-pass kernels");
     ct1 = (L1 == 1458 || !two_stage_schedule((int)L1).empty() || ct_schedule_matches((int)L1, r1_)) ? (int)L1 : 0;
     ct2 = (L2 == 144 || ct_dim2_matches((int)L2, r2_)) ? (int)L2 : 0;
-    ct3 = M3 == 729 ? 729 : (ct_row_matches((int)M3, fft_schedule((int)M3, false)) ? (int)M3 : 0);
+    ct3 = (warp_rows((int)M3) || ct_row_matches((int)M3, fft_schedule((int)M3, false))) ? (int)M3 : 0;
     const int smem_rows = rows1 * (int)L3h * (int)sizeof(float2);
     const int smem_d2 = d2_smem_values((int)L2, kb2) * (int)sizeof(float2);
     const int smem_pen = 3 * (int)L1 * (int)sizeof(float2);
