@@ -253,8 +253,9 @@ int lamino_mbir_footprint(int method, int ndatasets, const int64_t *proj_dims, i
  * all requests follow one another in projs / proj_dims (3 per dataset) / angles /
  * gammas, request by request.  recon_dims: 3 per request; params: nreq entries;
  * out3[r]: [3][recon_dims[3r]][recon_dims[3r+1]][recon_dims[3r+2]] (host).
- * Preparer threads (`threads`) set requests up in order while the sum of their
- * estimated footprints (lamino_mbir_footprint) fits in `budget` bytes; the
+ * Preparer threads (`threads`) set requests up, largest estimated footprint
+ * first, while the sum of their estimated footprints (lamino_mbir_footprint)
+ * fits in `budget` bytes; the
  * calling thread drives all prepared NAG solves, each with one line-search step
  * in flight on its own stream, deciding a step as soon as its reductions have
  * landed.  Optional outputs: times[2r], times[2r+1] = seconds

@@ -93,7 +93,13 @@ void mbir3_batch(std::vector<BatchRequest> &reqs, int64_t budget, int threads, B
 
     std::mutex mu;
     std::condition_variable cv;
-    size_t next = 0;       // next request to prepare
+    // largest first (estimated footprint, which grows with the volume and the
+    // projections): the big requests start early instead of running alone at
+    // the end of the batch
+    std::vector<size_t> order(N);
+    for (size_t i = 0; i < N; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return fp[a] > fp[b]; });
+    size_t next = 0;       // position in `order` of the next request to prepare
     int64_t in_use = 0;    // footprints of prepared and running requests
     bool abort = false;
     std::exception_ptr err;
@@ -112,11 +118,11 @@ void mbir3_batch(std::vector<BatchRequest> &reqs, int64_t budget, int threads, B
             std::unique_ptr<Slot> sl(new Slot);
             {
                 std::unique_lock<std::mutex> lk(mu);
-                // in order; a request waits until it fits beside the others
+                // in that order; a request waits until it fits beside the others
                 // (always admitted when nothing is held)
-                cv.wait(lk, [&] { return abort || next == N || in_use == 0 || in_use + fp[next] <= budget; });
+                cv.wait(lk, [&] { return abort || next == N || in_use == 0 || in_use + fp[order[next]] <= budget; });
                 if (abort || next == N) return;
-                sl->idx = next++;
+                sl->idx = order[next++];
                 sl->footprint = fp[sl->idx];
                 in_use += sl->footprint;
                 st.peak_in_use = std::max(st.peak_in_use, in_use);

@@ -1,9 +1,9 @@
 // The batched form of MBIR3 (src/mbir3.cpp:47-135 per request): many
 // reconstructions of uneven size run through one pipeline on one GPU.
 //
-// Preparer threads take the requests in order, each while the sum of the
-// estimated footprints of the prepared and running requests fits in the HBM
-// budget, and run their setup (normalisation, padding, setup adjoints,
+// Preparer threads take the requests largest first (by estimated footprint),
+// each while the sum of the estimated footprints of the prepared and running
+// requests fits in the HBM budget, and run their setup (normalisation, padding, setup adjoints,
 // Toeplitz operators, Lipschitz constant) on low-priority streams.  One solver
 // thread drives every prepared request's NAG solve: each request keeps one
 // line-search step in flight on its own high-priority stream (graph replays
