@@ -113,16 +113,31 @@ struct Fine {
 };
 
 // first tap of a coordinate on the fine grid (wrapped) and its offset d0 in
-// [-W/2, -W/2 + 1) from the coordinate, in grid units
+// [-W/2, -W/2 + 1) from the coordinate, in grid units; lu: the first tap unwrapped
 template <int W>
-__device__ __forceinline__ int es_start(float xc, int nf, double s, float &d0) {
+__device__ __forceinline__ int es_start(float xc, int nf, double s, float &d0, double &lu) {
     double u = (double)xc * s;
     double l0 = ceil(u - 0.5 * W);
     d0 = (float)(l0 - u);
+    lu = l0;
     int64_t l = (int64_t)l0;
     l %= nf;
     if (l < 0) l += nf;
     return (int)l;
+}
+template <int W>
+__device__ __forceinline__ int es_start(float xc, int nf, double s, float &d0) {
+    double lu;
+    return es_start<W>(xc, nf, s, d0, lu);
+}
+// offset d0 of a coordinate from another point's first tap lu (unwrapped);
+// true if the coordinate's own first tap is within one cell of lu, so that its
+// w taps on lu's footprint miss at most one edge tap (kernel value ~exp(-beta))
+template <int W>
+__device__ __forceinline__ bool es_offset_from(float xc, double s, double lu, float &d0) {
+    double u = (double)xc * s;
+    d0 = (float)(lu - u);
+    return fabs(ceil(u - 0.5 * W) - lu) <= 1.0;
 }
 
 template <int W>
@@ -303,8 +318,34 @@ __device__ __forceinline__ void decode_pid(uint32_t pid, const GeomView &g, int 
     k = (int)(r - (uint32_t)j * (uint32_t)g.ncols);
 }
 
+// Antipodal pairs (the adjoint).  The detector frequencies are symmetric about
+// zero (qX[k] = -qX[nc-1-k] and qY[j] = -qY[nr-1-j] up to float rounding), so
+// the points at in-plane flat index i and N-1-i of a projection (N = nrows
+// ncols) are antipodal: x_{N-1-i} = -x_i + d, |d| at the rounding level.  The
+// adjoint keeps only the real part of the type-1 sum, and on the periodic fine
+// grid (m -> -m, phi even) the term of a point i' with strength f equals, in
+// real part, the term of strength conj(f) at -x_{i'}.  That position lies next
+// to x_i, so one staged record carries both points and spreads them through
+// x_i's footprint: half the tile read-modify-writes per point.  Pair q of a
+// projection is (q, N-1-q), q in [0, (N+1)/2); for odd N the middle point is
+// its own partner and the pair's second strength is zero.
+__device__ __forceinline__ uint32_t pairs_per_proj(const GeomView &g) {
+    return ((uint32_t)g.nrows * (uint32_t)g.ncols + 1u) / 2u;
+}
+__device__ __forceinline__ void decode_pair(uint32_t pid, const GeomView &g, int &p, int &j, int &k, int &j2,
+                                            int &k2) {
+    const uint32_t H = pairs_per_proj(g);
+    p = (int)(pid / H);
+    const uint32_t q = pid - (uint32_t)p * H;
+    j = (int)(q / (uint32_t)g.ncols);
+    k = (int)(q - (uint32_t)j * (uint32_t)g.ncols);
+    j2 = g.nrows - 1 - j;
+    k2 = g.ncols - 1 - k;
+}
+
 // ---------------------------------------------------------------------------
-// bin sort: point ids grouped by the fine-grid bin of their footprint's first cell
+// bin sort: point (or pair) ids grouped by the fine-grid bin of their
+// footprint's first cell (a pair's: its first point's)
 
 // first cell of the kernel footprint along one dimension, in [0, nf) (as es_taps)
 template <int W>
@@ -316,10 +357,15 @@ __device__ __forceinline__ int es_start(float xc, int nf, double s) {
     return (int)l;
 }
 
-template <int W>
+template <int W, bool PAIRED>
 __device__ __forceinline__ uint32_t point_bin(const GeomView &g, const Fine &F, const BinLayout &B, uint32_t pid) {
     int p, j, k;
-    decode_pid(pid, g, p, j, k);
+    if (PAIRED) {
+        int j2, k2;
+        decode_pair(pid, g, p, j, k, j2, k2);
+    } else {
+        decode_pid(pid, g, p, j, k);
+    }
     float x, y, z;
     point_xyz(g, p, j, k, x, y, z);
     const int l1 = es_start<W>(z, F.nf1, F.s1), l2 = es_start<W>(y, F.nf2, F.s2), l3 = es_start<W>(x, F.nf3, F.s3);
@@ -329,24 +375,29 @@ __device__ __forceinline__ uint32_t point_bin(const GeomView &g, const Fine &F, 
 
 // Consecutive point ids walk a projection row, so the lanes of a warp mostly
 // share a bin: one atomic per distinct bin in the warp.
-template <int W>
+template <bool PAIRED>
+__device__ __forceinline__ uint32_t sort_ids(const GeomView &g) {
+    return (uint32_t)g.nproj * (PAIRED ? pairs_per_proj(g) : (uint32_t)g.nrows * (uint32_t)g.ncols);
+}
+
+template <int W, bool PAIRED>
 __global__ void __launch_bounds__(256) k_bin_count(GeomView g, Fine F, BinLayout B, uint32_t *__restrict__ cnt) {
-    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    const uint32_t M = sort_ids<PAIRED>(g);
     const int lane = threadIdx.x & 31;
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
-        const uint32_t bin = point_bin<W>(g, F, B, pid);
+        const uint32_t bin = point_bin<W, PAIRED>(g, F, B, pid);
         const unsigned grp = __match_any_sync(__activemask(), bin);
         if (lane == __ffs(grp) - 1) atomicAdd(cnt + bin, (uint32_t)__popc(grp));
     }
 }
 
-template <int W>
+template <int W, bool PAIRED>
 __global__ void __launch_bounds__(256) k_bin_scatter(GeomView g, Fine F, BinLayout B, uint32_t *__restrict__ cursor,
                                                      uint32_t *__restrict__ perm) {
-    const uint32_t M = (uint32_t)g.nproj * g.nrows * g.ncols;
+    const uint32_t M = sort_ids<PAIRED>(g);
     const int lane = threadIdx.x & 31;
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < M; pid += gridDim.x * blockDim.x) {
-        const uint32_t bin = point_bin<W>(g, F, B, pid);
+        const uint32_t bin = point_bin<W, PAIRED>(g, F, B, pid);
         const unsigned grp = __match_any_sync(__activemask(), bin);
         const int leader = __ffs(grp) - 1;
         uint32_t base = 0;
@@ -482,20 +533,6 @@ __device__ __forceinline__ bool point_taps(const GeomView &g, const Fine &F, con
     return (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
 }
 
-// strength of a point for the adjoint: coeff_i(th) * P[ifftshift2 position]
-struct AdjointStrength {
-    const float2 *Pf;
-    __device__ __forceinline__ void operator()(const GeomView &g, int p, int j, int k, uint32_t, float2 *s) const {
-        int js = j + (g.nrows + 1) / 2; if (js >= g.nrows) js -= g.nrows;
-        int ks = k + (g.ncols + 1) / 2; if (ks >= g.ncols) ks -= g.ncols;
-        const float2 c = Pf[((int64_t)p * g.nrows + js) * g.ncols + ks];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const float cq = __ldg(g.coeff + q * g.nproj + p);
-            s[q] = make_float2(cq * c.x, cq * c.y);
-        }
-    }
-};
 struct RawStrength {
     const float2 *c;
     __device__ __forceinline__ void operator()(const GeomView &, int, int, int, uint32_t pid, float2 *s) const {
@@ -529,10 +566,27 @@ struct PointRec {
     float w1[W], w2[W], w3[W];
     float2 s[NC];
 };
-constexpr int kStageChunk = 256;  // points staged per pass
+// A staged antipodal pair, laid out so that a visit reads each quantity of
+// both points with one load: per component the two strengths (s.x, s.y, g.x,
+// g.y), per tap the two weights (first, second point), and the first point's
+// tile offset packed as a1 | a2 << 8 | a3 << 20.
+template <int W, int NC>
+struct __align__(16) PairRec {
+    float4 sg[NC];
+    float2 w1[W], w2[W], w3[W];
+    int a;
+};
+constexpr int kStageChunk = 256;  // points staged per pass (threads of the staging CTAs)
+constexpr int kStagePairs = kStageChunk / 2;  // pairs staged per pass, two threads each
 constexpr size_t point_rec_bytes(int w, int nc) { return (size_t)((12 + 12 * w + 7) / 8 * 8 + 8 * nc); }
+constexpr size_t pair_rec_bytes(int w, int nc) { return (size_t)((16 * nc + 24 * w + 4 + 15) / 16 * 16); }
+// byte offset of the pair records after NC tiles of tsz cells (16-byte aligned)
+__host__ __device__ constexpr size_t pair_rec_offset(int64_t tsz, int nc) { return (size_t)((nc * tsz * 8 + 15) / 16 * 16); }
 static_assert(sizeof(PointRec<7, 3>) == point_rec_bytes(7, 3), "record layout");
 static_assert(sizeof(PointRec<8, 1>) == point_rec_bytes(8, 1), "record layout");
+static_assert(sizeof(PairRec<7, 3>) == pair_rec_bytes(7, 3), "record layout");
+static_assert(sizeof(PairRec<8, 3>) == pair_rec_bytes(8, 3), "record layout");
+static_assert(sizeof(PairRec<4, 3>) == pair_rec_bytes(4, 3), "record layout");
 
 // Records of a staged chunk in slab order.  Every CTA of the binned kernels
 // runs kStageChunk threads, one point each.  A point whose taps fit in the
@@ -639,6 +693,67 @@ __device__ __forceinline__ void spread_sorted(float2 *tile, int tsz, const BinLa
     }
 }
 
+// spread_sorted for pair records: each tap adds the first point's term, then
+// the second's
+template <int W, int NC>
+__device__ __forceinline__ void spread_pairs_sorted(float2 *tile, int tsz, const BinLayout &B,
+                                                    const PairRec<W, NC> *recs, const int *bstart) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    constexpr int NT = W * W;
+    constexpr int NR = (NT + 31) / 32;
+    int t2s[NR], t3s[NR], loff[NR];
+    bool act[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int q = lane + 32 * r;
+        act[r] = q < NT;
+        t2s[r] = act[r] ? q / W : 0;
+        t3s[r] = act[r] ? q - (q / W) * W : 0;
+        loff[r] = t2s[r] * B.r3 + t3s[r];
+    }
+    const int slab_stride = B.t2 * B.r3;
+    for (int slab = warp; slab < B.t1; slab += nwarps) {
+        const int lo = max(0, slab - (W - 1)), hi = min(B.b1 - 1, slab);
+        if (lo > hi) continue;
+        const int q1 = bstart[hi + 1];
+        float2 *srow = tile + slab * slab_stride;
+        for (int q = bstart[lo]; q < q1; ++q) {
+            const PairRec<W, NC> &pr = recs[q];
+            const int a = pr.a;
+            const float2 w1v = pr.w1[slab - (a & 0xff)];
+            float2 *cell0 = srow + ((a >> 8) & 0xfff) * B.r3 + (a >> 20);
+            float wt[NR], ut[NR];
+            float2 v[NR][NC];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const float2 b2 = pr.w2[t2s[r]], b3 = pr.w3[t3s[r]];
+                wt[r] = w1v.x * (b2.x * b3.x);
+                ut[r] = w1v.y * (b2.y * b3.y);
+                if (act[r]) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) v[r][c] = cell0[loff[r] + c * tsz];
+                }
+            }
+            float4 sg[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sg[c] = pr.sg[c];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                if (act[r]) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        v[r][c].x = fmaf(wt[r], sg[c].x, v[r][c].x);
+                        v[r][c].y = fmaf(wt[r], sg[c].y, v[r][c].y);
+                        v[r][c].x = fmaf(ut[r], sg[c].z, v[r][c].x);
+                        v[r][c].y = fmaf(ut[r], sg[c].w, v[r][c].y);
+                        cell0[loff[r] + c * tsz] = v[r][c];
+                    }
+                }
+            }
+        }
+    }
+}
+
 template <int NC>
 __device__ __forceinline__ void flush_tile(const float2 *tile, int tsz, const BinLayout &B, const BinOrigin &o,
                                            const Fine &F, float2 *H, int64_t NF) {
@@ -705,6 +820,108 @@ __global__ void __launch_bounds__(kStageChunk, 2) k_spread_binned(GeomView g, co
         __syncthreads();
     }
     flush_tile<NC>(tile, tsz, B, o, F, H, NF);
+}
+
+// Adjoint spread over antipodal pairs (see decode_pair): two threads stage a
+// pair, the even one its first point (offsets, weights, strengths
+// coeff_i(th) P), the odd one its second point -x_{i'} (weights on the first
+// point's footprint, strengths coeff_i(th) conj(P_{i'})); records are ranked
+// by the first point's slab and spread as k_spread_binned does.  A second
+// point whose own footprint starts more than one cell away (not the case for
+// the reference's symmetric detector grids) is spread through global memory.
+template <int W>
+__global__ void __launch_bounds__(kStageChunk, 2) k_spread_pairs(GeomView g, const uint32_t *__restrict__ perm,
+                                                      const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                      float2 *__restrict__ H, int64_t NF,
+                                                      const float2 *__restrict__ Pf) {
+    extern __shared__ __align__(16) unsigned char psm[];
+    float2 *tile = reinterpret_cast<float2 *>(psm);
+    const int bin = blockIdx.x;
+    const uint32_t p0 = start[bin], p1 = start[bin + 1];
+    if (p0 == p1) return;
+    const BinOrigin o = bin_origin(B, bin);
+    const int tsz = (int)B.tile_cells();
+    PairRec<W, 3> *recs = reinterpret_cast<PairRec<W, 3> *>(psm + pair_rec_offset(tsz, 3));
+    for (int i = threadIdx.x; i < 3 * tsz; i += blockDim.x) tile[i] = make_float2(0.f, 0.f);
+    __shared__ int wcnt[kStageWarps * kMaxB1];
+    __shared__ int bstart[kMaxB1 + 1];
+    const bool second = (threadIdx.x & 1) != 0;
+    const int t = threadIdx.x >> 1;  // pair slot (blockDim.x == kStageChunk == 2 kStagePairs)
+    for (uint32_t base = p0; base < p1; base += kStagePairs) {
+        const int n = (int)min((uint32_t)kStagePairs, p1 - base);
+        int p = 0, j = 0, k = 0, j2 = 0, k2 = 0, a1 = -1, a2 = 0, a3 = 0;
+        float x = 0.f, y = 0.f, z = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+        bool in = false, near = true;
+        if (t < n) {
+            decode_pair(__ldg(perm + base + t), g, p, j, k, j2, k2);
+            point_xyz(g, p, j, k, x, y, z);
+            double l1, l2, l3;
+            a3 = es_start<W>(x, F.nf3, F.s3, d3, l3) - o.o3;
+            a2 = es_start<W>(y, F.nf2, F.s2, d2, l2) - o.o2;
+            a1 = es_start<W>(z, F.nf1, F.s1, d1, l1) - o.o1;
+            in = (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
+            if (second) {
+                float xa, ya, za;
+                point_xyz(g, p, j2, k2, xa, ya, za);
+                x = -xa;
+                y = -ya;
+                z = -za;
+                near = es_offset_from<W>(x, F.s3, l3, d3) && es_offset_from<W>(y, F.s2, l2, d2) &&
+                       es_offset_from<W>(z, F.s1, l1, d1);
+            }
+        }
+        int pos = place_slot(in && !second ? a1 : -1, wcnt, bstart, B);
+        pos = __shfl_sync(0xffffffffu, pos, (threadIdx.x & 31) & ~1);
+        if (t < n) {
+            const int jj = second ? j2 : j, kk = second ? k2 : k;
+            int js = jj + (g.nrows + 1) / 2; if (js >= g.nrows) js -= g.nrows;
+            int ks = kk + (g.ncols + 1) / 2; if (ks >= g.ncols) ks -= g.ncols;
+            float2 c = Pf[((int64_t)p * g.nrows + js) * g.ncols + ks];
+            if (second) c = (j2 == j && k2 == k) ? make_float2(0.f, 0.f) : make_float2(c.x, -c.y);
+            float2 sv[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const float cq = __ldg(g.coeff + q * g.nproj + p);
+                sv[q] = make_float2(cq * c.x, cq * c.y);
+            }
+            if (in) {
+                // the even thread fills the first point's halves of the record,
+                // the odd thread the second point's
+                PairRec<W, 3> &pr = recs[pos];
+                const int h = second ? 1 : 0;
+                float *wx[3] = {&pr.w1[0].x + h, &pr.w2[0].x + h, &pr.w3[0].x + h};
+                float wt[3][W];
+                if (near) {
+                    es_weights<W>(d1, F.beta, wt[0]);
+                    es_weights<W>(d2, F.beta, wt[1]);
+                    es_weights<W>(d3, F.beta, wt[2]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < W; ++q) wt[0][q] = wt[1][q] = wt[2][q] = 0.f;
+                    spread_point_global<W, 3>(H, NF, F, x, y, z, sv);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) sv[q] = make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int q = 0; q < W; ++q) wx[d][2 * q] = wt[d][q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    float *sq = &pr.sg[q].x + 2 * h;
+                    sq[0] = sv[q].x;
+                    sq[1] = sv[q].y;
+                }
+                if (!second) pr.a = a1 | (a2 << 8) | (a3 << 20);
+            } else {
+                spread_point_global<W, 3>(H, NF, F, x, y, z, sv);
+            }
+        }
+        __syncthreads();
+        spread_pairs_sorted<W, 3>(tile, tsz, B, recs, bstart);
+        __syncthreads();
+    }
+    flush_tile<3>(tile, tsz, B, o, F, H, NF);
 }
 
 // Interpolation: the CTA loads its bin's tile, each thread gathers one point's
@@ -942,6 +1159,7 @@ static void with_width(int w, Fn &&fn) {
 void NufftPlan::set_bins(int b1, int b2, int b3) {
     if (b1 <= 0 || b2 <= 0 || b3 <= 0) throw Error(ERR_ARG, "bin sizes must be positive");
     if (b1 > kMaxB1) throw Error(ERR_ARG, "bin extent along n1 must be at most 16");
+    if (b2 > 4095 || b3 > 4095) throw Error(ERR_ARG, "bin extents along n2 and n3 must be below 4096");
     BinLayout B;
     B.b1 = b1; B.b2 = b2; B.b3 = b3;
     B.nb1 = (int)((nf1 + b1 - 1) / b1);
@@ -961,15 +1179,15 @@ void NufftPlan::set_bins(int b1, int b2, int b3) {
     drop_sorted();
 }
 
-const SortedPoints *NufftPlan::find_sorted(const Geom &g) const {
+const SortedPoints *NufftPlan::find_sorted(const Geom &g, bool paired) const {
     for (const auto &sp : sorted)
-        if (sp->uid == g.uid) return sp.get();
+        if (sp->uid == g.uid && sp->paired == paired) return sp.get();
     return nullptr;
 }
 
-const SortedPoints &NufftPlan::sort_points(const Geom &g, cudaStream_t s) {
+const SortedPoints &NufftPlan::sort_points(const Geom &g, cudaStream_t s, bool paired) {
     for (auto &sp : sorted)
-        if (sp->uid == g.uid) {
+        if (sp->uid == g.uid && sp->paired == paired) {
             sp->last_use = ++use_clock;
             return *sp;
         }
@@ -982,21 +1200,25 @@ const SortedPoints &NufftPlan::sort_points(const Geom &g, cudaStream_t s) {
     if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
     auto sp = std::make_unique<SortedPoints>();
     sp->uid = g.uid;
+    sp->paired = paired;
     const int64_t nb = bins.nbins();
+    const int64_t ids = paired ? g.nproj * ((g.nrows * g.ncols + 1) / 2) : g.npts();
     DevBuf<uint32_t> cnt(nb), cursor(nb);
     sp->start.alloc(nb + 1);
-    sp->perm.alloc(g.npts());
+    sp->perm.alloc(ids);
     LAMINO_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), s));
     const Fine F = fine_of(*this);
     const GeomView gv = g.view();
-    const unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
+    const unsigned grid = grid_for(ids, 256, 148LL * 16 * 8);
     with_width(w, [&](auto WC) {
         constexpr int W = decltype(WC)::value;
-        k_bin_count<W><<<grid, 256, 0, s>>>(gv, F, bins, cnt.p);
+        auto count = paired ? k_bin_count<W, true> : k_bin_count<W, false>;
+        auto scatter = paired ? k_bin_scatter<W, true> : k_bin_scatter<W, false>;
+        count<<<grid, 256, 0, s>>>(gv, F, bins, cnt.p);
         LAMINO_LAUNCH("k_bin_count");
         k_scan_offsets<<<1, 1024, 0, s>>>(cnt.p, (int)nb, sp->start.p, cursor.p);
         LAMINO_LAUNCH("k_scan_offsets");
-        k_bin_scatter<W><<<grid, 256, 0, s>>>(gv, F, bins, cursor.p, sp->perm.p);
+        scatter<<<grid, 256, 0, s>>>(gv, F, bins, cursor.p, sp->perm.p);
         LAMINO_LAUNCH("k_bin_scatter");
     });
     sp->last_use = ++use_clock;
@@ -1101,7 +1323,7 @@ void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_
 
 void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumulate, cudaStream_t s) {
     ensure_proj(g, s);
-    const SortedPoints &sp = sort_points(g, s);
+    const SortedPoints &sp = sort_points(g, s, true);
     k_proj_pre<<<grid_for(g.npts(), 256), 256, 0, s>>>(proj, (int)g.nproj, (int)g.nrows, (int)g.ncols, pbuf.p);
     LAMINO_LAUNCH("k_proj_pre");
     LAMINO_CUFFT(cufftSetStream(fft2.h, s));
@@ -1109,14 +1331,14 @@ void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumu
     LAMINO_CUDA(cudaMemsetAsync(gwork.p, 0, gwork.bytes(), s));
     const Fine F = fine_of(*this);
     const GeomView gv = g.view();
-    const int smem = (int)(3 * bins.tile_cells() * sizeof(float2) + kStageChunk * point_rec_bytes(w, 3));
+    const int smem = (int)(pair_rec_offset(bins.tile_cells(), 3) + kStagePairs * pair_rec_bytes(w, 3));
     with_width(w, [&](auto WC) {
         constexpr int W = decltype(WC)::value;
-        auto kern = k_spread_binned<W, 3, AdjointStrength>;
+        auto kern = k_spread_pairs<W>;
         raise_smem_limit((const void *)kern, smem);
         kern<<<(unsigned)bins.nbins(), kStageChunk, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
-                                                                AdjointStrength{pbuf.p});
-        LAMINO_LAUNCH("k_spread_binned<adjoint>");
+                                                                pbuf.p);
+        LAMINO_LAUNCH("k_spread_pairs");
     });
     fft_fine(+1, 3, s);
     extract_real(m3, 3, 1.0f / (float)(g.nrows * g.ncols), accumulate, s);

@@ -35,6 +35,7 @@ struct BinLayout {
 // Point ids of one geometry grouped by bin (counting sort), with bin offsets.
 struct SortedPoints {
     uint64_t uid = 0;
+    bool paired = false;     // ids of antipodal pairs (the adjoint), else of points
     uint64_t last_use = 0;
     DevBuf<uint32_t> perm;   // npts
     DevBuf<uint32_t> start;  // nbins + 1
@@ -65,9 +66,10 @@ struct NufftPlan {
     void ensure_proj(const Geom &g, cudaStream_t s);
     // bin layout for b1 x b2 x b3 bins (drops cached point orders)
     void set_bins(int b1, int b2, int b3);
-    // the geometry's bin-sorted order (built on first use, then cached)
-    const SortedPoints &sort_points(const Geom &g, cudaStream_t s);
-    const SortedPoints *find_sorted(const Geom &g) const;
+    // the geometry's bin-sorted order of points, or of antipodal point pairs
+    // (built on first use, then cached)
+    const SortedPoints &sort_points(const Geom &g, cudaStream_t s, bool paired = false);
+    const SortedPoints *find_sorted(const Geom &g, bool paired = false) const;
     // time candidate bin layouts and keep the fastest for objective 0 (adjoint of
     // the first geometry, including its sort: a setup pass) or 1 (the sum over
     // the geometries of sysmat, sorted orders reused: a solver's operator);

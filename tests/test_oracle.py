@@ -100,6 +100,41 @@ def test_golden_operators(O, gold_orc):
     assert rel(O.sysmat(gold_orc["op_m"], pg, np.float32(g), pe), gold_orc["op_sysmat"]) < 1e-12
 
 
+@pytest.mark.parametrize("nr,nc", [(31, 29), (26, 34), (180, 180), (462, 462), (1233, 1233)])
+def test_detector_points_pair_up_antipodally(O, nr, nc):
+    """The adjoint spreads points i and N-1-i of a projection (N = nrows ncols)
+    through one footprint: on the reference's detector grids, odd and even,
+    x_{N-1-i} = -x_i to within float rounding (here 1e-6 of [-pi, pi))."""
+    th = np.linspace(0, 2 * np.pi, 5, endpoint=False).astype(np.float32)
+    pg = O.PolarGrid(th, nr, nc, np.float32(0.6))
+    for a in (pg.x, pg.y, pg.z):
+        f = a.reshape(len(th), -1).astype(np.float64)
+        assert np.abs(f + f[:, ::-1]).max() < 2e-6
+
+
+def test_adjoint_pair_rule(O):
+    """Re sum_i f_i e^{i k.x_i} over all points equals the sum over pairs
+    (q, N-1-q), q < (N+1)/2, of f_q at x_q plus conj(f_{N-1-q}) at -x_{N-1-q},
+    the middle point of an odd N taken once: the rule the GPU adjoint spreads by."""
+    rng = np.random.default_rng(3)
+    th = rng.uniform(0, 2 * np.pi, 3).astype(np.float32)
+    for nr, nc in ((7, 5), (6, 4), (5, 6)):
+        pg = O.PolarGrid(th, nr, nc, np.float32(0.4))
+        N = nr * nc
+        pts = np.stack([a.reshape(len(th), N).astype(np.float64) for a in (pg.z, pg.y, pg.x)], -1)
+        f = rng.standard_normal((len(th), N)) + 1j * rng.standard_normal((len(th), N))
+        k = np.stack(np.meshgrid(*(np.arange(-3, 3),) * 3, indexing="ij"), -1).reshape(-1, 3)
+        full = np.einsum("pn,kpn->k", f, np.exp(1j * np.einsum("kd,pnd->kpn", k, pts))).real
+        H = (N + 1) // 2
+        q = np.arange(H)
+        g = np.conj(f[:, N - 1 - q])
+        g[:, q == N - 1 - q] = 0
+        second = -pts[:, N - 1 - q]
+        paired = (np.einsum("pn,kpn->k", f[:, :H], np.exp(1j * np.einsum("kd,pnd->kpn", k, pts[:, :H])))
+                  + np.einsum("pn,kpn->k", g, np.exp(1j * np.einsum("kd,pnd->kpn", k, second)))).real
+        assert np.allclose(paired, full, rtol=1e-12, atol=1e-10)
+
+
 def test_sysmat_equals_adjoint_forward_odd_grid(O):
     """tests/test_grad.cpp:15-55 of the reference: adjoint(forward(f)) vs gradient(f, 0)."""
     rng = np.random.default_rng(5)
