@@ -504,6 +504,40 @@ __device__ __forceinline__ void gather_tile(const float2 *tile, int tsz, const B
     }
 }
 
+// gather_tile for a pair: each tile value is read once and weighted for both
+// points (out: first point, same sums as gather_tile; outu: second point)
+template <int W, int NC>
+__device__ __forceinline__ void gather_tile_pair(const float2 *tile, int tsz, const BinLayout &B, int a1, int a2,
+                                                 int a3, const float (&w)[3][W], const float (&u)[3][W], float2 *out,
+                                                 float2 *outu) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = outu[c] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int t1 = 0; t1 < W; ++t1) {
+#pragma unroll
+        for (int t2 = 0; t2 < W; ++t2) {
+            const float2 *row = tile + ((a1 + t1) * B.t2 + a2 + t2) * B.r3 + a3;
+            const float k12 = w[0][t1] * w[1][t2], m12 = u[0][t1] * u[1][t2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                float rr = 0.f, ri = 0.f, sr = 0.f, si = 0.f;
+#pragma unroll
+                for (int t3 = 0; t3 < W; ++t3) {
+                    const float2 v = row[c * tsz + t3];
+                    rr = fmaf(w[2][t3], v.x, rr);
+                    ri = fmaf(w[2][t3], v.y, ri);
+                    sr = fmaf(u[2][t3], v.x, sr);
+                    si = fmaf(u[2][t3], v.y, si);
+                }
+                out[c].x = fmaf(k12, rr, out[c].x);
+                out[c].y = fmaf(k12, ri, out[c].y);
+                outu[c].x = fmaf(m12, sr, outu[c].x);
+                outu[c].y = fmaf(m12, si, outu[c].y);
+            }
+        }
+    }
+}
+
 // global-memory paths for a point outside its bin's tile (never taken when the
 // sort and the kernels agree on the taps); out of line to spare registers
 template <int W, int NC>
@@ -539,18 +573,16 @@ struct RawStrength {
         s[0] = c[pid];
     }
 };
-// forward: P[fftshift2 position] = sum_i coeff_i(th) * v_i
-struct ForwardSink {
-    float2 *P;
-    __device__ __forceinline__ void operator()(const GeomView &g, int p, int j, int k, uint32_t,
-                                               const float2 *v) const {
-        const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
-        const float2 o = make_float2(c0 * v[0].x + c1 * v[1].x + c2 * v[2].x, c0 * v[0].y + c1 * v[1].y + c2 * v[2].y);
-        int js = j - g.nrows / 2; if (js < 0) js += g.nrows;
-        int ks = k - g.ncols / 2; if (ks < 0) ks += g.ncols;
-        P[((int64_t)p * g.nrows + js) * g.ncols + ks] = o;
-    }
-};
+// forward: P[fftshift2 position of (j, k)] = sum_i coeff_i(th) * v_i
+__device__ __forceinline__ float2 beam_combine(const GeomView &g, int p, const float2 *v) {
+    const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p), c2 = __ldg(g.coeff + 2 * g.nproj + p);
+    return make_float2(c0 * v[0].x + c1 * v[1].x + c2 * v[2].x, c0 * v[0].y + c1 * v[1].y + c2 * v[2].y);
+}
+__device__ __forceinline__ void forward_store(const GeomView &g, int p, int j, int k, float2 o, float2 *P) {
+    int js = j - g.nrows / 2; if (js < 0) js += g.nrows;
+    int ks = k - g.ncols / 2; if (ks < 0) ks += g.ncols;
+    P[((int64_t)p * g.nrows + js) * g.ncols + ks] = o;
+}
 struct RawSink {
     float2 *c;
     __device__ __forceinline__ void operator()(const GeomView &, int, int, int, uint32_t pid, const float2 *v) const {
@@ -822,6 +854,35 @@ __global__ void __launch_bounds__(kStageChunk, 2) k_spread_binned(GeomView g, co
     flush_tile<NC>(tile, tsz, B, o, F, H, NF);
 }
 
+// Both points of pair `pid`: the first point's position, tile offsets (a1 < 0 when
+// outside the bin) and tap offsets d, and the second point's position x2 = -x_{i'}
+// with its tap offsets e on the first point's footprint; `near` as es_offset_from.
+struct PairPos {
+    int p, j, k, j2, k2, a1, a2, a3;
+    float x, y, z, x2, y2, z2;
+    float d1, d2, d3, e1, e2, e3;
+    bool in, near, self;
+};
+template <int W>
+__device__ __forceinline__ void pair_positions(const GeomView &g, const Fine &F, const BinLayout &B,
+                                               const BinOrigin &o, uint32_t pid, PairPos &q) {
+    decode_pair(pid, g, q.p, q.j, q.k, q.j2, q.k2);
+    q.self = q.j2 == q.j && q.k2 == q.k;
+    point_xyz(g, q.p, q.j, q.k, q.x, q.y, q.z);
+    double l1, l2, l3;
+    q.a3 = es_start<W>(q.x, F.nf3, F.s3, q.d3, l3) - o.o3;
+    q.a2 = es_start<W>(q.y, F.nf2, F.s2, q.d2, l2) - o.o2;
+    q.a1 = es_start<W>(q.z, F.nf1, F.s1, q.d1, l1) - o.o1;
+    q.in = (unsigned)q.a1 < (unsigned)B.b1 && (unsigned)q.a2 < (unsigned)B.b2 && (unsigned)q.a3 < (unsigned)B.b3;
+    float xa, ya, za;
+    point_xyz(g, q.p, q.j2, q.k2, xa, ya, za);
+    q.x2 = -xa;
+    q.y2 = -ya;
+    q.z2 = -za;
+    q.near = es_offset_from<W>(q.x2, F.s3, l3, q.e3) && es_offset_from<W>(q.y2, F.s2, l2, q.e2) &&
+             es_offset_from<W>(q.z2, F.s1, l1, q.e1);
+}
+
 // Adjoint spread over antipodal pairs (see decode_pair): two threads stage a
 // pair, the even one its first point (offsets, weights, strengths
 // coeff_i(th) P), the odd one its second point -x_{i'} (weights on the first
@@ -956,22 +1017,71 @@ __global__ void __launch_bounds__(256) k_interp_binned(GeomView g, const uint32_
     }
 }
 
-// sysmat per point, binned: gather 3 components from the input tile (a thread
-// per point), combine with the beam vector, stage, then spread into the output
-// tile as k_spread_binned (src/gradient.cpp:34-89)
+// Forward interpolation over antipodal pairs: a thread per pair gathers both
+// points from the tile (each tile value read once, weighted for both).  The
+// fine grid is the transform of a real volume, so G(-m) = conj(G(m)) and the
+// value at the antipode x_{i'} is conj of the gather at x2 = -x_{i'}; each is
+// combined with the beam vector and stored at its detector position.
 template <int W>
-__global__ void __launch_bounds__(kStageChunk, 2) k_sysmat_binned(GeomView g, const uint32_t *__restrict__ perm,
-                                                       const uint32_t *__restrict__ start, BinLayout B, Fine F,
-                                                       const float2 *__restrict__ G, float2 *__restrict__ H,
-                                                       int64_t NF, float inv_scale) {
-    extern __shared__ float2 sm[];
+__global__ void __launch_bounds__(256) k_interp_pairs(GeomView g, const uint32_t *__restrict__ perm,
+                                                      const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                      const float2 *__restrict__ G, int64_t NF, float2 *__restrict__ P) {
+    extern __shared__ float2 tile[];
     const int bin = blockIdx.x;
     const uint32_t p0 = start[bin], p1 = start[bin + 1];
     if (p0 == p1) return;
     const BinOrigin o = bin_origin(B, bin);
     const int tsz = (int)B.tile_cells();
-    float2 *gt = sm, *ht = sm + 3 * tsz;
-    PointRec<W, 3> *recs = reinterpret_cast<PointRec<W, 3> *>(sm + 6 * tsz);
+    for (int i = threadIdx.x; i < 3 * tsz; i += blockDim.x) {
+        const int c = i / tsz, cell = i - c * tsz;
+        tile[i] = __ldg(G + c * NF + tile_cell_index(B, o, F, cell));
+    }
+    __syncthreads();
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        PairPos q;
+        pair_positions<W>(g, F, B, o, __ldg(perm + i), q);
+        float w[3][W], u[3][W];
+        float2 v[3], vt[3];
+        if (q.in && q.near) {
+            es_weights<W>(q.d1, F.beta, w[0]);
+            es_weights<W>(q.d2, F.beta, w[1]);
+            es_weights<W>(q.d3, F.beta, w[2]);
+            es_weights<W>(q.e1, F.beta, u[0]);
+            es_weights<W>(q.e2, F.beta, u[1]);
+            es_weights<W>(q.e3, F.beta, u[2]);
+            gather_tile_pair<W, 3>(tile, tsz, B, q.a1, q.a2, q.a3, w, u, v, vt);
+        } else {
+            interp_point_global<W, 3>(G, NF, F, q.x, q.y, q.z, v);
+            interp_point_global<W, 3>(G, NF, F, q.x2, q.y2, q.z2, vt);
+        }
+        forward_store(g, q.p, q.j, q.k, beam_combine(g, q.p, v), P);
+        if (!q.self) {
+            const float2 b = beam_combine(g, q.p, vt);
+            forward_store(g, q.p, q.j2, q.k2, make_float2(b.x, -b.y), P);
+        }
+    }
+}
+
+// sysmat over antipodal pairs, binned (src/gradient.cpp:34-89): a thread per
+// pair gathers both points' 3 components from the input tile (the second as in
+// k_interp_pairs), forms both strengths c_i (sum_k c_k v_k) / (nrows ncols) and
+// stages one pair record; the records are spread into the output tile as the
+// adjoint's are.  The second point's record strength is formed from the gather
+// at x2 itself, without the conjugation: that is the conjugate of its true
+// strength, which is what the pair rule spreads at x2.
+template <int W>
+__global__ void __launch_bounds__(kStageChunk, 1) k_sysmat_pairs(GeomView g, const uint32_t *__restrict__ perm,
+                                                      const uint32_t *__restrict__ start, BinLayout B, Fine F,
+                                                      const float2 *__restrict__ G, float2 *__restrict__ H,
+                                                      int64_t NF, float inv_scale) {
+    extern __shared__ __align__(16) unsigned char psm[];
+    const int bin = blockIdx.x;
+    const uint32_t p0 = start[bin], p1 = start[bin + 1];
+    if (p0 == p1) return;
+    const BinOrigin o = bin_origin(B, bin);
+    const int tsz = (int)B.tile_cells();
+    float2 *gt = reinterpret_cast<float2 *>(psm), *ht = gt + 3 * tsz;
+    PairRec<W, 3> *recs = reinterpret_cast<PairRec<W, 3> *>(psm + pair_rec_offset(tsz, 6));
     for (int i = threadIdx.x; i < 3 * tsz; i += blockDim.x) {
         const int c = i / tsz, cell = i - c * tsz;
         gt[i] = __ldg(G + c * NF + tile_cell_index(B, o, F, cell));
@@ -980,51 +1090,64 @@ __global__ void __launch_bounds__(kStageChunk, 2) k_sysmat_binned(GeomView g, co
     __syncthreads();
     __shared__ int wcnt[kStageWarps * kMaxB1];
     __shared__ int bstart[kMaxB1 + 1];
+    const int t = threadIdx.x;  // one pair per thread (blockDim.x == kStageChunk)
     for (uint32_t base = p0; base < p1; base += kStageChunk) {
         const int n = (int)min((uint32_t)kStageChunk, p1 - base);
-        const int t = threadIdx.x;  // one point per thread (blockDim.x == kStageChunk)
-        int p = 0, j = 0, k = 0, a1 = -1, a2 = 0, a3 = 0;
-        float x = 0.f, y = 0.f, z = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-        bool in = false;
+        PairPos q;
+        q.in = false;
+        if (t < n) pair_positions<W>(g, F, B, o, __ldg(perm + base + t), q);
+        const int pos = place_slot(t < n && q.in ? q.a1 : -1, wcnt, bstart, B);
         if (t < n) {
-            const uint32_t pid = __ldg(perm + base + t);
-            decode_pid(pid, g, p, j, k);
-            point_xyz(g, p, j, k, x, y, z);
-            a3 = es_start<W>(x, F.nf3, F.s3, d3) - o.o3;
-            a2 = es_start<W>(y, F.nf2, F.s2, d2) - o.o2;
-            a1 = es_start<W>(z, F.nf1, F.s1, d1) - o.o1;
-            in = (unsigned)a1 < (unsigned)B.b1 && (unsigned)a2 < (unsigned)B.b2 && (unsigned)a3 < (unsigned)B.b3;
-        }
-        const int pos = place_slot(in ? a1 : -1, wcnt, bstart, B);
-        if (t < n) {
-            float2 v[3];
-            if (in) {
-                PointRec<W, 3> &pr = recs[pos];
-                pr.a1 = a1;
-                pr.a2 = a2;
-                pr.a3 = a3;
-                es_weights<W>(d1, F.beta, pr.w1);
-                es_weights<W>(d2, F.beta, pr.w2);
-                es_weights<W>(d3, F.beta, pr.w3);
-                gather_tile<W, 3>(gt, tsz, B, a1, a2, a3, pr.w1, pr.w2, pr.w3, v);
+            float w[3][W], u[3][W];
+            float2 v[3], vt[3];
+            es_weights<W>(q.d1, F.beta, w[0]);
+            es_weights<W>(q.d2, F.beta, w[1]);
+            es_weights<W>(q.d3, F.beta, w[2]);
+            if (q.near) {
+                es_weights<W>(q.e1, F.beta, u[0]);
+                es_weights<W>(q.e2, F.beta, u[1]);
+                es_weights<W>(q.e3, F.beta, u[2]);
             } else {
-                interp_point_global<W, 3>(G, NF, F, x, y, z, v);
+#pragma unroll
+                for (int r = 0; r < W; ++r) u[0][r] = u[1][r] = u[2][r] = 0.f;
             }
-            const float c0 = __ldg(g.coeff + p), c1 = __ldg(g.coeff + g.nproj + p),
-                        c2 = __ldg(g.coeff + 2 * g.nproj + p);
+            if (q.in)
+                gather_tile_pair<W, 3>(gt, tsz, B, q.a1, q.a2, q.a3, w, u, v, vt);
+            else
+                interp_point_global<W, 3>(G, NF, F, q.x, q.y, q.z, v);
+            const bool far2 = !q.in || !q.near;  // second point through global memory
+            if (far2) interp_point_global<W, 3>(G, NF, F, q.x2, q.y2, q.z2, vt);
+            const float c0 = __ldg(g.coeff + q.p), c1 = __ldg(g.coeff + g.nproj + q.p),
+                        c2 = __ldg(g.coeff + 2 * g.nproj + q.p);
             const float sr = (c0 * v[0].x + c1 * v[1].x + c2 * v[2].x) * inv_scale;
             const float si = (c0 * v[0].y + c1 * v[1].y + c2 * v[2].y) * inv_scale;
-            const float2 s[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
-                                 make_float2(c2 * sr, c2 * si)};
-            if (in) {
+            float tr = (c0 * vt[0].x + c1 * vt[1].x + c2 * vt[2].x) * inv_scale;
+            float ti = (c0 * vt[0].y + c1 * vt[1].y + c2 * vt[2].y) * inv_scale;
+            if (q.self) tr = ti = 0.f;
+            const float2 sv[3] = {make_float2(c0 * sr, c0 * si), make_float2(c1 * sr, c1 * si),
+                                  make_float2(c2 * sr, c2 * si)};
+            const float2 gv[3] = {make_float2(c0 * tr, c0 * ti), make_float2(c1 * tr, c1 * ti),
+                                  make_float2(c2 * tr, c2 * ti)};
+            if (far2) spread_point_global<W, 3>(H, NF, F, q.x2, q.y2, q.z2, gv);
+            if (q.in) {
+                PairRec<W, 3> &pr = recs[pos];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) recs[pos].s[c] = s[c];
+                for (int r = 0; r < W; ++r) {
+                    pr.w1[r] = make_float2(w[0][r], u[0][r]);
+                    pr.w2[r] = make_float2(w[1][r], u[1][r]);
+                    pr.w3[r] = make_float2(w[2][r], u[2][r]);
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    pr.sg[c] = far2 ? make_float4(sv[c].x, sv[c].y, 0.f, 0.f)
+                                    : make_float4(sv[c].x, sv[c].y, gv[c].x, gv[c].y);
+                pr.a = q.a1 | (q.a2 << 8) | (q.a3 << 20);
             } else {
-                spread_point_global<W, 3>(H, NF, F, x, y, z, s);
+                spread_point_global<W, 3>(H, NF, F, q.x, q.y, q.z, sv);
             }
         }
         __syncthreads();
-        spread_sorted<W, 3>(ht, tsz, B, recs, bstart);
+        spread_pairs_sorted<W, 3>(ht, tsz, B, recs, bstart);
         __syncthreads();
     }
     flush_tile<3>(ht, tsz, B, o, F, H, NF);
@@ -1167,7 +1290,7 @@ void NufftPlan::set_bins(int b1, int b2, int b3) {
     B.nb3 = (int)((nf3 + b3 - 1) / b3);
     B.t1 = b1 + w - 1; B.t2 = b2 + w - 1; B.t3 = b3 + w - 1;
     auto smem_need = [&](const BinLayout &L) {  // the largest kernel: sysmat, two 3-component tiles
-        return 6 * L.tile_cells() * (int64_t)sizeof(float2) + kStageChunk * (int64_t)point_rec_bytes(w, 3);
+        return (int64_t)pair_rec_offset(L.tile_cells(), 6) + kStageChunk * (int64_t)pair_rec_bytes(w, 3);
     };
     B.r3 = B.t3 + (((w - B.t3) % 16) + 16) % 16;  // conflict-free rows when they fit
     // 227 KB per CTA, less the binned kernels' static slab-start tables
@@ -1300,7 +1423,7 @@ double NufftPlan::autotune_bins(const std::vector<const Geom *> &gs, int objecti
 
 void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_t s) {
     ensure_proj(g, s);
-    const SortedPoints &sp = sort_points(g, s);
+    const SortedPoints &sp = sort_points(g, s, true);
     pad_real(m3, 3, s);
     fft_fine(-1, 3, s);
     const Fine F = fine_of(*this);
@@ -1308,11 +1431,10 @@ void NufftPlan::forward(const Geom &g, const float *m3, float *proj, cudaStream_
     const int smem = (int)(3 * bins.tile_cells() * sizeof(float2));
     with_width(w, [&](auto WC) {
         constexpr int W = decltype(WC)::value;
-        auto kern = k_interp_binned<W, 3, ForwardSink>;
+        auto kern = k_interp_pairs<W>;
         raise_smem_limit((const void *)kern, smem);
-        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(),
-                                                        ForwardSink{pbuf.p});
-        LAMINO_LAUNCH("k_interp_binned<forward>");
+        kern<<<(unsigned)bins.nbins(), 256, smem, s>>>(gv, sp.perm.p, sp.start.p, bins, F, gwork.p, nf(), pbuf.p);
+        LAMINO_LAUNCH("k_interp_pairs");
     });
     LAMINO_CUFFT(cufftSetStream(fft2.h, s));
     LAMINO_CUFFT(cufftExecC2C(fft2.h, (cufftComplex *)pbuf.p, (cufftComplex *)pbuf.p, CUFFT_INVERSE));
@@ -1348,21 +1470,21 @@ void NufftPlan::adjoint(const Geom &g, const float *proj, float *m3, bool accumu
 // `may_sort`: build missing point orders (allocates) or fall back to the direct kernel
 void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cudaStream_t s) {
     const Fine F = fine_of(*this);
-    const int smem = (int)(6 * bins.tile_cells() * sizeof(float2) + kStageChunk * point_rec_bytes(w, 3));
+    const int smem = (int)(pair_rec_offset(bins.tile_cells(), 6) + kStageChunk * pair_rec_bytes(w, 3));
     for (int i = 0; i < ng; ++i) {
         const Geom &g = *gs[i];
         if (g.npts() > (int64_t)UINT32_MAX / 2) throw Error(ERR_ARG, "too many points in one geometry");
         const GeomView gv = g.view();
         const float inv_scale = 1.0f / (float)(g.nrows * g.ncols);
-        const SortedPoints *sp = may_sort ? &sort_points(g, s) : find_sorted(g);
+        const SortedPoints *sp = may_sort ? &sort_points(g, s, true) : find_sorted(g, true);
         with_width(w, [&](auto WC) {
             constexpr int W = decltype(WC)::value;
             if (sp) {
-                auto kern = k_sysmat_binned<W>;
+                auto kern = k_sysmat_pairs<W>;
                 raise_smem_limit((const void *)kern, smem);
                 kern<<<(unsigned)bins.nbins(), kStageChunk, smem, s>>>(gv, sp->perm.p, sp->start.p, bins, F, gwork.p,
                                                                         gin.p, nf(), inv_scale);
-                LAMINO_LAUNCH("k_sysmat_binned");
+                LAMINO_LAUNCH("k_sysmat_pairs");
             } else {
                 unsigned grid = grid_for(g.npts(), 256, 148LL * 16 * 8);
                 k_sysmat_points<W><<<grid, 256, 0, s>>>(gv, gwork.p, gin.p, nf(), F, inv_scale);
@@ -1374,7 +1496,7 @@ void NufftPlan::normal_points(const Geom *const *gs, int ng, bool may_sort, cuda
 
 void NufftPlan::normal(const std::vector<const Geom *> &gs, const float *x3, float *y3, cudaStream_t s) {
     if (gs.empty()) throw Error(ERR_ARG, "normal operator needs at least one geometry");
-    for (const Geom *g : gs) sort_points(*g, s);  // before any work on the grids
+    for (const Geom *g : gs) sort_points(*g, s, true);  // before any work on the grids
     normal_impl(gs.data(), (int)gs.size(), true, x3, y3, s);
 }
 
