@@ -42,8 +42,9 @@ void normalize_pad2d(const float *proj, int64_t np, int64_t nr, int64_t nc, floa
     }
     onr = nr + p2;
     onc = nc + p3;
-    out.alloc(np * onr * onc);
-    LAMINO_CUDA(cudaMemsetAsync(out.p, 0, out.bytes(), s));
+    const int64_t need = np * onr * onc;
+    if ((int64_t)out.n < need) out.alloc(need);  // a buffer from an earlier dataset is reused
+    LAMINO_CUDA(cudaMemsetAsync(out.p, 0, need * sizeof(float), s));
     k_norm_pad2d<<<grid_for(np * nr * nc, 256), 256, 0, s>>>(proj, np, (int)nr, (int)nc, mx, (int)onr, (int)onc,
                                                             (int)(p2 / 2), (int)(p3 / 2), out.p);
     LAMINO_LAUNCH("k_norm_pad2d");
@@ -157,12 +158,12 @@ void MbirJob::prepare() {
     yT_.alloc(n);
     LAMINO_CUDA(cudaMemsetAsync(yT_.p, 0, yT_.bytes(), s));
     Reducer red(8);
+    DevBuf<float> y;  // normalised, padded projections of the dataset in hand
     for (const Dataset &ds : data) {
         red.zero(1, s);
         vec_max(ds.proj, ds.nproj * ds.nrows * ds.ncols, red.d, s);
         red.fetch(1, s);
         float mx = (float)red.h[0];
-        DevBuf<float> y;
         int64_t nr, nc;
         normalize_pad2d(ds.proj, ds.nproj, ds.nrows, ds.ncols, mx, pfac, y, nr, nc, s);
         geoms_.emplace_back(new Geom(ds.angles, ds.nproj, nr, nc, ds.gamma));

@@ -39,7 +39,8 @@ struct Dataset {
 // Padded volume dims n + 2 floor(n (PAD-1) / 2) (src/mbir_sb.cpp:50-60).
 int64_t pad_dim(int64_t n, float factor_minus_one);
 
-// pad2d (include/padding.h:94-131) fused with the 1/max normalisation; returns new dims
+// pad2d (include/padding.h:94-131) fused with the 1/max normalisation; returns new
+// dims; `out` is reallocated only when smaller than the padded projections
 void normalize_pad2d(const float *proj, int64_t np, int64_t nr, int64_t nc, float inv_max, float factor,
                      DevBuf<float> &out, int64_t &onr, int64_t &onc, cudaStream_t s);
 // crop3d (include/padding.h:207-232, symmetric), 3 components
