@@ -514,10 +514,18 @@ __device__ __forceinline__ void gather_tile_pair(const float2 *tile, int tsz, co
     for (int c = 0; c < NC; ++c) out[c] = outu[c] = make_float2(0.f, 0.f);
 #pragma unroll 1
     for (int t1 = 0; t1 < W; ++t1) {
+        // the slab weights by selects, so that no weight array is indexed at run
+        // time (which would move the arrays to local memory)
+        float w1 = w[0][0], u1 = u[0][0];
+#pragma unroll
+        for (int r = 1; r < W; ++r) {
+            w1 = t1 == r ? w[0][r] : w1;
+            u1 = t1 == r ? u[0][r] : u1;
+        }
 #pragma unroll
         for (int t2 = 0; t2 < W; ++t2) {
             const float2 *row = tile + ((a1 + t1) * B.t2 + a2 + t2) * B.r3 + a3;
-            const float k12 = w[0][t1] * w[1][t2], m12 = u[0][t1] * u[1][t2];
+            const float k12 = w1 * w[1][t2], m12 = u1 * u[1][t2];
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 float rr = 0.f, ri = 0.f, sr = 0.f, si = 0.f;
